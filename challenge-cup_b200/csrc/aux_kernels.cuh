@@ -1,0 +1,431 @@
+// Auxiliary kernels around the stencil: material setup, receiver sampling,
+// time-reversed injection, image fields, imaging conditions, viscoacoustic
+// stabilisation and image post-processing.  All are HBM-bound elementwise or
+// gather/scatter work.
+#pragma once
+
+#include "ertm_device.cuh"
+
+namespace ertm {
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---------------------------------------------------------------------------
+// material setup on the padded grid (propagation.py:165-187, 411-421,
+// 588-675, 858-871): edge padding, κ = ρ·v²·, 1/ρ averaged to faces,
+// μ averaged to corners.  Inputs are the physical (nz, nx) float32 arrays.
+// ---------------------------------------------------------------------------
+struct SetupArgs {
+  const float* vp; const float* vs; const float* rho;   // physical (nz, nx)
+  // visco relaxation tables, per unique Q value
+  const double* tau;     // [nq][L]
+  const double* delta;   // [nq][L] (already −αΔ under compensation)
+  const double* mref;    // [nq]
+  const float* relax_a;  // [nq][L] float32 exp(−dt/τ)
+  double dt;
+};
+
+__device__ __forceinline__ float padded_at(const float* a, int nz, int nx, int pad, int i, int j) {
+  return a[(size_t)clampi(i - pad, 0, nz - 1) * nx + clampi(j - pad, 0, nx - 1)];
+}
+
+__global__ void k_setup_materials(DevProp* props, int pi, SetupArgs A) {
+  const DevProp& P = props[pi];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= P.nzp || j >= P.nxp) return;
+  const int nz = P.nz, nx = P.nx, pad = P.pad;
+  const size_t g = (size_t)i * P.ld + j;
+  auto inv_rho = [&](int ii, int jj) { return fdiv(1.0f, padded_at(A.rho, nz, nx, pad, ii, jj)); };
+  const float ir = inv_rho(i, j);
+  const float irx = (j < P.nxp - 1) ? fmul(0.5f, fadd(ir, inv_rho(i, j + 1))) : ir;
+  const float irz = (i < P.nzp - 1) ? fmul(0.5f, fadd(ir, inv_rho(i + 1, j))) : ir;
+  const float rho = padded_at(A.rho, nz, nx, pad, i, j);
+  const float vp = padded_at(A.vp, nz, nx, pad, i, j);
+  float* const* C = const_cast<float* const*>(reinterpret_cast<const float* const*>(P.coef));
+  if (P.engine == ENGINE_ACOUSTIC) {
+    C[CA_KAPPA][g] = fmul(fmul(rho, vp), vp);
+    C[CA_IRX][g] = irx;
+    C[CA_IRZ][g] = irz;
+  } else if (P.engine == ENGINE_ELASTIC) {
+    auto mu_at = [&](int ii, int jj) {
+      const float r = padded_at(A.rho, nz, nx, pad, ii, jj), s = padded_at(A.vs, nz, nx, pad, ii, jj);
+      return fmul(fmul(r, s), s);
+    };
+    auto mux_at = [&](int ii, int jj) {  // _mean_x(mu)
+      return (jj < P.nxp - 1) ? fmul(0.5f, fadd(mu_at(ii, jj), mu_at(ii, jj + 1))) : mu_at(ii, jj);
+    };
+    const float vs = padded_at(A.vs, nz, nx, pad, i, j);
+    const float mu = fmul(fmul(rho, vs), vs);
+    const float lam = fmul(rho, fsub(fmul(vp, vp), fmul(fmul(2.0f, vs), vs)));
+    C[CE_LAM][g] = lam;
+    C[CE_L2M][g] = fadd(lam, fmul(2.0f, mu));
+    C[CE_MUXZ][g] = (i < P.nzp - 1) ? fmul(0.5f, fadd(mux_at(i, j), mux_at(i + 1, j))) : mux_at(i, j);
+    C[CE_IRX][g] = irx;
+    C[CE_IRZ][g] = irz;
+  } else {
+    const float kappa = fmul(fmul(rho, vp), vp);
+    const int q = P.qidx[g];
+    const float kr = __double2float_rn(__ddiv_rn((double)kappa, A.mref[q]));
+    C[CV_KR][g] = kr;
+    C[CV_IRX][g] = irx;
+    C[CV_IRZ][g] = irz;
+    for (int l = 0; l < P.L; ++l) {
+      const float one_minus_a = fsub(1.0f, A.relax_a[q * P.L + l]);
+      double b = dmul(dmul(dmul((double)kr, A.delta[q * P.L + l]), (double)one_minus_a), A.tau[q * P.L + l]);
+      C[CV_B0 + l][g] = __double2float_rn(__ddiv_rn(b, A.dt));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// receiver sampling (numerics.py:478-511, propagation.py:371-391)
+// ---------------------------------------------------------------------------
+enum SampleKind : int32_t { SAMPLE_FIELD = 0, SAMPLE_PRESSURE = 1, SAMPLE_ZERO = 2 };
+
+struct SamplePlanDev {
+  int32_t n;            // receivers
+  int32_t kind;         // SampleKind
+  int32_t field;        // field slot (SAMPLE_FIELD)
+  int32_t pad_;
+  const int32_t* cell;  // zc·ld + xc (clipped floor node)
+  const uint8_t* valid;
+  const double* w;      // [n][4]: 1−tz, tz, 1−tx, tx
+  float* out;           // row base for this step (n floats)
+};
+
+constexpr int MAX_SAMPLE = 8;
+struct SampleSet {
+  int32_t count;
+  SamplePlanDev plan[MAX_SAMPLE];
+};
+
+__device__ __forceinline__ double corner(const DevProp& P, int kind, int field, int32_t idx) {
+  if (kind == SAMPLE_PRESSURE) return (double)fmul(0.5f, fadd(P.f[E_SXX][idx], P.f[E_SZZ][idx]));
+  return (double)P.f[field][idx];
+}
+
+// One thread per (component, receiver); writes the float32 sample of this step.
+__global__ void k_sample(const DevProp* props, int pi, SampleSet S, int64_t row_offset) {
+  const DevProp& P = props[pi];
+  const int comp = blockIdx.y;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (comp >= S.count) return;
+  const SamplePlanDev& sp = S.plan[comp];
+  if (r >= sp.n) return;
+  float v = 0.f;
+  if (sp.kind != SAMPLE_ZERO && sp.valid[r]) {
+    const int32_t c0 = sp.cell[r];
+    const double* w = sp.w + 4 * r;
+    const double v00 = corner(P, sp.kind, sp.field, c0), v01 = corner(P, sp.kind, sp.field, c0 + 1);
+    const double v10 = corner(P, sp.kind, sp.field, c0 + P.ld), v11 = corner(P, sp.kind, sp.field, c0 + P.ld + 1);
+    double acc = dmul(dmul(v00, w[0]), w[2]);
+    acc = dadd(acc, dmul(dmul(v01, w[0]), w[3]));
+    acc = dadd(acc, dmul(dmul(v10, w[1]), w[2]));
+    acc = dadd(acc, dmul(dmul(v11, w[1]), w[3]));
+    v = __double2float_rn(acc);
+  }
+  sp.out[row_offset + r] = v;
+}
+
+// ---------------------------------------------------------------------------
+// time-reversed injection with np.add.at semantics (propagation.py:331-369,
+// 472-494, 916-942): every contribution is added in float64 and rounded to
+// float32, in the reference order (component, corner, receiver).  The host
+// groups contributions by target cell, so one thread owns one cell and the
+// launch is deterministic without atomics.
+// ---------------------------------------------------------------------------
+struct InjectPlanDev {
+  int32_t n_cells;
+  int32_t pad_;
+  const int32_t* cell_field;  // field slot per target cell
+  const int32_t* cell_index;  // i·ld + j per target cell
+  const int32_t* start;       // [n_cells + 1] into the contribution arrays
+  const int32_t* src;         // record offset (component·nt·nrec + receiver) per contribution
+  const double* wa;           // contribution = (value·wa)·wb
+  const double* wb;
+};
+
+__global__ void k_inject(const DevProp* props, int pi, InjectPlanDev plan, const float* record,
+                         int64_t time_offset) {
+  const DevProp& P = props[pi];
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= plan.n_cells) return;
+  float* f = P.f[plan.cell_field[u]] + plan.cell_index[u];
+  float acc = *f;
+  for (int k = plan.start[u]; k < plan.start[u + 1]; ++k) {
+    const double v = (double)record[plan.src[k] + time_offset];
+    acc = __double2float_rn(dadd((double)acc, dmul(dmul(v, plan.wa[k]), plan.wb[k])));
+  }
+  *f = acc;
+}
+
+// Single-cell add (elastic force_z source lands on vz after the stress phase).
+__global__ void k_point_add(float* f, int64_t idx, float amp) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) f[idx] = fadd(f[idx], amp);
+}
+
+// ---------------------------------------------------------------------------
+// image fields (propagation.py:500-501, 795-796, 945-977)
+// ---------------------------------------------------------------------------
+enum Wave : int32_t { WAVE_P = 0, WAVE_S = 1 };
+enum Separation : int32_t { SEP_STRESS = 0, SEP_DIVCURL = 1 };
+
+template <int M>
+__device__ __forceinline__ float image_value(const DevProp& P, int wave, int sep, int i, int j) {
+  const size_t g = (size_t)i * P.ld + j;
+  if (P.engine != ENGINE_ELASTIC) return P.f[A_P][g];
+  if (sep == SEP_STRESS) {
+    if (wave == WAVE_P) return fmul(0.5f, fadd(P.f[E_SXX][g], P.f[E_SZZ][g]));
+    return P.f[E_SXZ][g];
+  }
+  const float c[4] = {P.c[0], P.c[1], P.c[2], P.c[3]};
+  const float* vx = P.f[E_VX] + g;
+  const float* vz = P.f[E_VZ] + g;
+  // Physical cells are ≥ M+1 from every padded edge, so each D⁻ is in range.
+  if (wave == WAVE_P) return fadd(dminus<M>(vx, 1, c, P.hx), dminus<M>(vz, P.ld, c, P.hz));
+  return fsub(dminus<M>(vx, P.ld, c, P.hz), dminus<M>(vz, 1, c, P.hx));
+}
+
+template <int M>
+__global__ void k_image_field(const DevProp* props, int pi, int wave, int sep, float* out) {
+  const DevProp& P = props[pi];
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= P.nz || jj >= P.nx) return;
+  out[(size_t)ii * P.nx + jj] = image_value<M>(P, wave, sep, ii + P.pad, jj + P.pad);
+}
+
+// ---------------------------------------------------------------------------
+// imaging conditions (imaging.py:61-87, 279-331)
+// ---------------------------------------------------------------------------
+// Accumulators: FP64 (reference-exact, default) or Kahan-compensated FP32
+// (sum, compensation) pairs stored in the same 8 bytes per cell.
+struct Accum {
+  double* d;    // FP64 mode
+  float* s;     // Kahan mode: running sum
+  float* comp;  // Kahan mode: compensation
+};
+
+template <bool KAHAN>
+__device__ __forceinline__ void acc_add(const Accum& a, size_t c, float term) {
+  if constexpr (!KAHAN) {
+    a.d[c] = dadd(a.d[c], (double)term);
+  } else {
+    const float y = fsub(term, a.comp[c]);
+    const float s = a.s[c];
+    const float t = fadd(s, y);
+    a.comp[c] = fsub(fsub(t, s), y);
+    a.s[c] = t;
+  }
+}
+
+constexpr int MAX_IMAGES = 4;
+struct ImagingArgs {
+  int32_t n_images;
+  int32_t illum;                  // accumulate S² and R² (normalized / receiver normalisation)
+  int32_t cross;                  // accumulate S·R (t ≥ start_step)
+  int32_t sep;
+  int32_t src_wave[MAX_IMAGES];   // which stored source field (slot index into src)
+  int32_t rcv_wave[MAX_IMAGES];
+  const float* src[2];            // replayed source image fields of this step (P, S slots)
+  Accum num[MAX_IMAGES];
+  Accum illum_acc[MAX_IMAGES];
+  Accum rillum_acc[MAX_IMAGES];
+};
+
+template <int M, bool KAHAN>
+__global__ void k_imaging(const DevProp* props, int back, ImagingArgs A) {
+  const DevProp& P = props[back];
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= P.nz || jj >= P.nx) return;
+  const size_t c = (size_t)ii * P.nx + jj;
+  float rv[2];
+  rv[0] = image_value<M>(P, WAVE_P, A.sep, ii + P.pad, jj + P.pad);
+  rv[1] = (P.engine == ENGINE_ELASTIC) ? image_value<M>(P, WAVE_S, A.sep, ii + P.pad, jj + P.pad) : 0.f;
+  for (int k = 0; k < A.n_images; ++k) {
+    const float s = A.src[A.src_wave[k]][c];
+    const float r = rv[A.rcv_wave[k]];
+    if (A.illum) {
+      acc_add<KAHAN>(A.illum_acc[k], c, fmul(s, s));
+      acc_add<KAHAN>(A.rillum_acc[k], c, fmul(r, r));
+    }
+    if (A.cross) acc_add<KAHAN>(A.num[k], c, fmul(s, r));
+  }
+}
+
+// Excitation map: running argmax of |P| over the replayed source field
+// (imaging.py:450-474).  running is stored in float32 (it only ever holds
+// |P| values, which float64 would store exactly too).
+template <int M>
+__global__ void k_excitation_track(const DevProp* props, int pi, int sep, float* running, int32_t* peak_step,
+                                   int step) {
+  const DevProp& P = props[pi];
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= P.nz || jj >= P.nx) return;
+  const size_t c = (size_t)ii * P.nx + jj;
+  const float a = fabsf(image_value<M>(P, WAVE_P, sep, ii + P.pad, jj + P.pad));
+  if (a > running[c]) {
+    running[c] = a;
+    peak_step[c] = step;
+  }
+}
+
+// Excitation imaging at backward step t (imaging.py:290-303): where the
+// source peaked at t, num += A·R (float64 product) and rillum += R² (float32).
+template <int M>
+__global__ void k_excitation_image(const DevProp* props, int back, int sep, int n_images,
+                                   const int32_t* rcv_wave, const float* running, const int32_t* peak_step,
+                                   int step, Accum num0, Accum num1, Accum rill0, Accum rill1) {
+  const DevProp& P = props[back];
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ii >= P.nz || jj >= P.nx) return;
+  const size_t c = (size_t)ii * P.nx + jj;
+  if (peak_step[c] != step) return;
+  const double a = (double)running[c];
+  for (int k = 0; k < n_images; ++k) {
+    const float r = image_value<M>(P, rcv_wave[k], sep, ii + P.pad, jj + P.pad);
+    const Accum& num = k == 0 ? num0 : num1;
+    const Accum& ril = k == 0 ? rill0 : rill1;
+    num.d[c] = dadd(num.d[c], dmul(a, (double)r));
+    ril.d[c] = dadd(ril.d[c], (double)fmul(r, r));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// viscoacoustic compensation safety net (propagation.py:726-749)
+// ---------------------------------------------------------------------------
+struct StabState {
+  double ref_amp;   // reference amplitude: running max|p| over steps < 30
+  int32_t clipped;  // amplitude-cap events
+  int32_t pad_;
+};
+
+__global__ void k_stab_reference(const DevProp* props, int pi, StabState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const double peak = (double)*props[pi].peak;
+    st->ref_amp = st->ref_amp > peak ? st->ref_amp : peak;
+  }
+}
+
+// Scale p, ε, vx, vz, r_l by float32(limit/peak) when max|p| exceeds the cap.
+__global__ void k_stab_scale(const DevProp* props, int pi, StabState* st, double cap) {
+  const DevProp& P = props[pi];
+  const double peak = (double)*P.peak;
+  const double ref = st->ref_amp > 1e-30 ? st->ref_amp : 1e-30;
+  const double limit = cap * ref;
+  if (!(peak > limit)) return;
+  const float s = __double2float_rn(__ddiv_rn(limit, peak));
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->clipped += 1;
+  const size_t n = (size_t)P.nzp * P.ld;
+  const int nf = 4 + P.L;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    for (int f = 0; f < nf; ++f) P.f[f][k] = fmul(P.f[f][k], s);
+  }
+}
+
+// Radial wavenumber taper 1 − (k − c)/0.15 clipped to [0, 1], applied to a
+// half spectrum (numerics.py:424-442); the 1/(nz·nx) inverse-FFT scale is
+// folded in.
+__global__ void k_lowpass_apply(double2* spec, int nz, int nx, double dz, double dx, double cutoff) {
+  const int nxh = nx / 2 + 1;
+  const int jx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+  if (iz >= nz || jx >= nxh) return;
+  const int kzi = iz < (nz + 1) / 2 ? iz : iz - nz;
+  const int kxi = jx < (nx + 1) / 2 ? jx : jx - nx;
+  const double kz = (double)kzi * (1.0 / (nz * dz)) / (0.5 / dz);
+  const double kx = (double)kxi * (1.0 / (nx * dx)) / (0.5 / dx);
+  const double rad = sqrt(kz * kz + kx * kx);
+  double h = 1.0 - (rad - cutoff) / 0.15;
+  h = h < 0.0 ? 0.0 : (h > 1.0 ? 1.0 : h);
+  h /= (double)nz * (double)nx;
+  double2& v = spec[(size_t)iz * nxh + jx];
+  v.x *= h;
+  v.y *= h;
+}
+
+// padded float32 field (pitch ld) ↔ dense float64 (nzp, nxp)
+__global__ void k_f32_to_f64(const float* src, int ld, double* dst, int nz, int nx) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < nz && j < nx) dst[(size_t)i * nx + j] = (double)src[(size_t)i * ld + j];
+}
+__global__ void k_f64_to_f32(const double* src, float* dst, int ld, int nz, int nx) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < nz && j < nx) dst[(size_t)i * ld + j] = __double2float_rn(src[(size_t)i * nx + j]);
+}
+
+// ---------------------------------------------------------------------------
+// image post-processing (imaging.py:326-331, 476-502; numerics.py:398-404)
+// ---------------------------------------------------------------------------
+struct NormArgs {
+  const double* num; const double* illum; const double* rillum;
+  const float* num_s; const float* illum_s; const float* rillum_s;   // Kahan sums (comp ignored)
+  int32_t kahan;
+  int32_t by_illum, by_rillum;
+  double eps;
+  double* out;
+  int64_t n;
+};
+
+__global__ void k_normalize(NormArgs A) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= A.n) return;
+  double v = A.kahan ? (double)A.num_s[k] : A.num[k];
+  if (A.by_illum) v = __ddiv_rn(v, dadd(A.kahan ? (double)A.illum_s[k] : A.illum[k], A.eps));
+  if (A.by_rillum) v = __ddiv_rn(v, dadd(A.kahan ? (double)A.rillum_s[k] : A.rillum[k], A.eps));
+  A.out[k] = v;
+}
+
+__global__ void k_laplacian(const double* a, double* out, int nz, int nx, double dx, double dz) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= nz || j >= nx) return;
+  auto at = [&](int ii, int jj) { return a[(size_t)clampi(ii, 0, nz - 1) * nx + clampi(jj, 0, nx - 1)]; };
+  const double c = at(i, j);
+  const double d2x = __ddiv_rn(dadd(dsub(at(i, j + 1), dmul(2.0, c)), at(i, j - 1)), dmul(dx, dx));
+  const double d2z = __ddiv_rn(dadd(dsub(at(i + 1, j), dmul(2.0, c)), at(i - 1, j)), dmul(dz, dz));
+  out[(size_t)i * nx + j] = dadd(d2x, d2z);
+}
+
+__global__ void k_mask_cast(const double* a, float* out, int nz, int nx, int npml, int top) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= nz || j >= nx) return;
+  const bool zero = j < npml || j >= nx - npml || i >= nz - npml || (top && i < npml);
+  const double v = a[(size_t)i * nx + j] * (zero ? 0.0 : 1.0);
+  out[(size_t)i * nx + j] = __double2float_rn(v);
+}
+
+// stack_images (pipeline.py:133-161): per-image max|·| then normalised mean.
+__global__ void k_absmax_f32(const float* a, int64_t n, unsigned int* out_bits) {
+  float m = 0.f;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(a[k]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(m));
+}
+
+__global__ void k_stack_add(const float* img, int64_t n, const unsigned int* scale_bits, int normalize,
+                            double* acc) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double d = (double)img[k];
+  if (normalize) {
+    const double s = (double)__uint_as_float(*scale_bits);
+    if (s > 0.0) d = __ddiv_rn(d, s);
+  }
+  acc[k] = dadd(acc[k], d);
+}
+
+__global__ void k_stack_finish(const double* acc, int64_t n, int count, float* out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = __double2float_rn(__ddiv_rn(acc[k], (double)count));
+}
+
+}  // namespace ertm

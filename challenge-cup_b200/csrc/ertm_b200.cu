@@ -1,0 +1,1145 @@
+// Host runtime and C ABI of the B200-native ERTM hot path.
+//
+// A Prop is one propagator (reference: Propagator2D and subclasses,
+// ertm/propagation.py:190-980) whose fields, CPML strips and coefficients live
+// in HBM.  The whole-loop drivers (ertm_forward, ertm_migrate) run the time
+// loops in C++ and only enqueue kernels, so the Python host makes one call
+// per shot instead of one per time step.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ertm_b200.h"
+#include "aux_kernels.cuh"
+#include "step_kernels.cuh"
+
+using namespace ertm;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw Error(ERTM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+#define CKFFT(call)                                                                          \
+  do {                                                                                       \
+    cufftResult r_ = (call);                                                                 \
+    if (r_ != CUFFT_SUCCESS) throw Error(ERTM_ERR_CUDA, std::string(#call) + " failed"); \
+  } while (0)
+#define REQUIRE(cond, msg)                                   \
+  do {                                                       \
+    if (!(cond)) throw Error(ERTM_ERR_ARG, std::string(msg)); \
+  } while (0)
+
+template <class F>
+int32_t guarded(F&& f) {
+  try {
+    f();
+    return ERTM_OK;
+  } catch (const Error& e) {
+    g_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return ERTM_ERR_STATE;
+  }
+}
+
+constexpr int TZ = 32;   // tile rows
+constexpr int BY = 8;    // warps per block (4 rows per thread)
+
+size_t round64(size_t n) { return (n + 63) / 64 * 64; }
+
+// Device allocation that frees itself (stream-ordered).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t b, cudaStream_t s) : bytes(b), st(s) {
+    if (b) CK(cudaMallocAsync(&p, b, s));
+  }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    std::swap(p, o.p);
+    std::swap(bytes, o.bytes);
+    std::swap(st, o.st);
+    return *this;
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+void upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st));
+}
+
+int comp_offsets(int comp, double& xo, double& zo) {
+  // propagation.py:341-345, 380-384, 922-926
+  xo = 0.0;
+  zo = 0.0;
+  if (comp == ERTM_COMP_VX) xo = -0.5;
+  if (comp == ERTM_COMP_VZ) zo = -0.5;
+  if (comp == ERTM_COMP_SXZ) { xo = -0.5; zo = -0.5; }
+  return 0;
+}
+
+struct SamplePlanHost {
+  int kind = SAMPLE_FIELD, slot = 0;
+  DevBuf cell, valid, w;
+  int n = 0;
+};
+
+struct InjectTarget {
+  int slot;
+  int offset_comp;   // component whose offsets apply
+  int scaled;        // 0: (v·w_z)·w_x; 1: v·((w_z·w_x)·1); 2: v·((w_z·w_x)·1/|K_R|)
+};
+
+struct InjectPlanHost {
+  DevBuf cell_field, cell_index, start, src, wa, wb;
+  int n_cells = 0;
+  InjectPlanDev dev() const {
+    InjectPlanDev d{};
+    d.n_cells = n_cells;
+    d.cell_field = cell_field.as<int32_t>();
+    d.cell_index = cell_index.as<int32_t>();
+    d.start = start.as<int32_t>();
+    d.src = src.as<int32_t>();
+    d.wa = wa.as<double>();
+    d.wb = wb.as<double>();
+    return d;
+  }
+};
+
+struct Prop {
+  ertm_prop_config cfg{};
+  DevProp h{};
+  DevBuf d_desc;
+  cudaStream_t st = nullptr;
+  int M = 4;
+  int n_psi = 2;
+  size_t field_elems = 0, state_floats = 0;
+  DevBuf state, coefs, prof, qidx, relax, peak, stab;
+  int64_t step_index = 0;
+  int tiles_x = 0, tiles = 0;
+  int lowpass_steps = 0;
+  float k_src = 0.f;             // K_R at the source node (viscoacoustic)
+  std::vector<double> rx, rz;
+  std::map<int, std::unique_ptr<SamplePlanHost>> samples;
+  std::map<std::vector<int>, std::unique_ptr<InjectPlanHost>> injects;
+  std::vector<float> host_kr;    // K_R copy for the ε-injection weights (lazy)
+  // cuFFT for the compensated viscoacoustic low-pass
+  cufftHandle fwd_plan = 0, inv_plan = 0;
+  DevBuf fft_real, fft_spec;
+
+  ~Prop() {
+    if (fwd_plan) cufftDestroy(fwd_plan);
+    if (inv_plan) cufftDestroy(inv_plan);
+  }
+  DevProp* dp() const { return d_desc.as<DevProp>(); }
+  int n_fields() const { return h.n_fields; }
+  float* field(int slot) const { return h.f[slot]; }
+  void sync_desc() { upload(d_desc.p, &h, sizeof(DevProp), st); }
+};
+
+int field_slot(const Prop& P, int comp) {
+  // component → field slot for sampling/injection, −1 if absent
+  switch (P.h.engine) {
+    case ENGINE_ACOUSTIC:
+    case ENGINE_VISCO:
+      if (comp == ERTM_COMP_P) return A_P;
+      if (comp == ERTM_COMP_VX) return A_VX;
+      if (comp == ERTM_COMP_VZ) return A_VZ;
+      return -1;
+    default:
+      if (comp == ERTM_COMP_VX) return E_VX;
+      if (comp == ERTM_COMP_VZ) return E_VZ;
+      if (comp == ERTM_COMP_SXX) return E_SXX;
+      if (comp == ERTM_COMP_SZZ) return E_SZZ;
+      if (comp == ERTM_COMP_SXZ) return E_SXZ;
+      return -1;
+  }
+}
+
+void fractional(const Prop& P, double x, double z, double xo, double zo, double& xf, double& zf) {
+  // propagation.py:251-262
+  xf = (x - P.cfg.x0) / P.cfg.dx + (double)P.h.pad + xo;
+  zf = (z - P.cfg.z0) / P.cfg.dz + (double)P.h.pad + zo;
+}
+
+SamplePlanHost& sample_plan(Prop& P, int comp) {
+  auto it = P.samples.find(comp);
+  if (it != P.samples.end()) return *it->second;
+  auto sp = std::make_unique<SamplePlanHost>();
+  const int n = (int)P.rx.size();
+  sp->n = n;
+  if (P.h.engine == ENGINE_ELASTIC && comp == ERTM_COMP_P) {
+    sp->kind = SAMPLE_PRESSURE;  // ½(σxx+σzz) at the σxx node (propagation.py:891-893)
+  } else if (P.h.engine == ENGINE_ACOUSTIC && comp == ERTM_COMP_SXZ) {
+    sp->kind = SAMPLE_ZERO;      // propagation.py:464-466
+  } else {
+    sp->slot = field_slot(P, comp);
+    REQUIRE(sp->slot >= 0, "propagator has no component " + std::to_string(comp));
+  }
+  double xo, zo;
+  comp_offsets(sp->kind == SAMPLE_PRESSURE ? ERTM_COMP_SXX : comp, xo, zo);
+  std::vector<int32_t> cell(n);
+  std::vector<uint8_t> valid(n);
+  std::vector<double> w(4 * (size_t)n);
+  for (int r = 0; r < n; ++r) {
+    double xf, zf;
+    fractional(P, P.rx[r], P.rz[r], xo, zo, xf, zf);
+    const double z0 = std::floor(zf), x0 = std::floor(xf);
+    const double tz = zf - z0, tx = xf - x0;
+    const long long zi = (long long)z0, xi = (long long)x0;
+    valid[r] = (zi >= 0 && zi < P.h.nzp - 1 && xi >= 0 && xi < P.h.nxp - 1) ? 1 : 0;
+    const long long zc = std::min<long long>(std::max<long long>(zi, 0), P.h.nzp - 2);
+    const long long xc = std::min<long long>(std::max<long long>(xi, 0), P.h.nxp - 2);
+    cell[r] = (int32_t)(zc * P.h.ld + xc);
+    w[4 * r + 0] = 1 - tz;
+    w[4 * r + 1] = tz;
+    w[4 * r + 2] = 1 - tx;
+    w[4 * r + 3] = tx;
+  }
+  sp->cell = DevBuf(n * sizeof(int32_t), P.st);
+  sp->valid = DevBuf(n, P.st);
+  sp->w = DevBuf(w.size() * sizeof(double), P.st);
+  upload(sp->cell.p, cell.data(), n * sizeof(int32_t), P.st);
+  upload(sp->valid.p, valid.data(), n, P.st);
+  upload(sp->w.p, w.data(), w.size() * sizeof(double), P.st);
+  CK(cudaStreamSynchronize(P.st));  // host vectors go out of scope
+  auto& ref = *sp;
+  P.samples[comp] = std::move(sp);
+  return ref;
+}
+
+std::vector<InjectTarget> inject_targets(const Prop& P, int comp) {
+  // imaging.py:437-444 maps record names to these components; the per-engine
+  // field lists follow propagation.py:472-494, 764-774, 900-942.
+  std::vector<InjectTarget> t;
+  if (P.h.engine == ENGINE_ELASTIC) {
+    if (comp == ERTM_COMP_P) {
+      t.push_back({E_SXX, ERTM_COMP_SXX, 0});
+      t.push_back({E_SZZ, ERTM_COMP_SXX, 0});
+    } else {
+      const int s = field_slot(P, comp);
+      REQUIRE(s >= 0, "elastic propagator cannot inject component " + std::to_string(comp));
+      t.push_back({s, comp, 0});
+    }
+  } else if (P.h.engine == ENGINE_VISCO) {
+    const int s = field_slot(P, comp);
+    REQUIRE(s >= 0, "viscoacoustic propagator cannot inject component " + std::to_string(comp));
+    t.push_back({s, comp, 1});
+    if (comp == ERTM_COMP_P) t.push_back({V_EPS, comp, 2});
+  } else {
+    const int s = field_slot(P, comp);
+    REQUIRE(s >= 0, "acoustic propagator cannot inject component " + std::to_string(comp));
+    t.push_back({s, comp, 0});
+  }
+  return t;
+}
+
+// Build the contribution lists for injecting the record components `comps`
+// (record layout comps × nt × nrec).  Order inside a target cell follows the
+// reference: component, then target field, then corner (00, 01, 10, 11),
+// then receiver — np.add.at applies duplicates in index order.
+InjectPlanHost& inject_plan(Prop& P, const std::vector<int>& comps, int64_t nt) {
+  std::vector<int> key = comps;
+  key.push_back((int)nt);
+  auto it = P.injects.find(key);
+  if (it != P.injects.end()) return *it->second;
+  const int n = (int)P.rx.size();
+  struct Contrib { int32_t src; double wa, wb; };
+  std::map<std::pair<int, int64_t>, std::vector<Contrib>> cells;
+  std::vector<std::pair<int, int64_t>> order;
+  for (size_t ci = 0; ci < comps.size(); ++ci) {
+    for (const InjectTarget& tg : inject_targets(P, comps[ci])) {
+      if (tg.scaled == 2 && P.host_kr.empty()) {
+        P.host_kr.resize(P.field_elems);
+        CK(cudaMemcpyAsync(P.host_kr.data(), P.h.coef[CV_KR], P.field_elems * sizeof(float),
+                           cudaMemcpyDeviceToHost, P.st));
+        CK(cudaStreamSynchronize(P.st));
+      }
+      double xo, zo;
+      comp_offsets(tg.offset_comp, xo, zo);
+      std::vector<int64_t> zc(n), xc(n);
+      std::vector<double> tz(n), tx(n);
+      std::vector<char> ok(n);
+      for (int r = 0; r < n; ++r) {
+        double xf, zf;
+        fractional(P, P.rx[r], P.rz[r], xo, zo, xf, zf);
+        const double z0 = std::floor(zf), x0 = std::floor(xf);
+        tz[r] = zf - z0;
+        tx[r] = xf - x0;
+        const long long zi = (long long)z0, xi = (long long)x0;
+        ok[r] = (zi >= 0 && zi < P.h.nzp - 1 && xi >= 0 && xi < P.h.nxp - 1);
+        zc[r] = zi;
+        xc[r] = xi;
+      }
+      for (int corner = 0; corner < 4; ++corner) {
+        const int dz = corner >> 1, dx = corner & 1;
+        for (int r = 0; r < n; ++r) {
+          if (!ok[r]) continue;
+          const double wz = dz ? tz[r] : 1 - tz[r];
+          const double wx = dx ? tx[r] : 1 - tx[r];
+          Contrib c{(int32_t)(ci * nt * n + r), wz, wx};
+          if (tg.scaled) {
+            double fac = 1.0;  // np.float32(1.0)
+            if (tg.scaled == 2) {
+              const float kr = P.host_kr[(size_t)zc[r] * P.h.ld + xc[r]];
+              fac = (double)(1.0f / std::max(std::fabs(kr), 1e-20f));
+            }
+            c.wa = wz * wx * fac;
+            c.wb = 1.0;
+          }
+          const std::pair<int, int64_t> k{tg.slot, (zc[r] + dz) * P.h.ld + (xc[r] + dx)};
+          auto& v = cells[k];
+          if (v.empty()) order.push_back(k);
+          v.push_back(c);
+        }
+      }
+    }
+  }
+  std::vector<int32_t> cf, cidx, start{0}, src;
+  std::vector<double> wa, wb;
+  for (const auto& k : order) {
+    cf.push_back(k.first);
+    cidx.push_back((int32_t)k.second);
+    for (const Contrib& c : cells[k]) {
+      src.push_back(c.src);
+      wa.push_back(c.wa);
+      wb.push_back(c.wb);
+    }
+    start.push_back((int32_t)src.size());
+  }
+  auto ip = std::make_unique<InjectPlanHost>();
+  ip->n_cells = (int)cf.size();
+  auto put = [&](DevBuf& b, const void* data, size_t bytes) {
+    b = DevBuf(bytes, P.st);
+    upload(b.p, data, bytes, P.st);
+  };
+  put(ip->cell_field, cf.data(), cf.size() * 4);
+  put(ip->cell_index, cidx.data(), cidx.size() * 4);
+  put(ip->start, start.data(), start.size() * 4);
+  put(ip->src, src.data(), src.size() * 4);
+  put(ip->wa, wa.data(), wa.size() * 8);
+  put(ip->wb, wb.data(), wb.size() * 8);
+  CK(cudaStreamSynchronize(P.st));
+  auto& ref = *ip;
+  P.injects[key] = std::move(ip);
+  return ref;
+}
+
+// --------------------------------------------------------------------------
+// stepping
+// --------------------------------------------------------------------------
+template <int M>
+void launch_phases(const Prop& P, const WorkSet& ws, int blocks) {
+  const dim3 blk(TILE_X, BY);
+  switch (P.h.engine) {
+    case ENGINE_ACOUSTIC:
+      k_pressure_velocity<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      k_pressure_stress<M, TZ, BY, false><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      break;
+    case ENGINE_VISCO:
+      k_pressure_velocity<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      k_pressure_stress<M, TZ, BY, true><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      break;
+    default:
+      k_elastic_velocity<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      k_elastic_stress<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+  }
+}
+
+void lowpass_field(Prop& P, float* f, double cutoff) {
+  const int nz = P.h.nzp, nx = P.h.nxp;
+  if (!P.fwd_plan) {
+    CKFFT(cufftPlan2d(&P.fwd_plan, nz, nx, CUFFT_D2Z));
+    CKFFT(cufftPlan2d(&P.inv_plan, nz, nx, CUFFT_Z2D));
+    CKFFT(cufftSetStream(P.fwd_plan, P.st));
+    CKFFT(cufftSetStream(P.inv_plan, P.st));
+    P.fft_real = DevBuf((size_t)nz * nx * sizeof(double), P.st);
+    P.fft_spec = DevBuf((size_t)nz * (nx / 2 + 1) * sizeof(double2), P.st);
+  }
+  const dim3 b2(32, 8), g2((nx + 31) / 32, (nz + 7) / 8), gh((nx / 2 + 1 + 31) / 32, (nz + 7) / 8);
+  k_f32_to_f64<<<g2, b2, 0, P.st>>>(f, P.h.ld, P.fft_real.as<double>(), nz, nx);
+  CKFFT(cufftExecD2Z(P.fwd_plan, P.fft_real.as<double>(), P.fft_spec.as<cufftDoubleComplex>()));
+  k_lowpass_apply<<<gh, b2, 0, P.st>>>(P.fft_spec.as<double2>(), nz, nx, P.cfg.dz, P.cfg.dx, cutoff);
+  CKFFT(cufftExecZ2D(P.inv_plan, P.fft_spec.as<cufftDoubleComplex>(), P.fft_real.as<double>()));
+  k_f64_to_f32<<<g2, b2, 0, P.st>>>(P.fft_real.as<double>(), f, P.h.ld, nz, nx);
+}
+
+void step_once(Prop& P, double amp64) {
+  StepWork w{};
+  w.prop = 0;
+  w.tile0 = 0;
+  w.tiles_x = P.tiles_x;
+  w.tiles = P.tiles;
+  // `if source_amplitude != 0.0` on the float64 value, then float32 adds
+  const float amp = amp64 != 0.0 ? (float)amp64 : 0.f;
+  w.amp = amp;
+  if (P.h.engine == ENGINE_VISCO && amp64 != 0.0)
+    w.amp_eps = (float)(amp64 / (double)P.k_src);  // propagation.py:710-712
+  const bool comp = P.h.engine == ENGINE_VISCO && P.cfg.compensation;
+  w.flags = comp ? STEP_PEAK : 0;
+  WorkSet ws{nullptr, 0, w};
+  switch (P.M) {
+    case 1: launch_phases<1>(P, ws, P.tiles); break;
+    case 2: launch_phases<2>(P, ws, P.tiles); break;
+    case 3: launch_phases<3>(P, ws, P.tiles); break;
+    default: launch_phases<4>(P, ws, P.tiles); break;
+  }
+  if (P.h.engine == ENGINE_ELASTIC && P.h.mech == MECH_FORCE_Z && amp != 0.f && P.h.src_iz >= 0)
+    k_point_add<<<1, 32, 0, P.st>>>(P.field(E_VZ), (int64_t)P.h.src_iz * P.h.ld + P.h.src_ix, amp);
+  if (comp) {
+    // propagation.py:726-749, evaluated with the step index before the increment
+    const int64_t s = P.step_index;
+    if (s < 30) {
+      k_stab_reference<<<1, 32, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>());
+    } else {
+      k_stab_scale<<<296, 256, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>(), P.cfg.amplitude_cap);
+      const int every = P.cfg.lowpass_interval;
+      if (every > 1 && s % every == 0) {
+        ++P.lowpass_steps;
+        const double time = (double)s * P.cfg.dt;
+        const double ratio = std::max(0.9 - 0.4 * std::min(time / 1.0, 1.0), 0.35);
+        lowpass_field(P, P.field(V_P), ratio);
+        lowpass_field(P, P.field(V_EPS), ratio);
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  ++P.step_index;
+}
+
+void image_field(Prop& P, int wave, int sep, float* out) {
+  const dim3 b2(32, 8), g2((P.h.nx + 31) / 32, (P.h.nz + 7) / 8);
+  switch (P.M) {
+    case 1: k_image_field<1><<<g2, b2, 0, P.st>>>(P.dp(), 0, wave, sep, out); break;
+    case 2: k_image_field<2><<<g2, b2, 0, P.st>>>(P.dp(), 0, wave, sep, out); break;
+    case 3: k_image_field<3><<<g2, b2, 0, P.st>>>(P.dp(), 0, wave, sep, out); break;
+    default: k_image_field<4><<<g2, b2, 0, P.st>>>(P.dp(), 0, wave, sep, out); break;
+  }
+}
+
+Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, const float* rho,
+             const float* ax, const float* bx, const float* az, const float* bz, const uint8_t* qidx,
+             const double* tau, const double* delta, const double* mref, const float* relax_a, void* stream) {
+  REQUIRE(cfg, "null config");
+  REQUIRE(cfg->order == 2 || cfg->order == 4 || cfg->order == 6 || cfg->order == 8, "order must be 2/4/6/8");
+  REQUIRE(cfg->nx >= 2 && cfg->nz >= 2, "grid must be at least 2x2");
+  REQUIRE(cfg->engine >= 0 && cfg->engine <= 2, "unknown engine");
+  REQUIRE(vp && rho && ax && bx && az && bz, "null material or profile array");
+  auto P = std::make_unique<Prop>();
+  P->cfg = *cfg;
+  P->st = static_cast<cudaStream_t>(stream);
+  DevProp& h = P->h;
+  h.engine = cfg->engine;
+  h.M = cfg->order / 2;
+  P->M = h.M;
+  h.pad = h.M + 1;
+  h.nz = cfg->nz;
+  h.nx = cfg->nx;
+  h.nzp = cfg->nz + 2 * h.pad;
+  h.nxp = cfg->nx + 2 * h.pad;
+  REQUIRE(h.nzp > 2 * h.M && h.nxp > 2 * h.M, "grid too small for the stencil");
+  h.ld = (h.nxp + 31) / 32 * 32;
+  static const double C8[4][4] = {{1.0, 0, 0, 0},
+                                  {9.0 / 8.0, -1.0 / 24.0, 0, 0},
+                                  {75.0 / 64.0, -25.0 / 384.0, 3.0 / 640.0, 0},
+                                  {1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0}};
+  for (int k = 0; k < 4; ++k) h.c[k] = (float)C8[h.M - 1][k];
+  h.hx = (float)cfg->dx;
+  h.hz = (float)cfg->dz;
+  h.dt = (float)cfg->dt;
+  h.npx_l = cfg->npml_x_left;
+  h.npx_r = cfg->npml_x_right;
+  h.npz_t = cfg->npml_z_top;
+  h.npz_b = cfg->npml_z_bottom;
+  REQUIRE(h.npx_l >= 0 && h.npx_r >= 0 && h.npx_l + h.npx_r <= h.nxp, "bad x strips");
+  REQUIRE(h.npz_t >= 0 && h.npz_b >= 0 && h.npz_t + h.npz_b <= h.nzp, "bad z strips");
+  h.wx = h.npx_l + h.npx_r;
+  h.hz_rows = h.npz_t + h.npz_b;
+  h.free_surface = (cfg->free_surface && h.engine != ENGINE_VISCO) ? 1 : 0;
+  h.src_iz = h.src_ix = -1;
+  h.L = h.engine == ENGINE_VISCO ? cfg->n_mech : 0;
+  if (h.engine == ENGINE_VISCO) {
+    REQUIRE(h.L >= 1 && h.L <= MAX_MECH, "n_mech must be 1..8");
+    REQUIRE(cfg->n_q >= 1 && cfg->n_q <= 255, "n_q must be 1..255");
+    REQUIRE(qidx && tau && delta && mref && relax_a, "viscoacoustic tables missing");
+  }
+  if (h.engine == ENGINE_ELASTIC) REQUIRE(vs, "elastic needs vs");
+  h.n_fields = h.engine == ENGINE_ACOUSTIC ? 3 : (h.engine == ENGINE_ELASTIC ? 5 : 4 + h.L);
+  P->n_psi = h.engine == ENGINE_ELASTIC ? 4 : 2;
+  const int n_coef = h.engine == ENGINE_ACOUSTIC ? 3 : (h.engine == ENGINE_ELASTIC ? 5 : 3 + h.L);
+  P->field_elems = (size_t)h.nzp * h.ld;
+  const size_t fe = round64(P->field_elems);
+  const size_t px = round64((size_t)h.nzp * h.wx), pz = round64((size_t)h.hz_rows * h.ld);
+  P->state_floats = fe * h.n_fields + P->n_psi * (px + pz);
+  P->state = DevBuf(P->state_floats * 4, P->st);
+  CK(cudaMemsetAsync(P->state.p, 0, P->state_floats * 4, P->st));
+  float* s = P->state.as<float>();
+  for (int f = 0; f < h.n_fields; ++f) h.f[f] = s + f * fe;
+  for (int t = 0; t < P->n_psi; ++t) {
+    h.psix[t] = s + fe * h.n_fields + t * px;
+    h.psiz[t] = s + fe * h.n_fields + P->n_psi * px + t * pz;
+  }
+  P->coefs = DevBuf(fe * n_coef * 4, P->st);
+  CK(cudaMemsetAsync(P->coefs.p, 0, fe * n_coef * 4, P->st));
+  for (int c = 0; c < n_coef; ++c) h.coef[c] = P->coefs.as<float>() + c * fe;
+  P->prof = DevBuf((2 * (size_t)h.nxp + 2 * (size_t)h.nzp) * 4, P->st);
+  float* pr = P->prof.as<float>();
+  upload(pr, ax, h.nxp * 4, P->st);
+  upload(pr + h.nxp, bx, h.nxp * 4, P->st);
+  upload(pr + 2 * h.nxp, az, h.nzp * 4, P->st);
+  upload(pr + 2 * h.nxp + h.nzp, bz, h.nzp * 4, P->st);
+  h.ax = pr;
+  h.bx = pr + h.nxp;
+  h.az = pr + 2 * h.nxp;
+  h.bz = pr + 2 * h.nxp + h.nzp;
+  P->peak = DevBuf(64, P->st);
+  CK(cudaMemsetAsync(P->peak.p, 0, 64, P->st));
+  h.peak = P->peak.as<float>();
+  P->stab = DevBuf(sizeof(StabState), P->st);
+  CK(cudaMemsetAsync(P->stab.p, 0, sizeof(StabState), P->st));
+  DevBuf tables;
+  if (h.engine == ENGINE_VISCO) {
+    // per-cell Q index on the padded grid (host layout nzp × nxp → pitch ld)
+    P->qidx = DevBuf(P->field_elems, P->st);
+    CK(cudaMemsetAsync(P->qidx.p, 0, P->field_elems, P->st));
+    CK(cudaMemcpy2DAsync(P->qidx.p, h.ld, qidx, h.nxp, h.nxp, h.nzp, cudaMemcpyDefault, P->st));
+    h.qidx = P->qidx.as<uint8_t>();
+    const size_t nqL = (size_t)cfg->n_q * h.L;
+    P->relax = DevBuf(nqL * 4, P->st);
+    upload(P->relax.p, relax_a, nqL * 4, P->st);
+    h.relax_a = P->relax.as<float>();
+    tables = DevBuf((2 * nqL + cfg->n_q) * 8, P->st);
+    upload(tables.as<double>(), tau, nqL * 8, P->st);
+    upload(tables.as<double>() + nqL, delta, nqL * 8, P->st);
+    upload(tables.as<double>() + 2 * nqL, mref, cfg->n_q * 8, P->st);
+  }
+  // physical materials → device
+  const size_t nphys = (size_t)cfg->nz * cfg->nx;
+  DevBuf mat(nphys * 3 * 4, P->st);
+  upload(mat.as<float>(), vp, nphys * 4, P->st);
+  upload(mat.as<float>() + nphys, rho, nphys * 4, P->st);
+  if (vs) upload(mat.as<float>() + 2 * nphys, vs, nphys * 4, P->st);
+  P->d_desc = DevBuf(sizeof(DevProp), P->st);
+  P->sync_desc();
+  SetupArgs A{};
+  A.vp = mat.as<float>();
+  A.rho = mat.as<float>() + nphys;
+  A.vs = mat.as<float>() + 2 * nphys;
+  if (h.engine == ENGINE_VISCO) {
+    const size_t nqL = (size_t)cfg->n_q * h.L;
+    A.tau = tables.as<double>();
+    A.delta = tables.as<double>() + nqL;
+    A.mref = tables.as<double>() + 2 * nqL;
+    A.relax_a = h.relax_a;
+  }
+  A.dt = cfg->dt;
+  const dim3 b2(32, 8), g2((h.nxp + 31) / 32, (h.nzp + 7) / 8);
+  k_setup_materials<<<g2, b2, 0, P->st>>>(P->dp(), 0, A);
+  CK(cudaGetLastError());
+  P->tiles_x = (h.nxp + TILE_X - 1) / TILE_X;
+  P->tiles = P->tiles_x * ((h.nzp + TZ - 1) / TZ);
+  CK(cudaStreamSynchronize(P->st));  // materials/tables staging buffers are freed next
+  return P.release();
+}
+
+// --------------------------------------------------------------------------
+// migrate
+// --------------------------------------------------------------------------
+template <int M>
+void launch_imaging(const Prop& B, const ImagingArgs& A, bool kahan) {
+  const dim3 b2(32, 8), g2((B.h.nx + 31) / 32, (B.h.nz + 7) / 8);
+  if (kahan) k_imaging<M, true><<<g2, b2, 0, B.st>>>(B.dp(), 0, A);
+  else k_imaging<M, false><<<g2, b2, 0, B.st>>>(B.dp(), 0, A);
+}
+
+template <int M>
+void launch_excitation_track(const Prop& F, int sep, float* running, int32_t* peak_step, int t) {
+  const dim3 b2(32, 8), g2((F.h.nx + 31) / 32, (F.h.nz + 7) / 8);
+  k_excitation_track<M><<<g2, b2, 0, F.st>>>(F.dp(), 0, sep, running, peak_step, t);
+}
+
+template <int M>
+void launch_excitation_image(const Prop& B, int sep, int n_images, const int32_t* rcv, const float* running,
+                             const int32_t* peak_step, int t, const Accum* num, const Accum* ril) {
+  const dim3 b2(32, 8), g2((B.h.nx + 31) / 32, (B.h.nz + 7) / 8);
+  k_excitation_image<M><<<g2, b2, 0, B.st>>>(B.dp(), 0, sep, n_images, rcv, running, peak_step, t, num[0],
+                                             num[n_images > 1 ? 1 : 0], ril[0], ril[n_images > 1 ? 1 : 0]);
+}
+
+__global__ void k_kahan_to_f64(const float* s, const float* c, double* out, int64_t n) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = (double)s[k] - (double)c[k];
+}
+
+void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wavelet, const float* record,
+             double* num_out, double* illum_out, double* rillum_out) {
+  REQUIRE(F.h.engine == B.h.engine && F.h.nz == B.h.nz && F.h.nx == B.h.nx, "fwd/back mismatch");
+  REQUIRE(cfg.nt >= 1 && cfg.interval >= 1 && cfg.nt_spec >= 1, "bad nt/interval");
+  REQUIRE(cfg.n_images >= 1 && cfg.n_images <= MAX_IMAGES, "n_images must be 1..4");
+  REQUIRE(cfg.n_comp >= 0 && cfg.n_comp <= 8, "n_comp must be 0..8");
+  REQUIRE(!B.rx.empty() || cfg.n_comp == 0, "receivers must be set on the backward propagator");
+  const bool excitation = cfg.condition == ERTM_COND_EXCITATION;
+  REQUIRE(!excitation || cfg.n_images <= 2, "excitation supports at most 2 images");
+  cudaStream_t st = F.st;
+  if (B.st != st) {
+    // keep the two propagators ordered on the forward stream
+    CK(cudaStreamSynchronize(B.st));
+    B.st = st;
+  }
+  const int nt = cfg.nt, iv = cfg.interval;
+  const int n_states = (nt + iv - 1) / iv;
+  const size_t npix = (size_t)F.h.nz * F.h.nx;
+  const int nimg = cfg.n_images;
+  const bool kahan = cfg.accum == ERTM_ACCUM_KAHAN && !excitation;
+  // accumulators
+  DevBuf acc(npix * nimg * 3 * 8, st);
+  CK(cudaMemsetAsync(acc.p, 0, acc.bytes, st));
+  Accum num[MAX_IMAGES]{}, ill[MAX_IMAGES]{}, ril[MAX_IMAGES]{};
+  for (int k = 0; k < nimg; ++k) {
+    double* base = acc.as<double>() + (size_t)k * 3 * npix;
+    num[k].d = base;
+    ill[k].d = base + npix;
+    ril[k].d = base + 2 * npix;
+    if (kahan) {
+      // same 8 bytes per cell: (sum, compensation) float pairs
+      for (Accum* a : {&num[k], &ill[k], &ril[k]}) {
+        a->s = reinterpret_cast<float*>(a->d);
+        a->comp = a->s + npix;
+      }
+    }
+  }
+  // record + injection plan on the backward propagator
+  std::vector<int> comps(cfg.comp, cfg.comp + cfg.n_comp);
+  const int64_t nrec = (int64_t)B.rx.size();
+  DevBuf rec((size_t)cfg.n_comp * cfg.nt_spec * nrec * 4, st);
+  upload(rec.p, record, rec.bytes, st);
+  InjectPlanHost* plan = comps.empty() ? nullptr : &inject_plan(B, comps, cfg.nt_spec);
+  auto inject = [&](int t) {
+    if (!plan || plan->n_cells == 0) return;
+    k_inject<<<(plan->n_cells + 127) / 128, 128, 0, st>>>(B.dp(), 0, plan->dev(), rec.as<float>(),
+                                                          (int64_t)t * nrec);
+  };
+  // forward with checkpoints (imaging.py:113-137)
+  DevBuf ck((size_t)n_states * F.state_floats * 4, st);
+  std::vector<int64_t> ck_step(n_states);
+  for (int t = 0; t < nt; ++t) {
+    step_once(F, (double)wavelet[t]);
+    if (t % iv == 0) {
+      CK(cudaMemcpyAsync(ck.as<float>() + (size_t)(t / iv) * F.state_floats, F.state.p, F.state_floats * 4,
+                         cudaMemcpyDeviceToDevice, st));
+      ck_step[t / iv] = F.step_index;
+    }
+  }
+  auto restore = [&](int b) {
+    CK(cudaMemcpyAsync(F.state.p, ck.as<float>() + (size_t)b * F.state_floats, F.state_floats * 4,
+                       cudaMemcpyDeviceToDevice, st));
+    F.step_index = ck_step[b];
+  };
+  const int M = F.M;
+  if (!excitation) {
+    bool need[2] = {false, false};
+    for (int k = 0; k < nimg; ++k) need[cfg.src_wave[k]] = true;
+    DevBuf rbuf((size_t)iv * 2 * npix * 4, st);
+    ImagingArgs A{};
+    A.n_images = nimg;
+    A.illum = cfg.illumination;
+    A.sep = cfg.separation;
+    for (int k = 0; k < nimg; ++k) {
+      A.src_wave[k] = cfg.src_wave[k];
+      A.rcv_wave[k] = cfg.rcv_wave[k];
+      A.num[k] = num[k];
+      A.illum_acc[k] = ill[k];
+      A.rillum_acc[k] = ril[k];
+    }
+    for (int b = n_states - 1; b >= 0; --b) {
+      const int s0 = b * iv, e0 = std::min((b + 1) * iv, nt);
+      restore(b);
+      for (int t = s0; t < e0; ++t) {
+        step_once(F, (double)wavelet[t]);
+        float* slot = rbuf.as<float>() + (size_t)(t - s0) * 2 * npix;
+        for (int w = 0; w < 2; ++w)
+          if (need[w]) image_field(F, w, cfg.separation, slot + w * npix);
+      }
+      for (int t = e0 - 1; t >= s0; --t) {
+        inject(t);
+        step_once(B, 0.0);
+        const float* slot = rbuf.as<float>() + (size_t)(t - s0) * 2 * npix;
+        A.src[0] = slot;
+        A.src[1] = slot + npix;
+        A.cross = t >= cfg.start_step ? 1 : 0;
+        if (!A.cross && !A.illum) continue;
+        switch (M) {
+          case 1: launch_imaging<1>(B, A, kahan); break;
+          case 2: launch_imaging<2>(B, A, kahan); break;
+          case 3: launch_imaging<3>(B, A, kahan); break;
+          default: launch_imaging<4>(B, A, kahan); break;
+        }
+      }
+    }
+  } else {
+    DevBuf running(npix * 4, st), peak((size_t)npix * 4, st), rcvw(16, st);
+    CK(cudaMemsetAsync(running.p, 0, npix * 4, st));
+    CK(cudaMemsetAsync(peak.p, 0xff, npix * 4, st));  // −1
+    upload(rcvw.p, cfg.rcv_wave, sizeof(int32_t) * 4, st);
+    for (int b = 0; b < n_states; ++b) {
+      const int s0 = b * iv, e0 = std::min((b + 1) * iv, nt);
+      restore(b);
+      for (int t = s0; t < e0; ++t) {
+        step_once(F, (double)wavelet[t]);
+        switch (M) {
+          case 1: launch_excitation_track<1>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
+          case 2: launch_excitation_track<2>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
+          case 3: launch_excitation_track<3>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
+          default: launch_excitation_track<4>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
+        }
+      }
+    }
+    for (int b = n_states - 1; b >= 0; --b) {
+      const int s0 = b * iv, e0 = (b + 1 < n_states) ? (b + 1) * iv : cfg.nt_spec;
+      for (int t = e0 - 1; t >= s0; --t) {
+        inject(t);
+        step_once(B, 0.0);
+        if (t < cfg.start_step) continue;
+        switch (M) {
+          case 1: launch_excitation_image<1>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
+          case 2: launch_excitation_image<2>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
+          case 3: launch_excitation_image<3>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
+          default: launch_excitation_image<4>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
+        }
+      }
+    }
+    // illumination = A² is computed but never used by this condition (imaging.py:304, 328)
+  }
+  CK(cudaGetLastError());
+  // outputs: per image, num/illum/rillum as float64
+  DevBuf tmp(kahan ? npix * 8 : 0, st);
+  for (int k = 0; k < nimg; ++k) {
+    double* outs[3] = {num_out, illum_out, rillum_out};
+    Accum* srcs[3] = {&num[k], &ill[k], &ril[k]};
+    for (int q = 0; q < 3; ++q) {
+      if (!outs[q]) continue;
+      const double* from = srcs[q]->d;
+      if (kahan) {
+        k_kahan_to_f64<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(srcs[q]->s, srcs[q]->comp, tmp.as<double>(),
+                                                                    (int64_t)npix);
+        from = tmp.as<double>();
+      }
+      CK(cudaMemcpyAsync(outs[q] + (size_t)k * npix, from, npix * 8, cudaMemcpyDefault, st));
+    }
+  }
+  CK(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+const char* ertm_last_error(void) { return g_error.c_str(); }
+
+int32_t ertm_version(void) { return 1; }
+
+int32_t ertm_init(int32_t device) {
+  return guarded([&] {
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    REQUIRE(device >= 0 && device < n, "no such CUDA device");
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    CK(cudaGetDeviceProperties(&prop, device));
+    REQUIRE(prop.major == 10, "this library is built for sm_100a (B200); found sm_" +
+                                  std::to_string(prop.major) + std::to_string(prop.minor));
+  });
+}
+
+void* ertm_prop_create(const ertm_prop_config* cfg, const float* vp, const float* vs, const float* rho,
+                       const float* pml_ax, const float* pml_bx, const float* pml_az, const float* pml_bz,
+                       const uint8_t* qidx, const double* tau, const double* delta, const double* mref,
+                       const float* relax_a, void* stream) {
+  Prop* out = nullptr;
+  int rc = guarded([&] { out = create(cfg, vp, vs, rho, pml_ax, pml_bx, pml_az, pml_bz, qidx, tau, delta, mref,
+                                      relax_a, stream); });
+  return rc == ERTM_OK ? out : nullptr;
+}
+
+void ertm_prop_destroy(void* prop) {
+  if (!prop) return;
+  Prop* P = static_cast<Prop*>(prop);
+  cudaStreamSynchronize(P->st);
+  delete P;
+}
+
+int32_t ertm_prop_info_get(void* prop, ertm_prop_info* info) {
+  return guarded([&] {
+    REQUIRE(prop && info, "null argument");
+    Prop& P = *static_cast<Prop*>(prop);
+    info->nzp = P.h.nzp;
+    info->nxp = P.h.nxp;
+    info->ld = P.h.ld;
+    info->pad = P.h.pad;
+    info->state_bytes = (int64_t)P.state_floats * 4;
+    info->field_bytes = (int64_t)P.h.n_fields * P.h.nzp * P.h.nxp * 4;
+    info->step_index = P.step_index;
+    info->n_fields = P.h.n_fields;
+    StabState s{};
+    CK(cudaMemcpyAsync(&s, P.stab.p, sizeof(s), cudaMemcpyDeviceToHost, P.st));
+    CK(cudaStreamSynchronize(P.st));
+    info->clipped = s.clipped;
+    info->lowpass_steps = P.lowpass_steps;
+    info->n_receivers = (int32_t)P.rx.size();
+  });
+}
+
+int32_t ertm_prop_reset(void* prop) {
+  return guarded([&] {
+    REQUIRE(prop, "null propagator");
+    Prop& P = *static_cast<Prop*>(prop);
+    CK(cudaMemsetAsync(P.state.p, 0, P.state_floats * 4, P.st));
+    CK(cudaMemsetAsync(P.stab.p, 0, sizeof(StabState), P.st));
+    P.step_index = 0;
+    P.lowpass_steps = 0;
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_set_source(void* prop, int32_t iz, int32_t ix, int32_t mechanism) {
+  return guarded([&] {
+    REQUIRE(prop, "null propagator");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(iz >= 0 && iz < P.h.nzp && ix >= 0 && ix < P.h.nxp, "source node outside the padded grid");
+    REQUIRE(mechanism >= 0 && mechanism <= 2, "unknown mechanism");
+    P.h.src_iz = iz;
+    P.h.src_ix = ix;
+    P.h.mech = mechanism;
+    if (P.h.engine == ENGINE_VISCO) {
+      CK(cudaMemcpyAsync(&P.k_src, P.h.coef[CV_KR] + (size_t)iz * P.h.ld + ix, 4, cudaMemcpyDeviceToHost, P.st));
+    }
+    P.sync_desc();
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_set_receivers(void* prop, int32_t n, const double* x, const double* z) {
+  return guarded([&] {
+    REQUIRE(prop && n >= 0 && (n == 0 || (x && z)), "bad receivers");
+    Prop& P = *static_cast<Prop*>(prop);
+    P.rx.assign(x, x + n);
+    P.rz.assign(z, z + n);
+    P.samples.clear();
+    P.injects.clear();
+  });
+}
+
+int32_t ertm_prop_step(void* prop, int32_t n_steps, const double* amps) {
+  return guarded([&] {
+    REQUIRE(prop && n_steps >= 0, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    for (int t = 0; t < n_steps; ++t) step_once(P, amps ? amps[t] : 0.0);
+  });
+}
+
+int32_t ertm_prop_sample(void* prop, int32_t n_comp, const int32_t* comps, float* out) {
+  return guarded([&] {
+    REQUIRE(prop && n_comp >= 0 && (n_comp == 0 || comps), "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    const int n = (int)P.rx.size();
+    if (n == 0 || n_comp == 0) return;
+    DevBuf o((size_t)n_comp * n * 4, P.st);
+    for (int c = 0; c < n_comp; ++c) {
+      SamplePlanHost& sp = sample_plan(P, comps[c]);
+      SampleSet S{};
+      S.count = 1;
+      S.plan[0] = SamplePlanDev{n, sp.kind, sp.slot, 0, sp.cell.as<int32_t>(), sp.valid.as<uint8_t>(),
+                                sp.w.as<double>(), o.as<float>() + (size_t)c * n};
+      k_sample<<<dim3((n + 127) / 128, 1), 128, 0, P.st>>>(P.dp(), 0, S, 0);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, o.p, o.bytes, cudaMemcpyDefault, P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_inject(void* prop, int32_t comp, const float* values) {
+  return guarded([&] {
+    REQUIRE(prop && values, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(!P.rx.empty(), "receivers must be set before injection");
+    const int n = (int)P.rx.size();
+    InjectPlanHost& plan = inject_plan(P, std::vector<int>{comp}, 1);
+    DevBuf v((size_t)n * 4, P.st);
+    upload(v.p, values, v.bytes, P.st);
+    if (plan.n_cells)
+      k_inject<<<(plan.n_cells + 127) / 128, 128, 0, P.st>>>(P.dp(), 0, plan.dev(), v.as<float>(), 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_image_field(void* prop, int32_t wave, int32_t separation, float* out) {
+  return guarded([&] {
+    REQUIRE(prop && out, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(wave == 0 || (wave == 1 && P.h.engine == ENGINE_ELASTIC), "wave not available for this engine");
+    DevBuf o((size_t)P.h.nz * P.h.nx * 4, P.st);
+    image_field(P, wave, separation, o.as<float>());
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, o.p, o.bytes, cudaMemcpyDefault, P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_read_field(void* prop, int32_t slot, float* out) {
+  return guarded([&] {
+    REQUIRE(prop && out, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(slot >= 0 && slot < P.h.n_fields, "bad field slot");
+    CK(cudaMemcpy2DAsync(out, P.h.nxp * 4, P.field(slot), P.h.ld * 4, P.h.nxp * 4, P.h.nzp, cudaMemcpyDefault,
+                         P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_write_field(void* prop, int32_t slot, const float* in) {
+  return guarded([&] {
+    REQUIRE(prop && in, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(slot >= 0 && slot < P.h.n_fields, "bad field slot");
+    CK(cudaMemcpy2DAsync(P.field(slot), P.h.ld * 4, in, P.h.nxp * 4, P.h.nxp * 4, P.h.nzp, cudaMemcpyDefault,
+                         P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+// ψ terms are stored as strips; these expand to / extract from full padded arrays.
+int32_t ertm_prop_read_psi(void* prop, int32_t axis, int32_t term, float* out) {
+  return guarded([&] {
+    REQUIRE(prop && out, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(term >= 0 && term < P.n_psi && (axis == 0 || axis == 1), "bad psi term");
+    const int nzp = P.h.nzp, nxp = P.h.nxp;
+    std::vector<float> full((size_t)nzp * nxp, 0.f);
+    if (axis == 1 && P.h.wx > 0) {
+      std::vector<float> s((size_t)nzp * P.h.wx);
+      CK(cudaMemcpyAsync(s.data(), P.h.psix[term], s.size() * 4, cudaMemcpyDeviceToHost, P.st));
+      CK(cudaStreamSynchronize(P.st));
+      for (int i = 0; i < nzp; ++i)
+        for (int c = 0; c < P.h.wx; ++c) {
+          const int j = c < P.h.npx_l ? c : nxp - P.h.npx_r + (c - P.h.npx_l);
+          full[(size_t)i * nxp + j] = s[(size_t)i * P.h.wx + c];
+        }
+    }
+    if (axis == 0 && P.h.hz_rows > 0) {
+      std::vector<float> s((size_t)P.h.hz_rows * P.h.ld);
+      CK(cudaMemcpyAsync(s.data(), P.h.psiz[term], s.size() * 4, cudaMemcpyDeviceToHost, P.st));
+      CK(cudaStreamSynchronize(P.st));
+      for (int r = 0; r < P.h.hz_rows; ++r) {
+        const int i = r < P.h.npz_t ? r : nzp - P.h.npz_b + (r - P.h.npz_t);
+        std::memcpy(&full[(size_t)i * nxp], &s[(size_t)r * P.h.ld], nxp * 4);
+      }
+    }
+    CK(cudaMemcpy(out, full.data(), full.size() * 4, cudaMemcpyDefault));
+  });
+}
+
+int32_t ertm_prop_write_psi(void* prop, int32_t axis, int32_t term, const float* in) {
+  return guarded([&] {
+    REQUIRE(prop && in, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    REQUIRE(term >= 0 && term < P.n_psi && (axis == 0 || axis == 1), "bad psi term");
+    const int nzp = P.h.nzp, nxp = P.h.nxp;
+    std::vector<float> full((size_t)nzp * nxp);
+    CK(cudaMemcpy(full.data(), in, full.size() * 4, cudaMemcpyDefault));
+    if (axis == 1 && P.h.wx > 0) {
+      std::vector<float> s((size_t)nzp * P.h.wx);
+      for (int i = 0; i < nzp; ++i)
+        for (int c = 0; c < P.h.wx; ++c) {
+          const int j = c < P.h.npx_l ? c : nxp - P.h.npx_r + (c - P.h.npx_l);
+          s[(size_t)i * P.h.wx + c] = full[(size_t)i * nxp + j];
+        }
+      CK(cudaMemcpyAsync(P.h.psix[term], s.data(), s.size() * 4, cudaMemcpyHostToDevice, P.st));
+      CK(cudaStreamSynchronize(P.st));
+    }
+    if (axis == 0 && P.h.hz_rows > 0) {
+      std::vector<float> s((size_t)P.h.hz_rows * P.h.ld, 0.f);
+      for (int r = 0; r < P.h.hz_rows; ++r) {
+        const int i = r < P.h.npz_t ? r : nzp - P.h.npz_b + (r - P.h.npz_t);
+        std::memcpy(&s[(size_t)r * P.h.ld], &full[(size_t)i * nxp], nxp * 4);
+      }
+      CK(cudaMemcpyAsync(P.h.psiz[term], s.data(), s.size() * 4, cudaMemcpyHostToDevice, P.st));
+      CK(cudaStreamSynchronize(P.st));
+    }
+  });
+}
+
+int32_t ertm_prop_set_step_index(void* prop, int64_t step_index) {
+  return guarded([&] {
+    REQUIRE(prop && step_index >= 0, "bad arguments");
+    static_cast<Prop*>(prop)->step_index = step_index;
+  });
+}
+
+int32_t ertm_prop_save_state(void* prop, void* dst) {
+  return guarded([&] {
+    REQUIRE(prop && dst, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    CK(cudaMemcpyAsync(dst, P.state.p, P.state_floats * 4, cudaMemcpyDefault, P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_prop_load_state(void* prop, const void* src) {
+  return guarded([&] {
+    REQUIRE(prop && src, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    CK(cudaMemcpyAsync(P.state.p, src, P.state_floats * 4, cudaMemcpyDefault, P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_forward(void* prop, int32_t nt, const float* amps, int32_t n_comp, const int32_t* comps, float* out) {
+  return guarded([&] {
+    REQUIRE(prop && nt >= 0 && n_comp >= 0 && n_comp <= MAX_SAMPLE, "bad arguments");
+    Prop& P = *static_cast<Prop*>(prop);
+    const int n = (int)P.rx.size();
+    const bool sampling = n > 0 && n_comp > 0;
+    DevBuf o(sampling ? (size_t)n_comp * nt * n * 4 : 0, P.st);
+    SampleSet S{};
+    if (sampling) {
+      S.count = n_comp;
+      for (int c = 0; c < n_comp; ++c) {
+        SamplePlanHost& sp = sample_plan(P, comps[c]);
+        S.plan[c] = SamplePlanDev{n, sp.kind, sp.slot, 0, sp.cell.as<int32_t>(), sp.valid.as<uint8_t>(),
+                                  sp.w.as<double>(), o.as<float>() + (size_t)c * nt * n};
+      }
+    }
+    for (int t = 0; t < nt; ++t) {
+      step_once(P, amps ? (double)amps[t] : 0.0);
+      if (sampling) k_sample<<<dim3((n + 127) / 128, n_comp), 128, 0, P.st>>>(P.dp(), 0, S, (int64_t)t * n);
+    }
+    CK(cudaGetLastError());
+    if (sampling) CK(cudaMemcpyAsync(out, o.p, o.bytes, cudaMemcpyDefault, P.st));
+    CK(cudaStreamSynchronize(P.st));
+  });
+}
+
+int32_t ertm_migrate(void* fwd, void* back, const ertm_migrate_config* cfg, const float* wavelet,
+                     const float* record, double* num, double* illum, double* rillum) {
+  return guarded([&] {
+    REQUIRE(fwd && back && cfg && wavelet, "bad arguments");
+    REQUIRE(cfg->n_comp == 0 || record, "record missing");
+    migrate(*static_cast<Prop*>(fwd), *static_cast<Prop*>(back), *cfg, wavelet, record, num, illum, rillum);
+  });
+}
+
+int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const double* num, const double* illum,
+                         const double* rillum, int32_t by_illum, int32_t by_rillum, double eps, int32_t laplacian,
+                         double lowpass, int32_t npml, int32_t top_mask, float* out, void* stream) {
+  return guarded([&] {
+    REQUIRE(nz >= 1 && nx >= 1 && num && out, "bad arguments");
+    REQUIRE(!by_illum || illum, "illumination missing");
+    REQUIRE(!by_rillum || rillum, "receiver illumination missing");
+    REQUIRE(lowpass > 0.0 && lowpass <= 1.0, "lowpass fraction must lie in (0, 1]");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = (int64_t)nz * nx;
+    DevBuf in(n * 8 * 3, st), a(n * 8, st), b(n * 8, st), o(n * 4, st);
+    double* dn = in.as<double>();
+    upload(dn, num, n * 8, st);
+    if (by_illum) upload(dn + n, illum, n * 8, st);
+    if (by_rillum) upload(dn + 2 * n, rillum, n * 8, st);
+    NormArgs A{};
+    A.num = dn;
+    A.illum = dn + n;
+    A.rillum = dn + 2 * n;
+    A.by_illum = by_illum;
+    A.by_rillum = by_rillum;
+    A.eps = eps;
+    A.out = a.as<double>();
+    A.n = n;
+    k_normalize<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A);
+    const dim3 b2(32, 8), g2((nx + 31) / 32, (nz + 7) / 8);
+    double* cur = a.as<double>();
+    double* other = b.as<double>();
+    if (laplacian) {
+      k_laplacian<<<g2, b2, 0, st>>>(cur, other, nz, nx, dx, dz);
+      std::swap(cur, other);
+    }
+    cufftHandle pf = 0, pi = 0;
+    if (lowpass < 1.0) {
+      DevBuf spec((size_t)nz * (nx / 2 + 1) * 16, st);
+      CKFFT(cufftPlan2d(&pf, nz, nx, CUFFT_D2Z));
+      CKFFT(cufftPlan2d(&pi, nz, nx, CUFFT_Z2D));
+      CKFFT(cufftSetStream(pf, st));
+      CKFFT(cufftSetStream(pi, st));
+      CKFFT(cufftExecD2Z(pf, cur, spec.as<cufftDoubleComplex>()));
+      const dim3 gh((nx / 2 + 1 + 31) / 32, (nz + 7) / 8);
+      k_lowpass_apply<<<gh, b2, 0, st>>>(spec.as<double2>(), nz, nx, dz, dx, lowpass);
+      CKFFT(cufftExecZ2D(pi, spec.as<cufftDoubleComplex>(), other));
+      std::swap(cur, other);
+      CK(cudaStreamSynchronize(st));
+      cufftDestroy(pf);
+      cufftDestroy(pi);
+    }
+    k_mask_cast<<<g2, b2, 0, st>>>(cur, o.as<float>(), nz, nx, npml, top_mask);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
+                   void* stream) {
+  return guarded([&] {
+    REQUIRE(n_images >= 1 && n >= 1 && images && out, "bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n_images == 1) {
+      CK(cudaMemcpyAsync(out, images[0], n * 4, cudaMemcpyDefault, st));
+      CK(cudaStreamSynchronize(st));
+      return;
+    }
+    DevBuf acc(n * 8, st), img(n * 4, st), o(n * 4, st), sc(4, st);
+    CK(cudaMemsetAsync(acc.p, 0, n * 8, st));
+    const unsigned g = (unsigned)((n + 255) / 256);
+    for (int k = 0; k < n_images; ++k) {
+      upload(img.p, images[k], n * 4, st);
+      CK(cudaMemsetAsync(sc.p, 0, 4, st));
+      if (normalize) k_absmax_f32<<<std::min<unsigned>(g, 1184), 256, 0, st>>>(img.as<float>(), n, sc.as<unsigned>());
+      k_stack_add<<<g, 256, 0, st>>>(img.as<float>(), n, sc.as<unsigned>(), normalize, acc.as<double>());
+    }
+    k_stack_finish<<<g, 256, 0, st>>>(acc.as<double>(), n, n_images, o.as<float>());
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,350 @@
+"""Reverse-time migration with the reference's interface (ertm/imaging.py).
+
+``RTMImager.migrate`` keeps the reference signature and result; the
+checkpointed forward pass, the block replay, the time-reversed record
+injection, the backward pass and the imaging condition run in one call of
+the CUDA driver (``ertm_migrate``) with every wavefield, checkpoint and
+accumulator in HBM.  Normalisation, Laplacian, wavenumber low-pass and the
+PML mask run on the device as well (``ertm_postprocess``).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Any, Callable
+
+import numpy as np
+
+from . import _lib
+from . import numerics as num
+from .config import ImagingConfig, QConfig, SolverConfig
+from .exceptions import ImagingError, SolverError
+from .propagation import (PropagationSpec, Propagator2D, QOptions, build_propagator, check_stability,
+                          source_wavelet)
+from .types import ImageResult
+
+#: imaging mode → (source wave, receiver wave) (imaging.py:47-52)
+WAVE_MODES: dict[str, tuple[str, str]] = {"pp": ("P", "P"), "ps": ("P", "S"), "sp": ("S", "P"), "ss": ("S", "S")}
+_ACOUSTIC_MODES = {"pp"}
+
+
+def zero_lag_condition(source_wavefield: np.ndarray, receiver_wavefield: np.ndarray) -> np.ndarray:
+    """Integrand W_s·W_r of the zero-lag cross-correlation (imaging.py:61-66)."""
+    return np.asarray(source_wavefield) * np.asarray(receiver_wavefield)
+
+
+def normalized_terms(source_wavefield, receiver_wavefield):
+    """(W_s·W_r, W_s², W_r²) (imaging.py:69-79)."""
+    s, r = np.asarray(source_wavefield), np.asarray(receiver_wavefield)
+    return s * r, s * s, r * r
+
+
+def excitation_terms(source_amplitude, receiver_wavefield):
+    """A_s·W_r at the excitation time (imaging.py:82-87)."""
+    return np.asarray(source_amplitude) * np.asarray(receiver_wavefield)
+
+
+@dataclass
+class CheckpointStore:
+    """Checkpoint bookkeeping (imaging.py:93-110).
+
+    ``states`` holds ``(step, state)`` pairs when filled through the granular
+    ``record_source_wavefield``; the device driver keeps its checkpoints in
+    HBM and only reports interval and count here.
+    """
+
+    states: list = field(default_factory=list)
+    interval: int = 1
+    bytes_per_state: int = 0
+    n_states: int | None = None
+
+    @property
+    def memory_mb(self) -> float:
+        count = len(self.states) if self.n_states is None else self.n_states
+        return count * self.bytes_per_state / (1024.0**2)
+
+    def summary(self) -> dict[str, Any]:
+        count = len(self.states) if self.n_states is None else self.n_states
+        return {"interval": int(self.interval), "n_states": int(count), "memory_mb": round(self.memory_mb, 3)}
+
+
+def checkpoint_interval(nt: int, bytes_per_state: int, budget_mb: float) -> int:
+    """imaging.py:121-124 — states that fit the budget, then the step between them."""
+    per = max(int(bytes_per_state), 1)
+    budget = max(float(budget_mb), 1.0) * 1024.0**2
+    n_states = max(1, int(budget // per))
+    return max(1, int(np.ceil(nt / n_states)))
+
+
+def record_source_wavefield(prop: Propagator2D, wavelet: np.ndarray, *, budget_mb: float) -> CheckpointStore:
+    """Granular form of the checkpointed forward pass (imaging.py:113-137)."""
+    nt = int(len(wavelet))
+    per = max(int(prop.state_bytes()), 1)
+    store = CheckpointStore(interval=checkpoint_interval(nt, per, budget_mb), bytes_per_state=per)
+    for step in range(nt):
+        prop.step(float(wavelet[step]))
+        if step % store.interval == 0:
+            store.states.append((step, prop.state()))
+    return store
+
+
+def replay_block(prop: Propagator2D, wavelet: np.ndarray, store: CheckpointStore, block_index: int,
+                 separation: str) -> list[dict[str, np.ndarray]]:
+    """Granular block replay (imaging.py:140-162): restore, re-run, copy image fields."""
+    start, state = store.states[block_index]
+    prop.load_state(state)
+    end = store.states[block_index + 1][0] if block_index + 1 < len(store.states) else len(wavelet)
+    out = []
+    for step in range(start, end):
+        prop.step(float(wavelet[step]))
+        out.append({k: np.array(v, copy=True) for k, v in prop.image_fields(separation).items()})
+    return out
+
+
+def _target_component(name: str, engine: str) -> str:
+    """imaging.py:437-444."""
+    if name in ("primary", "p") and engine == "acoustic":
+        return "p"
+    if name == "primary":
+        return "vz"
+    return name
+
+
+def postprocess_image(num: np.ndarray, illum: np.ndarray | None, rillum: np.ndarray | None, *, dx: float,
+                      dz: float, by_illum: bool, by_rillum: bool, eps: float, laplacian: bool,
+                      lowpass_fraction: float, npml: int, boundary: str) -> np.ndarray:
+    """Normalisation + Laplacian + low-pass + PML mask on the device (imaging.py:326-333, 476-502)."""
+    nz, nx = num.shape
+    out = np.empty((nz, nx), dtype=np.float32)
+    n64 = np.ascontiguousarray(num, dtype=np.float64)
+    i64 = None if illum is None else np.ascontiguousarray(illum, dtype=np.float64)
+    r64 = None if rillum is None else np.ascontiguousarray(rillum, dtype=np.float64)
+    _lib.check(_lib.lib().ertm_postprocess(nz, nx, float(dx), float(dz), _lib.ptr(n64), _lib.ptr(i64),
+                                          _lib.ptr(r64), int(by_illum), int(by_rillum), float(eps),
+                                          int(bool(laplacian)), float(lowpass_fraction), int(npml),
+                                          int(boundary == "cpml"), _lib.ptr(out), None), "postprocess")
+    return out
+
+
+class RTMImager:
+    """Single-shot reverse-time migration (imaging.py:168-563)."""
+
+    name = "rtm-imager"
+
+    def __init__(self, imaging_config: ImagingConfig, solver_config: SolverConfig | None = None,
+                 q_config: QConfig | None = None, *, accumulation: str = "fp64") -> None:
+        self.config = imaging_config
+        self.config.validate()
+        self.solver_config = solver_config or SolverConfig()
+        self.solver_config.validate()
+        self.q_config = q_config or QConfig()
+        self.q_config.validate()
+        if accumulation not in _lib.ACCUM:
+            raise ImagingError(f"accumulation must be one of {sorted(_lib.ACCUM)}")
+        self.accumulation = accumulation
+        self._validate_engine_mode()
+
+    def q_options(self, *, compensation: bool = False) -> QOptions | None:
+        """imaging.py:187-202."""
+        if self.solver_config.engine != "viscoacoustic":
+            return None
+        q = self.q_config
+        return QOptions(enabled=True, f_ref=float(q.f_ref), n_mechanisms=int(q.n_mechanisms),
+                        band_ratio=float(q.band_ratio), compensation=bool(compensation and q.enabled),
+                        alpha_c=float(q.alpha_c), amplitude_cap=float(q.amplitude_cap),
+                        lowpass_interval=int(q.lowpass_interval),
+                        f_max=None if q.f_max is None else float(q.f_max), gain_budget_db=float(q.gain_budget_db))
+
+    # ------------------------------------------------------------- public API
+    def migrate(self, shot: Any, model: Any, *, wavelet: np.ndarray | None = None,
+                preprocess: Callable[[np.ndarray, float], np.ndarray] | None = None,
+                modes: tuple[str, ...] | None = None) -> ImageResult:
+        """Migrate one shot.  ``modes`` (extension) images several wave modes
+        from one forward/replay/backward pass; the result then carries the
+        extra images in ``meta['images']``."""
+        results = self.migrate_modes(shot, model, wavelet=wavelet, preprocess=preprocess,
+                                     modes=modes or (self.config.mode,))
+        first = results[0]
+        if len(results) > 1:
+            first.meta["images"] = {r.mode: r.image for r in results}
+        return first
+
+    def migrate_modes(self, shot: Any, model: Any, *, wavelet: np.ndarray | None = None,
+                      preprocess: Callable | None = None, modes: tuple[str, ...] = ("pp",)) -> list[ImageResult]:
+        try:
+            shot.validate()
+            model.validate()
+        except ValueError as exc:
+            raise ImagingError(f"invalid imaging input: {exc}") from exc
+        spec = PropagationSpec.from_config(self.solver_config, model)
+        try:
+            check_stability(model, spec)
+        except Exception as exc:
+            raise ImagingError(str(exc)) from exc
+        engine = self.solver_config.engine
+        separation = self.config.separation
+        pairs = [self._resolve_mode(m) for m in modes]
+        if engine in ("acoustic", "viscoacoustic") and any(m.lower() not in _ACOUSTIC_MODES for m in modes):
+            raise ImagingError("acoustic/viscoacoustic engines image PP only; use solver.engine='elastic'")
+        condition = str(self.config.condition).lower()
+        record = self._prepare_record(shot, spec, preprocess)
+        if not record:
+            raise ImagingError("empty shot record; nothing to back-propagate")
+        w = self._prepare_wavelet(shot, spec, wavelet)
+
+        prop = build_propagator(model, spec, engine=engine, q_options=self.q_options(compensation=False))
+        prop.set_source(shot.source)
+        prop.set_receivers(shot.receivers)
+        back = build_propagator(model, spec, engine=engine, q_options=self.q_options(compensation=True))
+        back.set_source(shot.source)
+        back.set_receivers(shot.receivers)
+
+        per_state = max(int(prop.state_bytes()), 1)   # fields only before the first step
+        interval = checkpoint_interval(len(w), per_state, float(self.config.checkpoint_mb))
+        n_states = (len(w) + interval - 1) // interval
+        store = CheckpointStore(interval=interval, bytes_per_state=per_state, n_states=n_states)
+        start_step = int(np.floor((float(shot.source.delay) + float(self.config.start_periods)
+                                   / max(float(shot.source.f0), 1e-6)) / spec.dt))
+        start_step = int(np.clip(start_step, 0, spec.nt))
+
+        names = list(record)
+        codes = []
+        for n in names:
+            tgt = _target_component(n, engine)
+            codes.append(back._check_component(tgt, "inject"))
+        rec = np.ascontiguousarray(np.stack([np.asarray(record[n], dtype=np.float32) for n in names]))
+        cfg = _lib.MigrateConfig()
+        cfg.nt = int(len(w))
+        cfg.nt_spec = int(spec.nt)
+        cfg.interval = int(interval)
+        cfg.condition = _lib.COND[condition]
+        cfg.illumination = int(condition == "normalized" or bool(self.config.receiver_normalization))
+        cfg.start_step = start_step
+        cfg.separation = _lib.SEP[separation]
+        cfg.n_images = len(pairs)
+        for k, (s, r) in enumerate(pairs):
+            cfg.src_wave[k] = _lib.WAVE[s]
+            cfg.rcv_wave[k] = _lib.WAVE[r]
+        cfg.accum = _lib.ACCUM[self.accumulation]
+        cfg.n_comp = len(codes)
+        for k, c in enumerate(codes):
+            cfg.comp[k] = c
+        nz, nx = model.grid.nz, model.grid.nx
+        num_acc = np.zeros((len(pairs), nz, nx))
+        ill_acc = np.zeros((len(pairs), nz, nx))
+        ril_acc = np.zeros((len(pairs), nz, nx))
+        if rec.shape[1] < spec.nt:
+            raise ImagingError("record shorter than nt after preparation")
+        _lib.check(_lib.lib().ertm_migrate(prop.handle, back.handle, cfg, _lib.ptr(w), _lib.ptr(rec),
+                                          _lib.ptr(num_acc), _lib.ptr(ill_acc), _lib.ptr(ril_acc)), "migrate")
+        prop._psi_allocated = back._psi_allocated = True
+        eps = float(self.config.eps)
+        results = []
+        for k, m in enumerate(modes):
+            image = postprocess_image(
+                num_acc[k], ill_acc[k], ril_acc[k], dx=model.grid.dx, dz=model.grid.dz,
+                by_illum=condition == "normalized" and bool(self.config.illumination),
+                by_rillum=bool(self.config.receiver_normalization), eps=eps, laplacian=bool(self.config.laplacian),
+                lowpass_fraction=float(self.config.lowpass_fraction), npml=spec.npml, boundary=spec.boundary)
+            res = ImageResult(image=image, grid=model.grid, mode=m,
+                              meta=self._meta(spec, engine, shot, store, condition, start_step, prop, back, m))
+            res.validate()
+            results.append(res)
+        return results
+
+    def image_condition(self, source_wavefield: np.ndarray, receiver_wavefield: np.ndarray) -> np.ndarray:
+        s, r = np.asarray(source_wavefield), np.asarray(receiver_wavefield)
+        if s.shape != r.shape:
+            raise ImagingError(f"imaging-condition inputs differ in shape: {s.shape} vs {r.shape}")
+        return zero_lag_condition(s, r).astype(np.float32)
+
+    # ---------------------------------------------------------------- helpers
+    def _validate_engine_mode(self) -> None:
+        if self.solver_config.engine in ("acoustic", "viscoacoustic") and self.config.mode not in _ACOUSTIC_MODES:
+            raise ImagingError(f"acoustic/viscoacoustic engines image PP only, got imaging.mode={self.config.mode!r}")
+
+    def _resolve_mode(self, mode: str | None = None) -> tuple[str, str]:
+        m = str(mode if mode is not None else self.config.mode).lower()
+        if m not in WAVE_MODES:
+            raise ImagingError(f"unsupported imaging mode {m!r}")
+        return WAVE_MODES[m]
+
+    def _prepare_wavelet(self, shot: Any, spec: PropagationSpec, wavelet: np.ndarray | None) -> np.ndarray:
+        if wavelet is not None:
+            return np.ascontiguousarray(wavelet, dtype=np.float32)
+        return source_wavelet(shot.source, spec.dt, spec.nt)
+
+    def _prepare_record(self, shot: Any, spec: PropagationSpec, preprocess: Callable | None) -> dict[str, np.ndarray]:
+        """imaging.py:396-423 — resample to spec.dt, optional hook, pad/trim to nt."""
+        comps = dict(getattr(shot, "components", {}) or {})
+        if not comps:
+            comps["primary"] = shot.data
+        out: dict[str, np.ndarray] = {}
+        for name, arr in comps.items():
+            data = np.asarray(arr, dtype=np.float64)
+            if abs(float(shot.dt) - spec.dt) > 1e-12 and data.shape[0] > 1:
+                data = num.resample_sinc(data, float(shot.dt), spec.dt)
+            if preprocess is not None:
+                data = np.asarray(preprocess(data, spec.dt), dtype=np.float64)
+            out[name] = self._fit_length(data, int(spec.nt))
+        return out
+
+    @staticmethod
+    def _fit_length(data: np.ndarray, nt: int) -> np.ndarray:
+        if data.shape[0] >= nt:
+            return data[:nt]
+        padded = np.zeros((nt, data.shape[1]), dtype=data.dtype)
+        padded[: data.shape[0]] = data
+        return padded
+
+    @staticmethod
+    def _pml_mask(model: Any, spec: PropagationSpec) -> np.ndarray:
+        nz, nx = model.shape
+        n = int(spec.npml)
+        mask = np.ones((nz, nx), dtype=np.float64)
+        mask[:, :n] = 0.0
+        mask[:, -n:] = 0.0
+        mask[-n:, :] = 0.0
+        if spec.boundary == "cpml":
+            mask[:n, :] = 0.0
+        return mask
+
+    def _meta(self, spec, engine, shot, store, condition, start_step=0, prop=None, back=None, mode=None):
+        q_meta: dict[str, Any] = {"model": str(self.q_config.model), "enabled": bool(self.q_config.enabled),
+                                  "alpha_c": float(self.q_config.alpha_c), "f_ref": float(self.q_config.f_ref)}
+        if engine == "viscoacoustic":
+            fs = getattr(prop, "quality_summary", None)
+            if isinstance(fs, dict):
+                q_meta.update(fs)
+            bs = getattr(back, "quality_summary", None)
+            if isinstance(bs, dict):
+                for key in ("compensation", "alpha_c", "alpha_mechanisms", "f_peak_mechanisms_hz", "f_max",
+                            "gain_budget_db"):
+                    if key in bs:
+                        q_meta[key] = bs[key]
+                q_meta["clipped_steps"] = int(bs.get("clipped", 0))
+                q_meta["lowpass_steps"] = int(bs.get("lowpass_steps", 0))
+        m = mode or self.config.mode
+        a, b = self._resolve_mode(m)
+        return {"placeholder": False, "method": "reverse-time migration (two-way wave equation)",
+                "imager": self.name, "engine": engine, "condition": condition,
+                "separation": self.config.separation, "modes": [f"{a}{b}"],
+                "illumination": bool(self.config.illumination),
+                "receiver_normalization": bool(self.config.receiver_normalization),
+                "laplacian": bool(self.config.laplacian), "lowpass_fraction": float(self.config.lowpass_fraction),
+                "checkpoints": store.summary(), "start_step": int(start_step),
+                "start_periods": float(self.config.start_periods), "q": q_meta, "nt": int(spec.nt),
+                "dt": float(spec.dt), "order": int(spec.order), "npml": int(spec.npml),
+                "source_x": float(shot.source.x), "source_z": float(shot.source.z),
+                "n_receivers": int(np.asarray(shot.receivers.x).size), "device": "B200 (sm_100a)",
+                "accumulation": self.accumulation}
+
+
+def build_imager(config: ImagingConfig, solver_config: SolverConfig | None = None,
+                 q_config: QConfig | None = None) -> RTMImager:
+    return RTMImager(config, solver_config, q_config)
+
+
+__all__ = ["WAVE_MODES", "zero_lag_condition", "normalized_terms", "excitation_terms", "CheckpointStore",
+           "checkpoint_interval", "record_source_wavefield", "replay_block", "postprocess_image", "RTMImager",
+           "build_imager", "SolverError"]

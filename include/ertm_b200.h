@@ -1,0 +1,179 @@
+/* ertm_b200 — C ABI of the B200-native ERTM reverse-time-migration hot path.
+ *
+ * The reference (Sherlyn7189/Challenge-Cup) is a Python/NumPy package; its
+ * hot path is ertm/propagation.py, ertm/imaging.py and ertm/numerics.py.  A
+ * Python host binds this ABI with ctypes (challenge-cup_b200/ertm_b200/_lib.py)
+ * and keeps the reference's call signatures; any other host can bind the
+ * same symbols.  Each entry point below names the reference interface it
+ * replaces.
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a negative code on failure;
+ *    ertm_last_error() gives the message of the calling thread's last error.
+ *  - Array arguments may be host or device pointers (unified addressing);
+ *    copies use cudaMemcpyDefault.  Arrays are C-order float32 unless stated.
+ *  - "padded" arrays have the reference geometry (nz+2·pad, nx+2·pad) with
+ *    pad = order/2 + 1 (numerics.py:60-62, propagation.py:206-208).
+ *  - A propagator owns one CUDA stream-ordered set of device buffers; all its
+ *    work is enqueued on the stream given at creation (0 = legacy default).
+ */
+#ifndef ERTM_B200_H
+#define ERTM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ERTM_OK 0
+#define ERTM_ERR_ARG (-1)
+#define ERTM_ERR_CUDA (-2)
+#define ERTM_ERR_STATE (-3)
+
+/* engines (propagation.py:986-1001) */
+#define ERTM_ENGINE_ACOUSTIC 0
+#define ERTM_ENGINE_ELASTIC 1
+#define ERTM_ENGINE_VISCO 2
+/* boundaries (propagation.py:64-65) */
+#define ERTM_BOUNDARY_CPML 0
+#define ERTM_BOUNDARY_FREE 1
+#define ERTM_BOUNDARY_NONE 2
+/* record components */
+#define ERTM_COMP_P 0
+#define ERTM_COMP_VX 1
+#define ERTM_COMP_VZ 2
+#define ERTM_COMP_SXX 3
+#define ERTM_COMP_SZZ 4
+#define ERTM_COMP_SXZ 5
+/* source mechanisms (types.py:137-159) */
+#define ERTM_MECH_EXPLOSIVE 0
+#define ERTM_MECH_SHEAR 1
+#define ERTM_MECH_FORCE_Z 2
+/* imaging conditions (imaging.py:61-87) */
+#define ERTM_COND_ZERO_LAG 0
+#define ERTM_COND_NORMALIZED 1
+#define ERTM_COND_EXCITATION 2
+/* wave types and P/S separation (imaging.py:47-52, propagation.py:945-977) */
+#define ERTM_WAVE_P 0
+#define ERTM_WAVE_S 1
+#define ERTM_SEP_STRESS 0
+#define ERTM_SEP_DIVCURL 1
+/* imaging accumulators */
+#define ERTM_ACCUM_FP64 0
+#define ERTM_ACCUM_KAHAN 1
+
+typedef struct ertm_prop_config {
+  int32_t engine;            /* ERTM_ENGINE_* */
+  int32_t order;             /* 2, 4, 6 or 8 */
+  int32_t nx, nz;            /* physical grid */
+  double dx, dz, x0, z0;     /* spacing and origin (types.py:20-82) */
+  double dt;                 /* time step */
+  int32_t free_surface;      /* 1: zero the free-surface row (acoustic p; elastic szz, sxz) */
+  int32_t npml_x_left, npml_x_right, npml_z_top, npml_z_bottom; /* CPML strip widths, 0 = none */
+  int32_t n_mech;            /* viscoacoustic: relaxation mechanisms L */
+  int32_t n_q;               /* viscoacoustic: distinct Q values in the tables */
+  int32_t compensation;      /* viscoacoustic: apply the amplitude cap / low-pass after each step */
+  double amplitude_cap;      /* QOptions.amplitude_cap */
+  int32_t lowpass_interval;  /* QOptions.lowpass_interval */
+  int32_t reserved;
+} ertm_prop_config;
+
+typedef struct ertm_prop_info {
+  int32_t nzp, nxp, ld, pad;
+  int64_t state_bytes;       /* device bytes of one checkpoint (fields + CPML strips) */
+  int64_t field_bytes;       /* reference field bytes (n_fields · nzp · nxp · 4) */
+  int64_t step_index;
+  int32_t n_fields, clipped, lowpass_steps, n_receivers;
+} ertm_prop_info;
+
+typedef struct ertm_migrate_config {
+  int32_t nt;                /* len(wavelet): forward and replay steps */
+  int32_t nt_spec;           /* spec.nt: excitation backward loop end (imaging.py:286-288) */
+  int32_t interval;          /* checkpoint interval (imaging.py:121-124) */
+  int32_t condition;         /* ERTM_COND_* */
+  int32_t illumination;      /* accumulate S² and R² (normalized or receiver normalisation) */
+  int32_t start_step;        /* cross-correlation starts here (imaging.py:268-277) */
+  int32_t separation;        /* ERTM_SEP_* (elastic) */
+  int32_t n_images;          /* 1..4 images sharing one forward/replay/backward pass */
+  int32_t src_wave[4];       /* ERTM_WAVE_* per image */
+  int32_t rcv_wave[4];
+  int32_t accum;             /* ERTM_ACCUM_* (excitation is always FP64) */
+  int32_t n_comp;            /* record components */
+  int32_t comp[8];           /* ERTM_COMP_* injection target per component (imaging.py:437-444) */
+} ertm_migrate_config;
+
+/* library ---------------------------------------------------------------- */
+const char* ertm_last_error(void);
+int32_t ertm_version(void);
+/* Select the device and check it is sm_100 (no reference counterpart). */
+int32_t ertm_init(int32_t device);
+
+/* propagators ------------------------------------------------------------ */
+/* Replaces AcousticPropagator/ViscoacousticPropagator/ElasticPropagator
+ * construction (propagation.py:411-421, 518-606, 858-871): materials are
+ * edge-padded and averaged on the device.  vp, vs, rho are physical (nz, nx).
+ * The pml_a and pml_b arrays are the float32 CPML profiles (numerics.py:143-219) of the
+ * padded axes.  The viscoacoustic tables (qidx, tau, delta, mref, relax_a)
+ * come from the host-side GSLS fit (propagation.py:563-675); NULL otherwise. */
+void* ertm_prop_create(const ertm_prop_config* cfg, const float* vp, const float* vs, const float* rho,
+                       const float* pml_ax, const float* pml_bx, const float* pml_az, const float* pml_bz,
+                       const uint8_t* qidx, const double* tau, const double* delta, const double* mref,
+                       const float* relax_a, void* stream);
+void ertm_prop_destroy(void* prop);
+int32_t ertm_prop_info_get(void* prop, ertm_prop_info* info);
+/* Propagator2D.reset (propagation.py:309-311, 423-428). */
+int32_t ertm_prop_reset(void* prop);
+/* Propagator2D.set_source (propagation.py:264-267): padded node and mechanism. */
+int32_t ertm_prop_set_source(void* prop, int32_t iz, int32_t ix, int32_t mechanism);
+/* Propagator2D.set_receivers (propagation.py:269-271): physical coordinates. */
+int32_t ertm_prop_set_receivers(void* prop, int32_t n, const double* x, const double* z);
+/* Propagator2D.step (propagation.py:314-316, 430-454, 686-723, 840-883):
+ * n_steps steps with source amplitudes amps[0..n_steps) (host float64 array,
+ * NULL = 0): the field receives float32(amp), the viscoacoustic strain
+ * float32(amp / K_R) (propagation.py:707-713). */
+int32_t ertm_prop_step(void* prop, int32_t n_steps, const double* amps);
+/* Propagator2D.sample (propagation.py:456-470, 885-898): out is n_comp × nrec. */
+int32_t ertm_prop_sample(void* prop, int32_t n_comp, const int32_t* comps, float* out);
+/* Propagator2D.inject (propagation.py:472-494, 764-774, 900-942). */
+int32_t ertm_prop_inject(void* prop, int32_t comp, const float* values);
+/* Propagator2D.image_fields (propagation.py:500-501, 795-796, 945-977): (nz, nx). */
+int32_t ertm_prop_image_field(void* prop, int32_t wave, int32_t separation, float* out);
+/* Field / CPML-memory access for state()/load_state() (propagation.py:283-306).
+ * Fields are padded (nzp, nxp); psi terms are expanded to full padded size. */
+int32_t ertm_prop_read_field(void* prop, int32_t slot, float* out);
+int32_t ertm_prop_write_field(void* prop, int32_t slot, const float* in);
+int32_t ertm_prop_read_psi(void* prop, int32_t axis, int32_t term, float* out);
+int32_t ertm_prop_write_psi(void* prop, int32_t axis, int32_t term, const float* in);
+int32_t ertm_prop_set_step_index(void* prop, int64_t step_index);
+/* Raw device checkpoint of the whole state block (state_bytes bytes). */
+int32_t ertm_prop_save_state(void* prop, void* dst);
+int32_t ertm_prop_load_state(void* prop, const void* src);
+
+/* whole-loop drivers ------------------------------------------------------ */
+/* run_forward (propagation.py:1018-1052): steps with amps[t] and samples the
+ * components after each step into out (n_comp × nt × nrec). */
+int32_t ertm_forward(void* prop, int32_t nt, const float* amps, int32_t n_comp, const int32_t* comps,
+                     float* out);
+/* RTMImager.migrate core (imaging.py:255-331): checkpointed forward,
+ * block replay, time-reversed injection, backward propagation and the
+ * imaging condition.  record is n_comp × nt_spec × nrec float32; the
+ * accumulators are n_images × (nz, nx) float64 (num, illum, rillum). */
+int32_t ertm_migrate(void* fwd, void* back, const ertm_migrate_config* cfg, const float* wavelet,
+                     const float* record, double* num, double* illum, double* rillum);
+/* Normalisation and _postprocess (imaging.py:326-333, 476-502): image =
+ * num/(illum+eps)/(rillum+eps) as selected, Laplacian, wavenumber low-pass
+ * (lowpass < 1), PML mask of width npml (top too when top_mask). */
+int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const double* num, const double* illum,
+                         const double* rillum, int32_t by_illum, int32_t by_rillum, double eps,
+                         int32_t laplacian, double lowpass, int32_t npml, int32_t top_mask, float* out,
+                         void* stream);
+/* stack_images (pipeline.py:133-161): images is n_images pointers to (n,) float32. */
+int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
+                   void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ERTM_B200_H */

@@ -1,0 +1,223 @@
+"""CUDA path vs the reference: golden vectors and the CPU oracle.
+
+Acoustic and elastic fields, CPML memories, shot records and image fields are
+compared bit for bit (the kernels reproduce the reference's float32
+operation order).  The viscoacoustic engine's GSLS tables go through exp()
+on the host and its compensated run through FFTs, so it is compared with a
+relative-L2 tolerance; RTM images go through an FP64 FFT low-pass and are
+compared at relative L2 ≤ 1e-6 (the north-star bar is 1e-4).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from helpers import (MIGRATE_CASES, PROPAGATION_CASES, imaging_from, load, model_from, q_from,
+                     q_options_for_migrate, receivers_from, rel_l2, solver_from, source_from)
+
+pytestmark = pytest.mark.gpu
+
+IMAGE_TOL = 1e-6     # images: FP64 cuFFT vs NumPy pocketfft in the post-processing
+VISCO_TOL = 1e-6     # viscoacoustic fields: host exp() tables / FFT low-pass
+
+
+@pytest.fixture(scope="module")
+def eb():
+    import ertm_b200
+    from ertm_b200 import _lib
+    _lib.lib()  # fails loudly without the library or a B200
+    return ertm_b200
+
+
+def _product_propagation(eb, fx):
+    from ertm_b200.propagation import PropagationSpec, QOptions, build_propagator
+    meta = fx["meta"]
+    dt, nt, order, npml = fx["spec"]
+    spec = PropagationSpec(dt=float(dt), nt=int(nt), order=int(order), npml=int(npml), dtype="float32",
+                           boundary=meta["boundary"])
+    q = QOptions(**meta["q"]) if meta["q"] else None
+    prop = build_propagator(model_from(fx), spec, engine=meta["engine"], q_options=q)
+    prop.set_source(source_from(fx, meta["mechanism"]))
+    prop.set_receivers(receivers_from(fx))
+    names = meta["names"]
+    rec = {n: np.zeros((int(nt), len(fx["rx"])), np.float32) for n in names}
+    for t in range(int(nt)):
+        if meta["inject_every"] and t % meta["inject_every"] == 0:
+            for n in names:
+                prop.inject(n, fx["inj_values"][t])
+        prop.step(float(fx["wavelet"][t]))
+        s = prop.sample(tuple(names))
+        for n in names:
+            rec[n][t] = s[n]
+    return prop, rec
+
+
+@pytest.mark.parametrize("case", PROPAGATION_CASES)
+def test_propagation_matches_reference_golden(eb, case):
+    fx = load(case)
+    prop, rec = _product_propagation(eb, fx)
+    exact = fx["meta"]["engine"] != "viscoacoustic"
+    st = prop.state()
+    for k, v in st.items():
+        key = f"state_{k.replace(':', '_')}"
+        assert key in fx, key
+        if exact:
+            assert np.array_equal(v, fx[key]), (case, k, rel_l2(v, fx[key]))
+        else:
+            assert rel_l2(v, fx[key]) < VISCO_TOL, (case, k, rel_l2(v, fx[key]))
+    for n, r in rec.items():
+        if exact:
+            assert np.array_equal(r, fx[f"rec_{n}"]), (case, n, rel_l2(r, fx[f"rec_{n}"]))
+        else:
+            assert rel_l2(r, fx[f"rec_{n}"]) < VISCO_TOL, (case, n)
+    assert prop.state_bytes() == fx["meta"]["state_bytes"]
+    if fx["meta"]["engine"] == "elastic":
+        for sep in ("stress", "divcurl"):
+            for k, v in prop.image_fields(sep).items():
+                assert np.array_equal(v, fx[f"img_{sep}_{k}"]), (case, sep, k)
+    if fx["meta"]["engine"] == "viscoacoustic":
+        qs = prop.quality_summary
+        assert qs["clipped"] == int(fx["clipped"])
+        assert qs["lowpass_steps"] == int(fx["lowpass_steps"])
+
+
+@pytest.mark.parametrize("case", MIGRATE_CASES)
+def test_migrate_matches_reference_golden(eb, case):
+    from ertm_b200 import ImagingConfig, QConfig, RTMImager, SolverConfig
+    from ertm_b200.types import ReceiverSpec, ShotRecord, SourceSpec
+    fx = load(case)
+    meta = fx["meta"]
+    comps = {k[len("shot_"):]: v for k, v in fx.items() if k.startswith("shot_") and k != "shot_dt"}
+    src = source_from(fx)
+    rec = receivers_from(fx)
+    primary = comps[meta["components"][0]]
+    shot = ShotRecord(data=primary, dt=float(fx["shot_dt"]), t=np.arange(primary.shape[0]) * float(fx["shot_dt"]),
+                      receivers=ReceiverSpec(x=rec.x, z=rec.z),
+                      source=SourceSpec(x=src.x, z=src.z, f0=src.f0, delay=src.delay), components=comps)
+    imaging = ImagingConfig(mode=meta["mode"], condition=meta["condition"], separation=meta["separation"],
+                            receiver_normalization=meta["receiver_normalization"], laplacian=True,
+                            lowpass_fraction=meta["lowpass"], checkpoint_mb=meta["checkpoint_mb"])
+    solver = SolverConfig(nt=meta["nt"], dt=meta["dt"], order=8, boundary=meta["boundary"], dtype="float32",
+                          engine=meta["engine"], npml=12)
+    q = QConfig(**meta["q"]) if meta["q"] else None
+    img = RTMImager(imaging, solver, q).migrate(shot, model_from_types(fx))
+    assert img.meta["checkpoints"]["interval"] == meta["checkpoints"]["interval"]
+    assert img.meta["checkpoints"]["n_states"] == meta["checkpoints"]["n_states"]
+    assert img.meta["start_step"] == meta["start_step"]
+    err = rel_l2(img.image, fx["image"])
+    assert err < IMAGE_TOL, (case, err)
+
+
+def model_from_types(fx):
+    from ertm_b200.types import ElasticModel, GridSpec
+    m = model_from(fx)
+    g = m.grid
+    return ElasticModel(grid=GridSpec(nx=g.nx, nz=g.nz, dx=g.dx, dz=g.dz, x0=g.x0, z0=g.z0),
+                        vp=m.vp, vs=m.vs, rho=m.rho, qp=m.qp, qs=m.qs)
+
+
+def test_migrate_pp_ps_in_one_pass_equals_separate_runs(eb):
+    """One forward/replay/backward pass imaging PP and PS gives the single-mode images."""
+    from ertm_b200 import ImagingConfig, RTMImager, SolverConfig
+    from ertm_b200.types import ReceiverSpec, ShotRecord, SourceSpec
+    fx = load("mig_elastic_pp_divcurl")
+    meta = fx["meta"]
+    comps = {k[len("shot_"):]: v for k, v in fx.items() if k.startswith("shot_") and k != "shot_dt"}
+    src = source_from(fx)
+    rec = receivers_from(fx)
+    primary = comps[meta["components"][0]]
+    shot = ShotRecord(data=primary, dt=float(fx["shot_dt"]), t=np.arange(primary.shape[0]) * float(fx["shot_dt"]),
+                      receivers=ReceiverSpec(x=rec.x, z=rec.z),
+                      source=SourceSpec(x=src.x, z=src.z, f0=src.f0, delay=src.delay), components=comps)
+    solver = SolverConfig(nt=meta["nt"], dt=meta["dt"], order=8, boundary=meta["boundary"], engine="elastic",
+                          npml=12)
+    model = model_from_types(fx)
+    both = RTMImager(ImagingConfig(mode="pp", condition="normalized", checkpoint_mb=1.0), solver).migrate_modes(
+        shot, model, modes=("pp", "ps"))
+    for res in both:
+        single = RTMImager(ImagingConfig(mode=res.mode, condition="normalized", checkpoint_mb=1.0),
+                           solver).migrate(shot, model)
+        assert np.array_equal(res.image, single.image), res.mode
+
+
+def test_checkpoint_replay_is_bit_exact(eb):
+    """Mirror of the reference KAT (tests/test_rtm.py:188-214) on the device."""
+    from ertm_b200.propagation import AcousticPropagator, PropagationSpec, source_wavelet
+    from ertm_b200.types import ElasticModel, GridSpec, SourceSpec
+    g = GridSpec(nx=61, nz=51, dx=10.0, dz=10.0)
+    sh = g.shape
+    model = ElasticModel(grid=g, vp=np.full(sh, 3000.0, np.float32), vs=np.full(sh, 1700.0, np.float32),
+                         rho=np.full(sh, 2400.0, np.float32), qp=np.full(sh, 100.0, np.float32),
+                         qs=np.full(sh, 50.0, np.float32))
+    spec = PropagationSpec(dt=5e-4, nt=80, order=8, npml=8, dtype="float32", boundary="cpml")
+    src = SourceSpec(x=300.0, z=250.0, f0=20.0, delay=0.03)
+    w = source_wavelet(src, spec.dt, spec.nt)
+    ref = AcousticPropagator(model, spec)
+    ref.set_source(src)
+    for t in range(60):
+        ref.step(float(w[t]))
+    rep = AcousticPropagator(model, spec)
+    rep.set_source(src)
+    rep.step(float(w[0]))
+    rep.load_state(rep.state())
+    for t in range(1, 60):
+        rep.step(float(w[t]))
+    assert np.array_equal(rep.p, ref.p)
+    expected = sum(getattr(rep, n).nbytes for n in ("p", "vx", "vz")) + rep.pml.memory_bytes()
+    assert rep.state_bytes() == expected
+
+
+@pytest.mark.parametrize("engine,boundary,order", [("acoustic", "cpml", 8), ("acoustic", "free", 4),
+                                                   ("elastic", "free", 8), ("elastic", "cpml", 6),
+                                                   ("viscoacoustic", "cpml", 8), ("acoustic", "none", 2)])
+def test_forward_record_matches_oracle_on_seeded_models(eb, engine, boundary, order):
+    """Seeded layered model, non-square grid, all stencil orders: GPU == oracle."""
+    from ertm_b200.propagation import PropagationSpec, QOptions, run_forward
+    rng = np.random.default_rng(7)
+    nz, nx = 53, 71
+    vp = rng.uniform(2000.0, 3000.0, size=(nz, nx)).astype(np.float32)
+    model = model_from({"m_vp": vp, "m_vs": (vp / 1.9).astype(np.float32),
+                        "m_rho": rng.uniform(1800, 2400, (nz, nx)).astype(np.float32),
+                        "m_qp": np.where(np.arange(nz)[:, None] < 25, 40.0, 90.0).repeat(nx, 1).astype(np.float32),
+                        "m_qs": np.full((nz, nx), 30.0, np.float32),
+                        "m_grid": np.array([nx, nz, 8.0, 6.0, 0.0, 0.0])})
+    dt = 0.8 * orc.cfl_dt(float(vp.max()), 8.0, 6.0, order, 0.5)
+    spec = PropagationSpec(dt=dt, nt=120, order=order, npml=10, boundary=boundary)
+    src = source_from({"src": np.array([260.0, 50.0, 30.0, 0.03, 1.0])})
+    rcv = receivers_from({"rx": rng.uniform(-10, 570, 23), "rz": rng.uniform(0, 320, 23)})
+    comps = ("p", "vx", "vz") if engine != "elastic" else ("p", "vx", "vz", "sxz")
+    q = QOptions(enabled=True, f_ref=30.0) if engine == "viscoacoustic" else None
+    got = run_forward(model, src, rcv, spec, engine=engine, components=comps, q_options=q)
+    ospec = orc.Spec(dt=dt, nt=120, order=order, npml=10, boundary=boundary)
+    want = orc.run_forward(model, src, rcv, ospec, engine=engine, components=comps, q=q)
+    for n in comps:
+        if engine == "viscoacoustic":
+            assert rel_l2(got[n], want[n]) < VISCO_TOL, n
+        else:
+            assert np.array_equal(got[n], want[n]), (n, rel_l2(got[n], want[n]))
+
+
+def test_stack_images_matches_reference_golden(eb):
+    from ertm_b200.stacking import stack_arrays
+    fx = load("stack")
+    assert np.array_equal(stack_arrays(list(fx["images"])), fx["stacked"])
+
+
+def test_kahan_accumulation_close_to_fp64(eb):
+    """Form (a): Kahan-compensated FP32 imaging sums vs the FP64 accumulators."""
+    from ertm_b200 import ImagingConfig, RTMImager, SolverConfig
+    from ertm_b200.types import ReceiverSpec, ShotRecord, SourceSpec
+    fx = load("mig_acoustic_norm_rn")
+    meta = fx["meta"]
+    src, rec = source_from(fx), receivers_from(fx)
+    data = fx["shot_p"]
+    shot = ShotRecord(data=data, dt=float(fx["shot_dt"]), t=np.arange(data.shape[0]) * float(fx["shot_dt"]),
+                      receivers=ReceiverSpec(x=rec.x, z=rec.z),
+                      source=SourceSpec(x=src.x, z=src.z, f0=src.f0, delay=src.delay), components={"p": data})
+    solver = SolverConfig(nt=meta["nt"], dt=meta["dt"], boundary=meta["boundary"], engine="acoustic", npml=12)
+    imaging = ImagingConfig(condition="normalized", receiver_normalization=True, checkpoint_mb=1.0)
+    a = RTMImager(imaging, solver).migrate(shot, model_from_types(fx))
+    b = RTMImager(imaging, solver, accumulation="kahan").migrate(shot, model_from_types(fx))
+    assert rel_l2(b.image, a.image) < 1e-5
