@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 RTM hot path.
+
+Default workload (one GPU): elastic P-SV borehole 4C RTM with PP and PS
+imaging — 401×601 grid at 5 m, 8 surface shots, 100 well receivers, 4912
+steps (1.5 s at the CFL dt), normalized condition, divcurl separation.  A
+benchmark step migrates all shots of the job (PP and PS from one
+forward/replay/backward pass per shot) and stacks them.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (weak scaling: every
+        rank migrates its own 8 shots; the stacks are summed with NCCL)
+
+One JSON line is printed by rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT), str(ROOT / "challenge-cup_b200")]
+
+import numpy as np  # noqa: E402
+
+METRIC = "shots/s & Gcell-updates/s batched vs plain on 1 B200; p99 latency @ 1e-4 err"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", default="elastic4c")
+    ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (profiling runs)")
+    ap.add_argument("--shots", type=int, default=None, help="override shots per rank")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=48)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self) -> None:
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self) -> None:
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_(self, t) -> None:
+        if self.pg:
+            self.pg.all_reduce(t)
+
+    def close(self) -> None:
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"bench_clocks_{os.getpid()}.csv"
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(name: str) -> float | None:
+    """Per-launch DRAM bytes from the committed ncu summary, if one exists."""
+    p = ROOT / "profiles" / f"{name}.traffic"
+    try:
+        return float(p.read_text().split()[0])
+    except (OSError, ValueError, IndexError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# workload helpers
+# ---------------------------------------------------------------------------
+def build_workload(args, rank: int):
+    from ertm_b200 import workloads
+    wl = workloads.WORKLOADS[args.config](seed=0, **({"n_shots": args.shots} if args.shots else {}),
+                                          **({"nt": args.nt} if args.nt else {}))
+    if rank:
+        # weak scaling: same model, a different seeded shot set per rank
+        rng = np.random.default_rng(1000 + rank)
+        g = wl.model.grid
+        from ertm_b200.types import SourceSpec
+        wl.sources = [SourceSpec(x=float(x), z=s.z, f0=s.f0, delay=s.delay)
+                      for x, s in zip(np.sort(rng.uniform(0.05, 0.95, len(wl.sources)) * g.x_max), wl.sources)]
+    return wl
+
+
+def imager_for(wl):
+    from ertm_b200 import ImagingConfig, QConfig, RTMImager, SolverConfig
+    solver = SolverConfig(nt=wl.nt, dt=wl.dt, order=8, boundary=wl.boundary, dtype="float32", engine=wl.engine,
+                          npml=wl.npml)
+    imaging = ImagingConfig(mode=wl.modes[0], condition=wl.condition, separation=wl.separation,
+                            checkpoint_mb=wl.checkpoint_mb)
+    q = QConfig(**wl.q) if wl.q else None
+    return RTMImager(imaging, solver, q), solver
+
+
+def synthesize(wl, solver):
+    """Shot records from the GPU forward model (untimed set-up)."""
+    from ertm_b200.solver import FiniteDifferenceSolver
+    fd = FiniteDifferenceSolver(solver)
+    return [fd.forward(wl.model, s, wl.receivers, components=wl.components) for s in wl.sources]
+
+
+def step_bytes(prop) -> float:
+    """Algorithmic HBM bytes of one propagator step: each state array read and
+    written once, each per-cell coefficient read once, CPML strips read and
+    written (8 B per strip cell per term)."""
+    info = prop.info()
+    npad = info.nzp * info.nxp
+    n_state = {"acoustic": 3, "elastic": 5, "viscoacoustic": 4 + getattr(prop, "n_mechanisms", 0)}[prop._engine]
+    n_coef = {"acoustic": 3, "elastic": 5, "viscoacoustic": 3 + 2 * getattr(prop, "n_mechanisms", 0)}[prop._engine]
+    _, _, _, _, (xl, xr, zt, zb) = prop._strips()
+    nterm = len(prop._psi_terms) // 2
+    strips = nterm * ((xl + xr) * info.nzp + (zt + zb) * info.nxp)
+    return float(npad * (8 * n_state + 4 * n_coef) + 8 * strips)
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle sample (baseline)
+# ---------------------------------------------------------------------------
+def cpu_sample(config: str, nt_sample: int) -> dict:
+    """Time the CPU oracle (NumPy restatement of the reference) migrating one
+    shot of the workload for nt_sample steps; extrapolate to the full job."""
+    import oracle as orc
+    from ertm_b200 import workloads
+    wl = workloads.WORKLOADS[config](seed=0)
+    imager, solver = imager_for(wl)
+    nrec = wl.receivers.nrec
+    rng = np.random.default_rng(5)
+    comps = {c: rng.normal(scale=1e-3, size=(nt_sample, nrec)).astype(np.float32) for c in wl.components}
+    from types import SimpleNamespace
+    sv = SimpleNamespace(**{k: getattr(solver, k) for k in ("dt", "order", "boundary", "dtype", "engine", "npml")},
+                         nt=nt_sample)
+    q = None
+    if wl.q:
+        q = SimpleNamespace(enabled=True, f_ref=wl.q["f_ref"], n_mechanisms=wl.q["n_mechanisms"], band_ratio=1.5,
+                            compensation=True, alpha_c=wl.q["alpha_c"], amplitude_cap=wl.q["amplitude_cap"],
+                            lowpass_interval=wl.q["lowpass_interval"], f_max=wl.q["f_max"],
+                            gain_budget_db=wl.q["gain_budget_db"])
+    t0 = time.perf_counter()
+    orc.migrate(comps, wl.dt, wl.sources[0], wl.receivers, wl.model, sv, imager.config, q)
+    secs = time.perf_counter() - t0
+    migrates_per_shot = len(wl.modes)      # the reference runs one RTMImager per mode
+    per_shot = secs * (wl.nt / nt_sample) * migrates_per_shot
+    return {"per_shot_s": per_shot, "sample_s": secs, "nt_sample": nt_sample, "nt": wl.nt,
+            "migrates_per_shot": migrates_per_shot, "cells": wl.cells}
+
+
+def _cpu_worker(args):
+    config, nt_sample = args
+    sys.path[:0] = [str(ROOT), str(ROOT / "challenge-cup_b200")]
+    return cpu_sample(config, nt_sample)
+
+
+def run_reference(args, dist: Dist) -> None:
+    if dist.rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    nt_sample = max(8, args.cpu_sample_steps // 4)
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_worker, [(args.config, nt_sample)] * cores)
+            if i >= args.warmup:
+                times.append((time.perf_counter() - t0, res))
+    wall = sum(t for t, _ in times) / len(times)
+    per_shot = statistics.mean(r["per_shot_s"] for _, rs in times for r in rs)
+    value = cores / per_shot
+    cells = times[0][1][0]["cells"]
+    nt = times[0][1][0]["nt"]
+    sample = (f"{cores} spawned processes, each migrating one shot of the workload for {nt_sample} of {nt} "
+              f"steps with the NumPy oracle; extrapolated linearly in steps, x{times[0][1][0]['migrates_per_shot']}"
+              f" migrates per shot (one per imaging mode)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": args.config},
+            "gcell_updates_per_s": value * 3 * nt * cells * times[0][1][0]["migrates_per_shot"] / 1e9,
+            "cpu_baseline": {"value": value, "unit": "shots/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, dist: Dist) -> None:
+    import torch
+
+    from ertm_b200 import _lib
+    from ertm_b200.imaging import ShotMigrator
+    from ertm_b200.stacking import stack_images
+    from ertm_b200.types import ShotRecord
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    _lib.lib(dev)
+    L = _lib.lib(dev)
+    wl = build_workload(args, dist.rank)
+    imager, solver = imager_for(wl)
+    shots = synthesize(wl, solver)
+    names = list(wl.components)
+    rec_dev = [torch.from_numpy(np.stack([s.components[n] for n in names])).cuda() for s in shots]
+    from ertm_b200.propagation import source_wavelet
+    wavelets = [source_wavelet(s, wl.dt, wl.nt) for s in wl.sources]
+    mig = ShotMigrator(imager, wl.model)
+    g = wl.model.grid
+    n_modes = len(wl.modes)
+    stack_out = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
+
+    import ctypes as C
+
+    def device_job():
+        imgs = [mig.migrate_device(src, wl.receivers, rec_dev[i], names, wavelets[i], modes=wl.modes)
+                for i, src in enumerate(wl.sources)]
+        for k in range(n_modes):
+            ptrs = (C.c_void_p * len(imgs))(*[im[k].data_ptr() for im in imgs])
+            _lib.check(L.ertm_stack(len(imgs), g.nz * g.nx, C.cast(ptrs, C.c_void_p), 1, stack_out[k].data_ptr(),
+                                    None), "stack")
+        return stack_out
+
+    for _ in range(args.warmup):
+        device_job()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    _lib.check(L.ertm_profile_stencil(1, 8), "profile")
+    launches0 = L.ertm_launch_count()
+    times = []
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        device_job()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = int(L.ertm_launch_count() - launches0)
+    tot, cnt = C.c_double(), C.c_int64()
+    _lib.check(L.ertm_profile_read(C.byref(tot), C.byref(cnt)), "profile read")
+    _lib.check(L.ertm_profile_stencil(0, 1), "profile off")
+    step_ms = float(tot.value) / max(int(cnt.value), 1)
+
+    total_ms = dist.max(float(sum(times)))
+    shots_total = len(wl.sources) * dist.world * args.steps
+    value = shots_total / (total_ms / 1e3)
+    cell_updates = 3 * wl.nt * wl.cells * shots_total
+    # combined stack across ranks: the only collective
+    if dist.world > 1:
+        dist.sum_(stack_out)
+        stack_out /= dist.world
+
+    # end to end through the public API: pinned host records in, host image out
+    pinned = [{n: torch.from_numpy(s.components[n]).pin_memory().numpy() for n in names} for s in shots]
+    e2e_times = []
+    h2d = d2h = 0
+    for _ in range(args.e2e_steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        per_mode = {m: [] for m in wl.modes}
+        for i, s in enumerate(shots):
+            shot = ShotRecord(data=pinned[i][names[0]], dt=s.dt, t=s.t, receivers=s.receivers, source=s.source,
+                              components=pinned[i])
+            for res in imager.migrate_modes(shot, wl.model, modes=wl.modes):
+                per_mode[res.mode].append(res)
+        stacked = {m: stack_images(v, normalize=True).image for m, v in per_mode.items()}
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+        assert all(np.isfinite(v).all() for v in stacked.values())
+    npix = g.nx * g.nz
+    n_shots = len(shots)
+    comp_bytes = len(names) * wl.nt * wl.receivers.nrec * 4
+    model_bytes = 3 * npix * 4 * 2                      # vp, vs, rho per propagator, two propagators
+    h2d = n_shots * (comp_bytes + model_bytes + 3 * n_modes * npix * 8 + wl.nt * 4)
+    d2h = n_shots * (3 * n_modes * npix * 8 + n_modes * npix * 4) + n_modes * npix * 4
+    e2e_s = dist.max(statistics.mean(e2e_times))
+    e2e_value = n_shots * dist.world / e2e_s
+
+    peak, peak_kind = measured_hbm_peak()
+    bytes_step = step_bytes(mig.prop)
+    achieved = bytes_step / (step_ms * 1e-3) / 1e9
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cs = cpu_sample(args.config, args.cpu_sample_steps)
+        cpu = {"value": 1.0 / cs["per_shot_s"], "unit": "shots/s", "cores": 1, "kind": "port",
+               "sample": (f"one shot, {cs['nt_sample']} of {cs['nt']} steps of the NumPy oracle migrate "
+                          f"({cs['sample_s']:.1f} s), extrapolated linearly in steps and x{cs['migrates_per_shot']} "
+                          f"for one migrate per imaging mode as the reference runs them")}
+    line = {
+        "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded layered model with cavities and a fault; records from the GPU forward model",
+        "config": {"workload": wl.name, "config": args.config, "nx": g.nx, "nz": g.nz, "dx": g.dx, "nt": wl.nt,
+                   "dt": wl.dt, "engine": wl.engine, "modes": list(wl.modes), "condition": wl.condition,
+                   "separation": wl.separation, "shots_per_rank": len(wl.sources), "receivers": wl.receivers.nrec,
+                   "components": names, "accumulation": "fp64", "l2": "flushed between steps (256 MiB write)",
+                   "path": "plain: one shot at a time, PP and PS from one pass", "parallelism": f"shots x{dist.world}"},
+        "gcell_updates_per_s": cell_updates / (total_ms / 1e3) / 1e9,
+        "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": committed_traffic(f"{wl.engine}_step"),
+                     "kernel": f"{wl.engine} step (velocity + stress kernels)",
+                     "bytes_per_step": bytes_step, "step_us": step_ms * 1e3, "timed_steps": int(cnt.value),
+                     "peak_source": peak_kind},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse_args()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "ertm_device.cuh"
+#include "step_kernels.cuh"
 
 namespace ertm {
 
@@ -76,6 +77,21 @@ __global__ void k_setup_materials(DevProp* props, int pi, SetupArgs A) {
       C[CV_B0 + l][g] = __double2float_rn(__ddiv_rn(b, A.dt));
     }
   }
+}
+
+// Exhaustive check of divh() against __fdiv_rn for a fixed divisor h: all
+// 2^32 float inputs; mismatches are counted (NaNs compare equal to NaNs).
+__global__ void k_verify_division(float h, double r, unsigned long long* mismatches) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long bad = 0;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < (1ull << 32); k += stride) {
+    const float a = __uint_as_float((uint32_t)k);
+    const float q = divh(a, h, r, 1);
+    const float ref = __fdiv_rn(a, h);
+    const bool same = (__float_as_uint(q) == __float_as_uint(ref)) || (q != q && ref != ref);
+    bad += same ? 0ull : 1ull;
+  }
+  if (bad) atomicAdd(mismatches, bad);
 }
 
 // ---------------------------------------------------------------------------
@@ -160,9 +176,14 @@ __global__ void k_inject(const DevProp* props, int pi, InjectPlanDev plan, const
   *f = acc;
 }
 
-// Single-cell add (elastic force_z source lands on vz after the stress phase).
+// Single-cell add (elastic force_z source lands on vz after the stress phase,
+// propagation.py:872-873).
 __global__ void k_point_add(float* f, int64_t idx, float amp) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) f[idx] = fadd(f[idx], amp);
+  if (threadIdx.x == 0 && blockIdx.x == 0 && amp != 0.f) f[idx] = fadd(f[idx], amp);
+}
+__global__ void k_point_add_wave(float* f, int64_t idx, const float* wave, int t) {
+  const float amp = wave[t];
+  if (threadIdx.x == 0 && blockIdx.x == 0 && amp != 0.f) f[idx] = fadd(f[idx], amp);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,102 +218,26 @@ __global__ void k_image_field(const DevProp* props, int pi, int wave, int sep, f
 }
 
 // ---------------------------------------------------------------------------
-// imaging conditions (imaging.py:61-87, 279-331)
+// stand-alone epilogue: the imaging step when it cannot be fused into the
+// stress phase (after the compensated viscoacoustic stabilisation, or when a
+// force_z source lands on vz after the stress phase and divcurl is imaged)
 // ---------------------------------------------------------------------------
-// Accumulators: FP64 (reference-exact, default) or Kahan-compensated FP32
-// (sum, compensation) pairs stored in the same 8 bytes per cell.
-struct Accum {
-  double* d;    // FP64 mode
-  float* s;     // Kahan mode: running sum
-  float* comp;  // Kahan mode: compensation
-};
-
-template <bool KAHAN>
-__device__ __forceinline__ void acc_add(const Accum& a, size_t c, float term) {
-  if constexpr (!KAHAN) {
-    a.d[c] = dadd(a.d[c], (double)term);
-  } else {
-    const float y = fsub(term, a.comp[c]);
-    const float s = a.s[c];
-    const float t = fadd(s, y);
-    a.comp[c] = fsub(fsub(t, s), y);
-    a.s[c] = t;
-  }
-}
-
-constexpr int MAX_IMAGES = 4;
-struct ImagingArgs {
-  int32_t n_images;
-  int32_t illum;                  // accumulate S² and R² (normalized / receiver normalisation)
-  int32_t cross;                  // accumulate S·R (t ≥ start_step)
-  int32_t sep;
-  int32_t src_wave[MAX_IMAGES];   // which stored source field (slot index into src)
-  int32_t rcv_wave[MAX_IMAGES];
-  const float* src[2];            // replayed source image fields of this step (P, S slots)
-  Accum num[MAX_IMAGES];
-  Accum illum_acc[MAX_IMAGES];
-  Accum rillum_acc[MAX_IMAGES];
-};
-
-template <int M, bool KAHAN>
-__global__ void k_imaging(const DevProp* props, int back, ImagingArgs A) {
-  const DevProp& P = props[back];
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
-  const int ii = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ii >= P.nz || jj >= P.nx) return;
-  const size_t c = (size_t)ii * P.nx + jj;
-  float rv[2];
-  rv[0] = image_value<M>(P, WAVE_P, A.sep, ii + P.pad, jj + P.pad);
-  rv[1] = (P.engine == ENGINE_ELASTIC) ? image_value<M>(P, WAVE_S, A.sep, ii + P.pad, jj + P.pad) : 0.f;
-  for (int k = 0; k < A.n_images; ++k) {
-    const float s = A.src[A.src_wave[k]][c];
-    const float r = rv[A.rcv_wave[k]];
-    if (A.illum) {
-      acc_add<KAHAN>(A.illum_acc[k], c, fmul(s, s));
-      acc_add<KAHAN>(A.rillum_acc[k], c, fmul(r, r));
-    }
-    if (A.cross) acc_add<KAHAN>(A.num[k], c, fmul(s, r));
-  }
-}
-
-// Excitation map: running argmax of |P| over the replayed source field
-// (imaging.py:450-474).  running is stored in float32 (it only ever holds
-// |P| values, which float64 would store exactly too).
 template <int M>
-__global__ void k_excitation_track(const DevProp* props, int pi, int sep, float* running, int32_t* peak_step,
-                                   int step) {
+__global__ void k_epilogue(const DevProp* props, int pi, Epilogue E) {
   const DevProp& P = props[pi];
   const int jj = blockIdx.x * blockDim.x + threadIdx.x;
   const int ii = blockIdx.y * blockDim.y + threadIdx.y;
   if (ii >= P.nz || jj >= P.nx) return;
   const size_t c = (size_t)ii * P.nx + jj;
-  const float a = fabsf(image_value<M>(P, WAVE_P, sep, ii + P.pad, jj + P.pad));
-  if (a > running[c]) {
-    running[c] = a;
-    peak_step[c] = step;
-  }
+  const float pv = image_value<M>(P, WAVE_P, E.sep, ii + P.pad, jj + P.pad);
+  const float sv = (P.engine == ENGINE_ELASTIC && E.need_s) ? image_value<M>(P, WAVE_S, E.sep, ii + P.pad, jj + P.pad)
+                                                             : 0.f;
+  run_epilogue(E, c, (size_t)P.nz * P.nx, pv, sv);
 }
 
-// Excitation imaging at backward step t (imaging.py:290-303): where the
-// source peaked at t, num += A·R (float64 product) and rillum += R² (float32).
-template <int M>
-__global__ void k_excitation_image(const DevProp* props, int back, int sep, int n_images,
-                                   const int32_t* rcv_wave, const float* running, const int32_t* peak_step,
-                                   int step, Accum num0, Accum num1, Accum rill0, Accum rill1) {
-  const DevProp& P = props[back];
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
-  const int ii = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ii >= P.nz || jj >= P.nx) return;
-  const size_t c = (size_t)ii * P.nx + jj;
-  if (peak_step[c] != step) return;
-  const double a = (double)running[c];
-  for (int k = 0; k < n_images; ++k) {
-    const float r = image_value<M>(P, rcv_wave[k], sep, ii + P.pad, jj + P.pad);
-    const Accum& num = k == 0 ? num0 : num1;
-    const Accum& ril = k == 0 ? rill0 : rill1;
-    num.d[c] = dadd(num.d[c], dmul(a, (double)r));
-    ril.d[c] = dadd(ril.d[c], (double)fmul(r, r));
-  }
+__global__ void k_kahan_to_f64(const float* s, const float* c, double* out, int64_t n) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = (double)s[k] - (double)c[k];
 }
 
 // ---------------------------------------------------------------------------

@@ -8,10 +8,13 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -62,8 +65,64 @@ int32_t guarded(F&& f) {
   }
 }
 
-constexpr int TZ = 32;   // tile rows
-constexpr int BY = 8;    // warps per block (4 rows per thread)
+// Instrumentation: kernel launches issued by this library, and optional
+// CUDA-event timing of the stencil phases (every `every`-th step) on the
+// stream they run on.
+std::atomic<int64_t> g_launches{0};
+struct StencilProfile {
+  bool on = false;
+  int every = 8;
+  int64_t counter = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  std::vector<cudaEvent_t> pool;
+  double total_ms = 0.0;
+  int64_t samples = 0;
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    return e;
+  }
+  void drain() {
+    for (auto& pr : pending) {
+      float ms = 0.f;
+      CK(cudaEventSynchronize(pr.second));
+      CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      total_ms += ms;
+      ++samples;
+      pool.push_back(pr.first);
+      pool.push_back(pr.second);
+    }
+    pending.clear();
+  }
+};
+StencilProfile g_prof;
+
+// cuFFT plans for the image low-pass, cached by shape (and stream).
+struct FftPair {
+  cufftHandle fwd = 0, inv = 0;
+};
+std::map<std::tuple<int, int, cudaStream_t>, FftPair> g_fft_plans;
+std::mutex g_fft_mutex;
+
+FftPair image_fft(int nz, int nx, cudaStream_t st) {
+  std::lock_guard<std::mutex> lock(g_fft_mutex);
+  auto key = std::make_tuple(nz, nx, st);
+  auto it = g_fft_plans.find(key);
+  if (it != g_fft_plans.end()) return it->second;
+  FftPair p;
+  CKFFT(cufftPlan2d(&p.fwd, nz, nx, CUFFT_D2Z));
+  CKFFT(cufftPlan2d(&p.inv, nz, nx, CUFFT_Z2D));
+  CKFFT(cufftSetStream(p.fwd, st));
+  CKFFT(cufftSetStream(p.inv, st));
+  g_fft_plans[key] = p;
+  return p;
+}
+
 
 size_t round64(size_t n) { return (n + 63) / 64 * 64; }
 
@@ -144,7 +203,7 @@ struct Prop {
   size_t field_elems = 0, state_floats = 0;
   DevBuf state, coefs, prof, qidx, relax, peak, stab;
   int64_t step_index = 0;
-  int tiles_x = 0, tiles = 0;
+  int tiles_x = 0, tiles = 0, tz = 32;
   int lowpass_steps = 0;
   float k_src = 0.f;             // K_R at the source node (viscoacoustic)
   std::vector<double> rx, rz;
@@ -356,23 +415,86 @@ InjectPlanHost& inject_plan(Prop& P, const std::vector<int>& comps, int64_t nt) 
 // --------------------------------------------------------------------------
 // stepping
 // --------------------------------------------------------------------------
-template <int M>
-void launch_phases(const Prop& P, const WorkSet& ws, int blocks) {
-  const dim3 blk(TILE_X, BY);
-  switch (P.h.engine) {
+template <int M, int BZ, int R>
+void launch_step_shape(int engine, const DevProp* d, const WorkSet& ws, int blocks, cudaStream_t st) {
+  const dim3 blk(XT, BZ);
+  switch (engine) {
     case ENGINE_ACOUSTIC:
-      k_pressure_velocity<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
-      k_pressure_stress<M, TZ, BY, false><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      k_pressure_velocity<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
+      k_pressure_stress<M, BZ, R, false><<<blocks, blk, 0, st>>>(d, ws);
       break;
     case ENGINE_VISCO:
-      k_pressure_velocity<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
-      k_pressure_stress<M, TZ, BY, true><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      k_pressure_velocity<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
+      k_pressure_stress<M, BZ, R, true><<<blocks, blk, 0, st>>>(d, ws);
       break;
     default:
-      k_elastic_velocity<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
-      k_elastic_stress<M, TZ, BY><<<blocks, blk, 0, P.st>>>(P.dp(), ws);
+      k_elastic_velocity<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
+      k_elastic_stress<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
   }
 }
+
+// Both phases of one step for every work in ws (one tile height for all):
+// TZ 8 = 8×8 threads, 16 = 8×16 threads, 32 = 8×16 threads × 2 rows.
+void launch_step(int M, int tz, int engine, const DevProp* d, const WorkSet& ws, int blocks, cudaStream_t st) {
+  if (M == 4) {
+    if (tz == 32) launch_step_shape<4, 16, 2>(engine, d, ws, blocks, st);
+    else if (tz == 16) launch_step_shape<4, 16, 1>(engine, d, ws, blocks, st);
+    else launch_step_shape<4, 8, 1>(engine, d, ws, blocks, st);
+  } else if (M == 3) {
+    launch_step_shape<3, 16, 1>(engine, d, ws, blocks, st);
+  } else if (M == 2) {
+    launch_step_shape<2, 16, 1>(engine, d, ws, blocks, st);
+  } else {
+    launch_step_shape<1, 16, 1>(engine, d, ws, blocks, st);
+  }
+  g_launches += 2;
+}
+
+// Fast exact division by a grid spacing: verified once per float value of h
+// over all 2^32 inputs (k_verify_division), then cached for the process.
+std::map<uint32_t, bool> g_div_ok;
+std::mutex g_div_mutex;
+
+bool division_verified(float h, double r, cudaStream_t st) {
+  uint32_t key;
+  std::memcpy(&key, &h, 4);
+  {
+    std::lock_guard<std::mutex> lock(g_div_mutex);
+    auto it = g_div_ok.find(key);
+    if (it != g_div_ok.end()) return it->second;
+  }
+  DevBuf bad(8, st);
+  CK(cudaMemsetAsync(bad.p, 0, 8, st));
+  k_verify_division<<<148 * 8, 256, 0, st>>>(h, r, bad.as<unsigned long long>());
+  ++g_launches;
+  CK(cudaGetLastError());
+  unsigned long long n = 1;
+  CK(cudaMemcpyAsync(&n, bad.p, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::lock_guard<std::mutex> lock(g_div_mutex);
+  g_div_ok[key] = (n == 0);
+  return n == 0;
+}
+
+// Tile height for a launch: the tallest tile that still gives ≥ 4 blocks per
+// SM, unless the autotuner pinned one (ertm_set_tile_rows).
+std::atomic<int> g_tile_rows{0};
+int choose_tz(int M, int nxp, int64_t rows_total_tiles32, int64_t rows16, int64_t rows8) {
+  (void)nxp;
+  (void)rows8;
+  if (M != 4) return 16;
+  const int forced = g_tile_rows.load();
+  if (forced == 8 || forced == 16 || forced == 32) return forced;
+  const int64_t want = 148 * 4;
+  if (rows_total_tiles32 >= want) return 32;
+  if (rows16 >= want) return 16;
+  return 8;
+}
+
+int tiles_for(const DevProp& h, int tz) { return ((h.nxp + TILE_X - 1) / TILE_X) * ((h.nzp + tz - 1) / tz); }
+
+template <int M>
+void launch_epilogue_M(const Prop& P, const Epilogue& E);
 
 void lowpass_field(Prop& P, float* f, double cutoff) {
   const int nz = P.h.nzp, nx = P.h.nxp;
@@ -385,6 +507,7 @@ void lowpass_field(Prop& P, float* f, double cutoff) {
     P.fft_spec = DevBuf((size_t)nz * (nx / 2 + 1) * sizeof(double2), P.st);
   }
   const dim3 b2(32, 8), g2((nx + 31) / 32, (nz + 7) / 8), gh((nx / 2 + 1 + 31) / 32, (nz + 7) / 8);
+  g_launches += 5;  // conversion, D2Z, filter, Z2D, conversion
   k_f32_to_f64<<<g2, b2, 0, P.st>>>(f, P.h.ld, P.fft_real.as<double>(), nz, nx);
   CKFFT(cufftExecD2Z(P.fwd_plan, P.fft_real.as<double>(), P.fft_spec.as<cufftDoubleComplex>()));
   k_lowpass_apply<<<gh, b2, 0, P.st>>>(P.fft_spec.as<double2>(), nz, nx, P.cfg.dz, P.cfg.dx, cutoff);
@@ -392,31 +515,49 @@ void lowpass_field(Prop& P, float* f, double cutoff) {
   k_f64_to_f32<<<g2, b2, 0, P.st>>>(P.fft_real.as<double>(), f, P.h.ld, nz, nx);
 }
 
-void step_once(Prop& P, double amp64) {
+// One step of one propagator.  Amplitude: wavelet[t] from device memory when
+// `wave` is given, else amp64 (float32 for the field, float32(amp64/K_R) for
+// the viscoacoustic strain).  `epi` is fused into the stress phase.
+void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, const Epilogue* epi = nullptr) {
   StepWork w{};
   w.prop = 0;
   w.tile0 = 0;
   w.tiles_x = P.tiles_x;
   w.tiles = P.tiles;
-  // `if source_amplitude != 0.0` on the float64 value, then float32 adds
-  const float amp = amp64 != 0.0 ? (float)amp64 : 0.f;
-  w.amp = amp;
-  if (P.h.engine == ENGINE_VISCO && amp64 != 0.0)
-    w.amp_eps = (float)(amp64 / (double)P.k_src);  // propagation.py:710-712
+  w.wavelet = wave;
+  w.t = t;
+  if (!wave) {
+    // `if source_amplitude != 0.0` on the float64 value, then float32 adds
+    w.amp = amp64 != 0.0 ? (float)amp64 : 0.f;
+    if (P.h.engine == ENGINE_VISCO && amp64 != 0.0) w.amp_eps = (float)(amp64 / (double)P.k_src);
+  }
   const bool comp = P.h.engine == ENGINE_VISCO && P.cfg.compensation;
   w.flags = comp ? STEP_PEAK : 0;
+  if (epi) w.epi = *epi;
   WorkSet ws{nullptr, 0, w};
-  switch (P.M) {
-    case 1: launch_phases<1>(P, ws, P.tiles); break;
-    case 2: launch_phases<2>(P, ws, P.tiles); break;
-    case 3: launch_phases<3>(P, ws, P.tiles); break;
-    default: launch_phases<4>(P, ws, P.tiles); break;
+  const bool timed = g_prof.on && (g_prof.counter++ % g_prof.every == 0);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (timed) {
+    e0 = g_prof.get();
+    e1 = g_prof.get();
+    CK(cudaEventRecord(e0, P.st));
   }
-  if (P.h.engine == ENGINE_ELASTIC && P.h.mech == MECH_FORCE_Z && amp != 0.f && P.h.src_iz >= 0)
-    k_point_add<<<1, 32, 0, P.st>>>(P.field(E_VZ), (int64_t)P.h.src_iz * P.h.ld + P.h.src_ix, amp);
+  launch_step(P.M, P.tz, P.h.engine, P.dp(), ws, P.tiles, P.st);
+  if (timed) {
+    CK(cudaEventRecord(e1, P.st));
+    g_prof.pending.emplace_back(e0, e1);
+  }
+  const bool force_z = P.h.engine == ENGINE_ELASTIC && P.h.mech == MECH_FORCE_Z && P.h.src_iz >= 0;
+  if (force_z && (wave || amp64 != 0.0)) {
+    const int64_t idx = (int64_t)P.h.src_iz * P.h.ld + P.h.src_ix;
+    if (wave) k_point_add_wave<<<1, 32, 0, P.st>>>(P.field(E_VZ), idx, wave, t);
+    else k_point_add<<<1, 32, 0, P.st>>>(P.field(E_VZ), idx, (float)amp64);
+    ++g_launches;
+  }
   if (comp) {
     // propagation.py:726-749, evaluated with the step index before the increment
     const int64_t s = P.step_index;
+    ++g_launches;
     if (s < 30) {
       k_stab_reference<<<1, 32, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>());
     } else {
@@ -437,6 +578,7 @@ void step_once(Prop& P, double amp64) {
 
 void image_field(Prop& P, int wave, int sep, float* out) {
   const dim3 b2(32, 8), g2((P.h.nx + 31) / 32, (P.h.nz + 7) / 8);
+  ++g_launches;
   switch (P.M) {
     case 1: k_image_field<1><<<g2, b2, 0, P.st>>>(P.dp(), 0, wave, sep, out); break;
     case 2: k_image_field<2><<<g2, b2, 0, P.st>>>(P.dp(), 0, wave, sep, out); break;
@@ -475,6 +617,10 @@ Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, cons
   h.hx = (float)cfg->dx;
   h.hz = (float)cfg->dz;
   h.dt = (float)cfg->dt;
+  h.rx = 1.0 / (double)h.hx;   // IEEE double division on the host: RN64(1/hx)
+  h.rz = 1.0 / (double)h.hz;
+  h.fast_x = division_verified(h.hx, h.rx, P->st) ? 1 : 0;
+  h.fast_z = division_verified(h.hz, h.rz, P->st) ? 1 : 0;
   h.npx_l = cfg->npml_x_left;
   h.npx_r = cfg->npml_x_right;
   h.npz_t = cfg->npml_z_top;
@@ -564,8 +710,9 @@ Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, cons
   const dim3 b2(32, 8), g2((h.nxp + 31) / 32, (h.nzp + 7) / 8);
   k_setup_materials<<<g2, b2, 0, P->st>>>(P->dp(), 0, A);
   CK(cudaGetLastError());
+  P->tz = choose_tz(h.M, h.nxp, tiles_for(h, 32), tiles_for(h, 16), tiles_for(h, 8));
   P->tiles_x = (h.nxp + TILE_X - 1) / TILE_X;
-  P->tiles = P->tiles_x * ((h.nzp + TZ - 1) / TZ);
+  P->tiles = tiles_for(h, P->tz);
   CK(cudaStreamSynchronize(P->st));  // materials/tables staging buffers are freed next
   return P.release();
 }
@@ -574,43 +721,35 @@ Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, cons
 // migrate
 // --------------------------------------------------------------------------
 template <int M>
-void launch_imaging(const Prop& B, const ImagingArgs& A, bool kahan) {
-  const dim3 b2(32, 8), g2((B.h.nx + 31) / 32, (B.h.nz + 7) / 8);
-  if (kahan) k_imaging<M, true><<<g2, b2, 0, B.st>>>(B.dp(), 0, A);
-  else k_imaging<M, false><<<g2, b2, 0, B.st>>>(B.dp(), 0, A);
+void launch_epilogue_M(const Prop& P, const Epilogue& E) {
+  const dim3 b2(32, 8), g2((P.h.nx + 31) / 32, (P.h.nz + 7) / 8);
+  k_epilogue<M><<<g2, b2, 0, P.st>>>(P.dp(), 0, E);
 }
 
-template <int M>
-void launch_excitation_track(const Prop& F, int sep, float* running, int32_t* peak_step, int t) {
-  const dim3 b2(32, 8), g2((F.h.nx + 31) / 32, (F.h.nz + 7) / 8);
-  k_excitation_track<M><<<g2, b2, 0, F.st>>>(F.dp(), 0, sep, running, peak_step, t);
-}
-
-template <int M>
-void launch_excitation_image(const Prop& B, int sep, int n_images, const int32_t* rcv, const float* running,
-                             const int32_t* peak_step, int t, const Accum* num, const Accum* ril) {
-  const dim3 b2(32, 8), g2((B.h.nx + 31) / 32, (B.h.nz + 7) / 8);
-  k_excitation_image<M><<<g2, b2, 0, B.st>>>(B.dp(), 0, sep, n_images, rcv, running, peak_step, t, num[0],
-                                             num[n_images > 1 ? 1 : 0], ril[0], ril[n_images > 1 ? 1 : 0]);
-}
-
-__global__ void k_kahan_to_f64(const float* s, const float* c, double* out, int64_t n) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) out[k] = (double)s[k] - (double)c[k];
+void launch_epilogue(const Prop& P, const Epilogue& E) {
+  switch (P.M) {
+    case 1: launch_epilogue_M<1>(P, E); break;
+    case 2: launch_epilogue_M<2>(P, E); break;
+    case 3: launch_epilogue_M<3>(P, E); break;
+    default: launch_epilogue_M<4>(P, E); break;
+  }
+  ++g_launches;
 }
 
 void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wavelet, const float* record,
              double* num_out, double* illum_out, double* rillum_out) {
   REQUIRE(F.h.engine == B.h.engine && F.h.nz == B.h.nz && F.h.nx == B.h.nx, "fwd/back mismatch");
   REQUIRE(cfg.nt >= 1 && cfg.interval >= 1 && cfg.nt_spec >= 1, "bad nt/interval");
-  REQUIRE(cfg.n_images >= 1 && cfg.n_images <= MAX_IMAGES, "n_images must be 1..4");
+  REQUIRE(cfg.n_images >= 1 && cfg.n_images <= MAX_EPI_IMAGES, "n_images must be 1..2");
   REQUIRE(cfg.n_comp >= 0 && cfg.n_comp <= 8, "n_comp must be 0..8");
   REQUIRE(!B.rx.empty() || cfg.n_comp == 0, "receivers must be set on the backward propagator");
+  for (int k = 0; k < cfg.n_images; ++k)
+    REQUIRE((cfg.src_wave[k] == 0 || cfg.src_wave[k] == 1) && (cfg.rcv_wave[k] == 0 || cfg.rcv_wave[k] == 1) &&
+                (F.h.engine == ENGINE_ELASTIC || (cfg.src_wave[k] == 0 && cfg.rcv_wave[k] == 0)),
+            "wave not available for this engine");
   const bool excitation = cfg.condition == ERTM_COND_EXCITATION;
-  REQUIRE(!excitation || cfg.n_images <= 2, "excitation supports at most 2 images");
   cudaStream_t st = F.st;
   if (B.st != st) {
-    // keep the two propagators ordered on the forward stream
     CK(cudaStreamSynchronize(B.st));
     B.st = st;
   }
@@ -619,24 +758,21 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
   const size_t npix = (size_t)F.h.nz * F.h.nx;
   const int nimg = cfg.n_images;
   const bool kahan = cfg.accum == ERTM_ACCUM_KAHAN && !excitation;
+  const bool want_ill = (cfg.illumination & 1) && !excitation;
+  const bool want_ril = (cfg.illumination & 2) != 0;
   // accumulators
-  DevBuf acc(npix * nimg * 3 * 8, st);
+  DevBuf acc(npix * 8 * (2 * nimg + 2), st);
   CK(cudaMemsetAsync(acc.p, 0, acc.bytes, st));
-  Accum num[MAX_IMAGES]{}, ill[MAX_IMAGES]{}, ril[MAX_IMAGES]{};
+  double* num[MAX_EPI_IMAGES] = {};
+  double* ril[MAX_EPI_IMAGES] = {};
+  double* ill_slot[2] = {acc.as<double>() + 2 * nimg * npix, acc.as<double>() + (2 * nimg + 1) * npix};
   for (int k = 0; k < nimg; ++k) {
-    double* base = acc.as<double>() + (size_t)k * 3 * npix;
-    num[k].d = base;
-    ill[k].d = base + npix;
-    ril[k].d = base + 2 * npix;
-    if (kahan) {
-      // same 8 bytes per cell: (sum, compensation) float pairs
-      for (Accum* a : {&num[k], &ill[k], &ril[k]}) {
-        a->s = reinterpret_cast<float*>(a->d);
-        a->comp = a->s + npix;
-      }
-    }
+    num[k] = acc.as<double>() + k * npix;
+    ril[k] = acc.as<double>() + (nimg + k) * npix;
   }
-  // record + injection plan on the backward propagator
+  // wavelet on the device; record + injection plan on the backward propagator
+  DevBuf dwave((size_t)nt * 4, st);
+  upload(dwave.p, wavelet, (size_t)nt * 4, st);
   std::vector<int> comps(cfg.comp, cfg.comp + cfg.n_comp);
   const int64_t nrec = (int64_t)B.rx.size();
   DevBuf rec((size_t)cfg.n_comp * cfg.nt_spec * nrec * 4, st);
@@ -644,6 +780,7 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
   InjectPlanHost* plan = comps.empty() ? nullptr : &inject_plan(B, comps, cfg.nt_spec);
   auto inject = [&](int t) {
     if (!plan || plan->n_cells == 0) return;
+    ++g_launches;
     k_inject<<<(plan->n_cells + 127) / 128, 128, 0, st>>>(B.dp(), 0, plan->dev(), rec.as<float>(),
                                                           (int64_t)t * nrec);
   };
@@ -651,7 +788,7 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
   DevBuf ck((size_t)n_states * F.state_floats * 4, st);
   std::vector<int64_t> ck_step(n_states);
   for (int t = 0; t < nt; ++t) {
-    step_once(F, (double)wavelet[t]);
+    step_once(F, 0.0, dwave.as<float>(), t);
     if (t % iv == 0) {
       CK(cudaMemcpyAsync(ck.as<float>() + (size_t)(t / iv) * F.state_floats, F.state.p, F.state_floats * 4,
                          cudaMemcpyDeviceToDevice, st));
@@ -663,97 +800,125 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
                        cudaMemcpyDeviceToDevice, st));
     F.step_index = ck_step[b];
   };
-  const int M = F.M;
-  if (!excitation) {
-    bool need[2] = {false, false};
-    for (int k = 0; k < nimg; ++k) need[cfg.src_wave[k]] = true;
-    DevBuf rbuf((size_t)iv * 2 * npix * 4, st);
-    ImagingArgs A{};
-    A.n_images = nimg;
-    A.illum = cfg.illumination;
-    A.sep = cfg.separation;
-    for (int k = 0; k < nimg; ++k) {
-      A.src_wave[k] = cfg.src_wave[k];
-      A.rcv_wave[k] = cfg.rcv_wave[k];
-      A.num[k] = num[k];
-      A.illum_acc[k] = ill[k];
-      A.rillum_acc[k] = ril[k];
+  // epilogue templates
+  Epilogue base{};
+  base.sep = cfg.separation;
+  base.n_images = nimg;
+  base.kahan = kahan ? 1 : 0;
+  bool need_src[2] = {false, false}, need_rcv_s = false;
+  for (int k = 0; k < nimg; ++k) {
+    base.src_slot[k] = cfg.src_wave[k];
+    base.rcv_wave[k] = cfg.rcv_wave[k];
+    base.num[k] = num[k];
+    base.ril[k] = want_ril ? ril[k] : nullptr;
+    need_src[cfg.src_wave[k]] = true;
+    need_rcv_s |= cfg.rcv_wave[k] == 1;
+  }
+  // each distinct source wave's illumination is accumulated once
+  for (int k = 0; k < nimg; ++k) {
+    bool first = true;
+    for (int q = 0; q < k; ++q) first &= cfg.src_wave[q] != cfg.src_wave[k];
+    base.ill[k] = (want_ill && first) ? ill_slot[cfg.src_wave[k]] : nullptr;
+  }
+  // The fused epilogue sees the fields right after the stress phase; it is
+  // run stand-alone when something still changes them afterwards.
+  const bool bwd_unfused = B.h.engine == ENGINE_VISCO && B.cfg.compensation;
+  const bool fwd_force_z = F.h.engine == ENGINE_ELASTIC && F.h.mech == MECH_FORCE_Z && cfg.separation == 1;
+  auto fwd_step = [&](int t, const Epilogue& e) {
+    if (fwd_force_z) {
+      step_once(F, 0.0, dwave.as<float>(), t);
+      launch_epilogue(F, e);
+    } else {
+      step_once(F, 0.0, dwave.as<float>(), t, &e);
     }
+  };
+  auto bwd_step = [&](const Epilogue& e) {
+    if (e.kind == EPI_NONE) {
+      step_once(B, 0.0);
+    } else if (bwd_unfused) {
+      step_once(B, 0.0);
+      launch_epilogue(B, e);
+    } else {
+      step_once(B, 0.0, nullptr, 0, &e);
+    }
+  };
+  if (!excitation) {
+    DevBuf rbuf((size_t)iv * 2 * npix * 4, st);
+    Epilogue store = base;
+    store.kind = EPI_STORE;
+    store.need_s = need_src[1] ? 1 : 0;
+    Epilogue image = base;
+    image.kind = EPI_IMAGE;
+    image.need_s = need_rcv_s ? 1 : 0;
+    image.illum = want_ill ? 1 : 0;
+    image.rillum = want_ril ? 1 : 0;
     for (int b = n_states - 1; b >= 0; --b) {
       const int s0 = b * iv, e0 = std::min((b + 1) * iv, nt);
       restore(b);
       for (int t = s0; t < e0; ++t) {
-        step_once(F, (double)wavelet[t]);
         float* slot = rbuf.as<float>() + (size_t)(t - s0) * 2 * npix;
-        for (int w = 0; w < 2; ++w)
-          if (need[w]) image_field(F, w, cfg.separation, slot + w * npix);
+        store.out[0] = need_src[0] ? slot : nullptr;
+        store.out[1] = need_src[1] ? slot + npix : nullptr;
+        fwd_step(t, store);
       }
       for (int t = e0 - 1; t >= s0; --t) {
         inject(t);
-        step_once(B, 0.0);
         const float* slot = rbuf.as<float>() + (size_t)(t - s0) * 2 * npix;
-        A.src[0] = slot;
-        A.src[1] = slot + npix;
-        A.cross = t >= cfg.start_step ? 1 : 0;
-        if (!A.cross && !A.illum) continue;
-        switch (M) {
-          case 1: launch_imaging<1>(B, A, kahan); break;
-          case 2: launch_imaging<2>(B, A, kahan); break;
-          case 3: launch_imaging<3>(B, A, kahan); break;
-          default: launch_imaging<4>(B, A, kahan); break;
-        }
+        image.src[0] = slot;
+        image.src[1] = slot + npix;
+        image.cross = t >= cfg.start_step ? 1 : 0;
+        Epilogue e = image;
+        if (!e.cross && !e.illum && !e.rillum) e.kind = EPI_NONE;
+        bwd_step(e);
       }
     }
   } else {
-    DevBuf running(npix * 4, st), peak((size_t)npix * 4, st), rcvw(16, st);
+    DevBuf running(npix * 4, st), peak((size_t)npix * 4, st);
     CK(cudaMemsetAsync(running.p, 0, npix * 4, st));
     CK(cudaMemsetAsync(peak.p, 0xff, npix * 4, st));  // −1
-    upload(rcvw.p, cfg.rcv_wave, sizeof(int32_t) * 4, st);
+    Epilogue track = base;
+    track.kind = EPI_EXC_TRACK;
+    track.running = running.as<float>();
+    track.peak_step = peak.as<int32_t>();
+    Epilogue image = track;
+    image.kind = EPI_EXC_IMAGE;
+    image.need_s = need_rcv_s ? 1 : 0;
     for (int b = 0; b < n_states; ++b) {
       const int s0 = b * iv, e0 = std::min((b + 1) * iv, nt);
       restore(b);
       for (int t = s0; t < e0; ++t) {
-        step_once(F, (double)wavelet[t]);
-        switch (M) {
-          case 1: launch_excitation_track<1>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
-          case 2: launch_excitation_track<2>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
-          case 3: launch_excitation_track<3>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
-          default: launch_excitation_track<4>(F, cfg.separation, running.as<float>(), peak.as<int32_t>(), t); break;
-        }
+        track.step = t;
+        fwd_step(t, track);
       }
     }
     for (int b = n_states - 1; b >= 0; --b) {
       const int s0 = b * iv, e0 = (b + 1 < n_states) ? (b + 1) * iv : cfg.nt_spec;
       for (int t = e0 - 1; t >= s0; --t) {
         inject(t);
-        step_once(B, 0.0);
-        if (t < cfg.start_step) continue;
-        switch (M) {
-          case 1: launch_excitation_image<1>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
-          case 2: launch_excitation_image<2>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
-          case 3: launch_excitation_image<3>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
-          default: launch_excitation_image<4>(B, cfg.separation, nimg, rcvw.as<int32_t>(), running.as<float>(), peak.as<int32_t>(), t, num, ril); break;
-        }
+        Epilogue e = image;
+        e.step = t;
+        if (t < cfg.start_step) e.kind = EPI_NONE;
+        bwd_step(e);
       }
     }
-    // illumination = A² is computed but never used by this condition (imaging.py:304, 328)
+    // illumination = A² is set but never used by this condition (imaging.py:304, 328)
   }
   CK(cudaGetLastError());
   // outputs: per image, num/illum/rillum as float64
   DevBuf tmp(kahan ? npix * 8 : 0, st);
-  for (int k = 0; k < nimg; ++k) {
-    double* outs[3] = {num_out, illum_out, rillum_out};
-    Accum* srcs[3] = {&num[k], &ill[k], &ril[k]};
-    for (int q = 0; q < 3; ++q) {
-      if (!outs[q]) continue;
-      const double* from = srcs[q]->d;
-      if (kahan) {
-        k_kahan_to_f64<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(srcs[q]->s, srcs[q]->comp, tmp.as<double>(),
-                                                                    (int64_t)npix);
-        from = tmp.as<double>();
-      }
-      CK(cudaMemcpyAsync(outs[q] + (size_t)k * npix, from, npix * 8, cudaMemcpyDefault, st));
+  auto out = [&](double* dst, const double* src) {
+    const double* from = src;
+    if (kahan) {
+      const float* s = reinterpret_cast<const float*>(src);
+      k_kahan_to_f64<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(s, s + npix, tmp.as<double>(), (int64_t)npix);
+      from = tmp.as<double>();
     }
+    CK(cudaMemcpyAsync(dst, from, npix * 8, cudaMemcpyDefault, st));
+  };
+  for (int k = 0; k < nimg; ++k) {
+    if (num_out) out(num_out + (size_t)k * npix, num[k]);
+    if (illum_out) out(illum_out + (size_t)k * npix, ill_slot[cfg.src_wave[k]]);
+    if (rillum_out) out(rillum_out + (size_t)k * npix, ril[k]);
   }
   CK(cudaStreamSynchronize(st));
 }
@@ -769,12 +934,46 @@ const char* ertm_last_error(void) { return g_error.c_str(); }
 
 int32_t ertm_version(void) { return 1; }
 
+int64_t ertm_launch_count(void) { return g_launches.load(); }
+
+int32_t ertm_set_tile_rows(int32_t rows) {
+  return guarded([&] {
+    REQUIRE(rows == 0 || rows == 8 || rows == 16 || rows == 32, "tile rows must be 0 (auto), 8, 16 or 32");
+    g_tile_rows = rows;
+  });
+}
+
+int32_t ertm_profile_stencil(int32_t enable, int32_t every) {
+  return guarded([&] {
+    g_prof.drain();
+    g_prof.on = enable != 0;
+    g_prof.every = every > 0 ? every : 1;
+    g_prof.counter = 0;
+    g_prof.total_ms = 0.0;
+    g_prof.samples = 0;
+  });
+}
+
+int32_t ertm_profile_read(double* total_ms, int64_t* samples) {
+  return guarded([&] {
+    REQUIRE(total_ms && samples, "null argument");
+    g_prof.drain();
+    *total_ms = g_prof.total_ms;
+    *samples = g_prof.samples;
+  });
+}
+
 int32_t ertm_init(int32_t device) {
   return guarded([&] {
     int n = 0;
     CK(cudaGetDeviceCount(&n));
     REQUIRE(device >= 0 && device < n, "no such CUDA device");
     CK(cudaSetDevice(device));
+    // keep freed stream-ordered allocations in the pool between calls
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     cudaDeviceProp prop{};
     CK(cudaGetDeviceProperties(&prop, device));
     REQUIRE(prop.major == 10, "this library is built for sm_100a (B200); found sm_" +
@@ -817,6 +1016,9 @@ int32_t ertm_prop_info_get(void* prop, ertm_prop_info* info) {
     info->clipped = s.clipped;
     info->lowpass_steps = P.lowpass_steps;
     info->n_receivers = (int32_t)P.rx.size();
+    info->fast_div_x = P.h.fast_x;
+    info->fast_div_z = P.h.fast_z;
+    info->tile_rows = P.tz;
   });
 }
 
@@ -1042,9 +1244,15 @@ int32_t ertm_forward(void* prop, int32_t nt, const float* amps, int32_t n_comp, 
                                   sp.w.as<double>(), o.as<float>() + (size_t)c * nt * n};
       }
     }
+    DevBuf dwave(amps ? (size_t)nt * 4 : 0, P.st);
+    if (amps) upload(dwave.p, amps, (size_t)nt * 4, P.st);
     for (int t = 0; t < nt; ++t) {
-      step_once(P, amps ? (double)amps[t] : 0.0);
-      if (sampling) k_sample<<<dim3((n + 127) / 128, n_comp), 128, 0, P.st>>>(P.dp(), 0, S, (int64_t)t * n);
+      if (amps) step_once(P, 0.0, dwave.as<float>(), t);
+      else step_once(P, 0.0);
+      if (sampling) {
+        k_sample<<<dim3((n + 127) / 128, n_comp), 128, 0, P.st>>>(P.dp(), 0, S, (int64_t)t * n);
+        ++g_launches;
+      }
     }
     CK(cudaGetLastError());
     if (sampling) CK(cudaMemcpyAsync(out, o.p, o.bytes, cudaMemcpyDefault, P.st));
@@ -1093,21 +1301,16 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
       k_laplacian<<<g2, b2, 0, st>>>(cur, other, nz, nx, dx, dz);
       std::swap(cur, other);
     }
-    cufftHandle pf = 0, pi = 0;
+    g_launches += 2 + (laplacian ? 1 : 0);
     if (lowpass < 1.0) {
       DevBuf spec((size_t)nz * (nx / 2 + 1) * 16, st);
-      CKFFT(cufftPlan2d(&pf, nz, nx, CUFFT_D2Z));
-      CKFFT(cufftPlan2d(&pi, nz, nx, CUFFT_Z2D));
-      CKFFT(cufftSetStream(pf, st));
-      CKFFT(cufftSetStream(pi, st));
-      CKFFT(cufftExecD2Z(pf, cur, spec.as<cufftDoubleComplex>()));
+      const FftPair fp = image_fft(nz, nx, st);
+      CKFFT(cufftExecD2Z(fp.fwd, cur, spec.as<cufftDoubleComplex>()));
       const dim3 gh((nx / 2 + 1 + 31) / 32, (nz + 7) / 8);
       k_lowpass_apply<<<gh, b2, 0, st>>>(spec.as<double2>(), nz, nx, dz, dx, lowpass);
-      CKFFT(cufftExecZ2D(pi, spec.as<cufftDoubleComplex>(), other));
+      ++g_launches;
+      CKFFT(cufftExecZ2D(fp.inv, spec.as<cufftDoubleComplex>(), other));
       std::swap(cur, other);
-      CK(cudaStreamSynchronize(st));
-      cufftDestroy(pf);
-      cufftDestroy(pi);
     }
     k_mask_cast<<<g2, b2, 0, st>>>(cur, o.as<float>(), nz, nx, npml, top_mask);
     CK(cudaGetLastError());

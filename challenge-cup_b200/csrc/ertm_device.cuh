@@ -51,6 +51,8 @@ struct DevProp {
   int32_t n_fields;
   float c[4];           // float32 stencil coefficients (unused ones = 0)
   float hx, hz, dt;     // float32 spacing and time step
+  double rx, rz;        // RN64(1/hx), RN64(1/hz) for the verified fast division
+  int32_t fast_x, fast_z;  // 1: divh() by hx / hz was verified equal to __fdiv_rn for all inputs
   int32_t npx_l, npx_r; // x-strip widths (0 when absent)
   int32_t npz_t, npz_b; // z-strip widths (top is 0 under a free surface)
   int32_t wx;           // npx_l + npx_r
@@ -68,16 +70,50 @@ struct DevProp {
   float* peak;                        // visco compensation: max|p| of the last step (float bits)
 };
 
+// What the stress phase does with the finished fields of each physical cell
+// (fused so the image fields are never re-read from HBM).
+enum EpilogueKind : int32_t {
+  EPI_NONE = 0,
+  EPI_STORE = 1,       // write the P (and S) image fields to out[] (replay)
+  EPI_IMAGE = 2,       // imaging condition against stored source fields (backward)
+  EPI_EXC_TRACK = 3,   // excitation map: running argmax |P| (replay)
+  EPI_EXC_IMAGE = 4,   // excitation imaging at this step (backward)
+};
+
+constexpr int MAX_EPI_IMAGES = 2;
+
+struct Epilogue {
+  int32_t kind;
+  int32_t sep;                       // 0 stress, 1 divcurl (elastic)
+  int32_t need_s;                    // S is needed (elastic)
+  int32_t n_images;
+  int32_t src_slot[MAX_EPI_IMAGES];  // stored source field per image (0 P, 1 S)
+  int32_t rcv_wave[MAX_EPI_IMAGES];  // receiver wave per image (0 P, 1 S)
+  int32_t cross, illum, rillum;      // which sums to accumulate at this step
+  int32_t kahan;                     // accumulators are Kahan float pairs
+  int32_t step;                      // time label (excitation)
+  int32_t pad_;
+  float* out[2];                     // EPI_STORE destinations (P, S), (nz, nx)
+  const float* src[2];               // EPI_IMAGE stored source fields (P, S)
+  double* num[MAX_EPI_IMAGES];       // FP64 accumulators, (nz, nx); Kahan: float pairs
+  double* ill[MAX_EPI_IMAGES];       // source illumination S² (nullptr: shared with image 0 / unused)
+  double* ril[MAX_EPI_IMAGES];       // receiver illumination R² (nullptr: unused)
+  float* running;                    // excitation |P| running max
+  int32_t* peak_step;                // excitation argmax step
+};
+
 // One propagator advance inside a (possibly batched) launch.
 struct StepWork {
-  int32_t prop;       // index into the DevProp table
-  int32_t tile0;      // first block of this work in the launch
-  int32_t tiles_x;    // tiles along x for this propagator
-  int32_t tiles;      // total tiles for this propagator
-  float amp;          // source amplitude at this step (0: none)
-  float amp_eps;      // visco: float32(amp / K_R at the source)
-  int32_t flags;      // STEP_* bits
-  int32_t pad_;
+  int32_t prop;         // index into the DevProp table
+  int32_t tile0;        // first block of this work in the launch
+  int32_t tiles_x;      // tiles along x for this propagator
+  int32_t tiles;        // total tiles for this propagator
+  const float* wavelet; // source time series (device); nullptr → use amp/amp_eps
+  int32_t t;            // index into wavelet
+  float amp;            // source amplitude (when wavelet == nullptr)
+  float amp_eps;        // viscoacoustic strain amplitude (when wavelet == nullptr)
+  int32_t flags;        // STEP_* bits
+  Epilogue epi;
 };
 constexpr int STEP_PEAK = 1;        // visco: reduce max|p| into DevProp::peak
 
@@ -118,6 +154,17 @@ __device__ __forceinline__ float dminus(const float* s, int stride, const float*
   for (int k = 2; k <= M; ++k)
     acc = fadd(acc, fmul(c[k - 1], fsub(s[(k - 1) * stride], s[-k * stride])));
   return fdiv(acc, h);
+}
+
+// a / h rounded to nearest.  Fast form: float32(RN64(double(a) · R)) with
+// R = RN64(1/h): the float64 product is within 2^-52 relative of a/h, so the
+// single rounding to float32 matches RN32(a/h) unless a/h lies that close to
+// a float32 rounding midpoint.  Whether that ever happens for a given h is
+// decided by the host, which compares this form with __fdiv_rn(a, h) for all
+// 2^32 float inputs a (k_verify_division) and only then sets `fast`.
+__device__ __forceinline__ float divh(float a, float h, double r64, int fast) {
+  if (fast) return __double2float_rn(__dmul_rn((double)a, r64));
+  return __fdiv_rn(a, h);
 }
 
 // CPML memory update and corrected derivative: ψ ← ψ·b + a·D; return D + ψ

@@ -3,17 +3,22 @@
 // One time step of a propagator is two launches: the velocity phase (reads
 // the stresses with a halo, updates vx, vz and their ψ strips in place) and
 // the stress phase (reads the new velocities with a halo, updates the
-// stresses, injects the source, applies the free surface).  Each block owns
-// a 32-column × TZ-row tile of one propagator; the staged fields are copied
-// to shared memory with an M-cell halo on all sides, the per-cell
-// coefficients and the field being updated are read straight from HBM with
-// coalesced 128-byte warp accesses.  A launch may carry many propagators
-// (the batched form): the block finds its propagator by binary search over
-// the StepWork table.
+// stresses, injects the source, applies the free surface, then runs the
+// fused epilogue: image-field store, imaging condition or excitation map).
+// Each block owns a 32-column × TZ-row tile of one propagator and runs
+// 8 × BZ threads; a thread owns 4 adjacent columns (one float4) of R rows
+// (TZ = BZ·R).  The staged fields go to shared memory with an M-cell halo by
+// 16-byte cp.async; x-stencils read three 128-bit words per row, z-stencils
+// one 128-bit word per row offset; per-cell coefficients and the updated
+// fields move as float4 with coalesced 128-byte warp accesses.  TZ (8, 16 or
+// 32) is picked per launch so the grid fills the 148 SMs.  A launch may carry many
+// propagators (the batched form): a block finds its propagator by binary
+// search over the StepWork table.
 //
 // Arithmetic order follows ertm/propagation.py (acoustic :430-454,
-// viscoacoustic :686-723, elastic :840-883) and ertm/numerics.py (:68-117,
-// :221-227) so the fields match the reference float32 fields bit for bit.
+// viscoacoustic :686-723, elastic :840-883), ertm/numerics.py (:68-117,
+// :221-227) and ertm/imaging.py (:305-324) so fields and image sums match the
+// reference bit for bit.
 #pragma once
 
 #include "ertm_device.cuh"
@@ -21,30 +26,45 @@
 namespace ertm {
 
 constexpr int TILE_X = 32;
+constexpr int XT = 8;   // threads across a tile (4 columns each)
 
+// Shared-memory tile of one staged field: rows [i0−M, i0+TZ+M), columns
+// [j0−4, j0+36) — 40 floats per row for every order, so each row is ten
+// 16-byte chunks aligned like the global rows (j0 is a multiple of 32, the
+// row pitch a multiple of 32 floats).  Column j of the tile sits at OFF + j−j0.
 template <int M, int TZ>
 struct TileShape {
-  static constexpr int W = TILE_X + 2 * M;
+  static constexpr int W = TILE_X + 8;
+  static constexpr int OFF = 4;
   static constexpr int H = TZ + 2 * M;
   static constexpr int N = W * H;
+  static constexpr int CHUNKS = H * (W / 4);
 };
 
-// Copy rows [i0−M, i0+TZ+M) × cols [j0−M, j0+32+M) of a padded field into
-// shared memory; cells outside the padded grid read as 0 (never used by a
-// valid stencil, which stays inside [0, n)).
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, bool valid) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int src_size = valid ? 16 : 0;   // 0 → zero-fill, nothing is read
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_size) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Issue the asynchronous copy of one field tile; rows outside [0, nzp) and
+// chunks outside [0, ld) are zero-filled (a valid stencil never reads them;
+// columns in [nxp, ld) are the row padding, which stays zero).
 template <int M, int TZ, int NT>
-__device__ __forceinline__ void stage(float* s, const float* __restrict__ g, int nzp, int nxp, int ld,
-                                      int i0, int j0) {
+__device__ __forceinline__ void stage(float* s, const float* __restrict__ g, int nzp, int ld, int i0, int j0) {
   using T = TileShape<M, TZ>;
-  const int tid = threadIdx.y * TILE_X + threadIdx.x;
-#pragma unroll 4
-  for (int idx = tid; idx < T::N; idx += NT) {
-    const int r = idx / T::W;
-    const int c = idx - r * T::W;
-    const int gi = i0 - M + r, gj = j0 - M + c;
-    float v = 0.f;
-    if (gi >= 0 && gi < nzp && gj >= 0 && gj < nxp) v = __ldg(g + (size_t)gi * ld + gj);
-    s[idx] = v;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (T::CHUNKS + NT - 1) / NT; ++it) {
+    const int idx = tid + it * NT;
+    if (T::CHUNKS % NT != 0 && idx >= T::CHUNKS) break;
+    const int r = idx / (T::W / 4);
+    const int ch = idx - r * (T::W / 4);
+    const int gi = i0 - M + r, gj = j0 - T::OFF + 4 * ch;
+    const bool ok = gi >= 0 && gi < nzp && gj >= 0 && gj < ld;
+    cp_async16(s + r * T::W + 4 * ch, ok ? g + (size_t)gi * ld + gj : g, ok);
   }
 }
 
@@ -58,122 +78,384 @@ __device__ __forceinline__ TileLoc tile_of(const StepWork& w, int block, int tz)
   return {ti * tz, (t - ti * w.tiles_x) * TILE_X};
 }
 
+// Source amplitudes of this step: float32(amp) for the field and, for the
+// viscoacoustic strain, float32(amp / K_R) computed in float64
+// (propagation.py:707-713).
+__device__ __forceinline__ void source_amps(const StepWork& w, const DevProp& P, float& amp, float& amp_eps) {
+  if (w.wavelet == nullptr) {
+    amp = w.amp;
+    amp_eps = w.amp_eps;
+    return;
+  }
+  amp = w.wavelet[w.t];
+  amp_eps = 0.f;
+  if (P.engine == ENGINE_VISCO && amp != 0.f && P.src_iz >= 0) {
+    const float kr = P.coef[CV_KR][(size_t)P.src_iz * P.ld + P.src_ix];
+    amp_eps = __double2float_rn(__ddiv_rn((double)amp, (double)kr));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fused epilogue on one physical cell
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void acc_term(double* base, int kahan, size_t c, size_t npix, float term) {
+  if (!kahan) {
+    base[c] = dadd(base[c], (double)term);
+  } else {
+    float* s = reinterpret_cast<float*>(base);
+    float* comp = s + npix;
+    const float y = fsub(term, comp[c]);
+    const float sv = s[c];
+    const float t = fadd(sv, y);
+    comp[c] = fsub(fsub(t, sv), y);
+    s[c] = t;
+  }
+}
+
+__device__ __forceinline__ void run_epilogue(const Epilogue& E, size_t c, size_t npix, float pv, float sv) {
+  switch (E.kind) {
+    case EPI_STORE:
+      if (E.out[0]) E.out[0][c] = pv;
+      if (E.out[1]) E.out[1][c] = sv;
+      break;
+    case EPI_IMAGE: {
+      // imaging.py:313-324: illum += S², rillum += R² (all steps); num += S·R (t ≥ start)
+      const float s0 = E.src[0] ? E.src[0][c] : 0.f;
+      const float s1 = E.src[1] ? E.src[1][c] : 0.f;
+#pragma unroll
+      for (int k = 0; k < MAX_EPI_IMAGES; ++k) {
+        if (k >= E.n_images) break;
+        const float s = E.src_slot[k] ? s1 : s0;
+        const float r = E.rcv_wave[k] ? sv : pv;
+        if (E.illum && E.ill[k]) acc_term(E.ill[k], E.kahan, c, npix, fmul(s, s));
+        if (E.rillum && E.ril[k]) acc_term(E.ril[k], E.kahan, c, npix, fmul(r, r));
+        if (E.cross) acc_term(E.num[k], E.kahan, c, npix, fmul(s, r));
+      }
+      break;
+    }
+    case EPI_EXC_TRACK: {
+      // imaging.py:466-473: strict '>' against the running |P| maximum
+      const float a = fabsf(pv);
+      if (a > E.running[c]) {
+        E.running[c] = a;
+        E.peak_step[c] = E.step;
+      }
+      break;
+    }
+    case EPI_EXC_IMAGE: {
+      // imaging.py:295-303: num += A·R in float64, rillum += R² (float32 square)
+      if (E.peak_step[c] != E.step) break;
+      const double a = (double)E.running[c];
+#pragma unroll
+      for (int k = 0; k < MAX_EPI_IMAGES; ++k) {
+        if (k >= E.n_images) break;
+        const float r = E.rcv_wave[k] ? sv : pv;
+        E.num[k][c] = dadd(E.num[k][c], dmul(a, (double)r));
+        if (E.ril[k]) E.ril[k][c] = dadd(E.ril[k][c], (double)fmul(r, r));
+      }
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// Scalars and pointers of one propagator, loaded once into registers at the
+// top of a kernel (the kernels store through float pointers, so reading the
+// DevProp in global memory after a store would force a reload).
+struct Geo {
+  int nzp, nxp, ld, wx, npx_l, npx_r, npz_t, npz_b, pad, nz, nx, src_iz, src_ix, free_surface, fast_x, fast_z;
+  float c[4];
+  float dt, hx, hz;
+  double rx, rz;
+  __device__ __forceinline__ explicit Geo(const DevProp& P)
+      : nzp(P.nzp), nxp(P.nxp), ld(P.ld), wx(P.wx), npx_l(P.npx_l), npx_r(P.npx_r), npz_t(P.npz_t),
+        npz_b(P.npz_b), pad(P.pad), nz(P.nz), nx(P.nx), src_iz(P.src_iz), src_ix(P.src_ix),
+        free_surface(P.free_surface), fast_x(P.fast_x), fast_z(P.fast_z), c{P.c[0], P.c[1], P.c[2], P.c[3]},
+        dt(P.dt), hx(P.hx), hz(P.hz), rx(P.rx), rz(P.rz) {}
+  __device__ __forceinline__ float dx_(float a) const { return divh(a, hx, rx, fast_x); }
+  __device__ __forceinline__ float dz_(float a) const { return divh(a, hz, rz, fast_z); }
+  __device__ __forceinline__ int sx(int j) const {
+    if (j < npx_l) return j;
+    if (j >= nxp - npx_r) return npx_l + (j - (nxp - npx_r));
+    return -1;
+  }
+  __device__ __forceinline__ int sz(int i) const {
+    if (i < npz_t) return i;
+    if (i >= nzp - npz_b) return npz_t + (i - (nzp - npz_b));
+    return -1;
+  }
+  __device__ __forceinline__ bool physical(int i, int j, size_t& c) const {
+    const int ii = i - pad, jj = j - pad;
+    if (ii < 0 || ii >= nz || jj < 0 || jj >= nx) return false;
+    c = (size_t)ii * nx + jj;
+    return true;
+  }
+};
+
+__device__ __forceinline__ bool physical(const DevProp& P, int i, int j, size_t& c) {
+  const int ii = i - P.pad, jj = j - P.pad;
+  if (ii < 0 || ii >= P.nz || jj < 0 || jj >= P.nx) return false;
+  c = (size_t)ii * P.nx + jj;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// register stencils on 4 adjacent columns
+// ---------------------------------------------------------------------------
+// Twelve consecutive values of one staged row, columns j−4 … j+7 of the
+// thread's first column j (shared-memory column 4·tx … 4·tx+11).
+__device__ __forceinline__ void row12(const float* p, float v[12]) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  const float4 b = *reinterpret_cast<const float4*>(p + 4);
+  const float4 c = *reinterpret_cast<const float4*>(p + 8);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  v[8] = c.x; v[9] = c.y; v[10] = c.z; v[11] = c.w;
+}
+
+// Column c (0..3) of rows −M … +M around the thread's row: z[c][M+k] = f[i+k].
+template <int M>
+__device__ __forceinline__ void col9(const float* p /* row i, column j */, float z[4][2 * M + 1]) {
+#pragma unroll
+  for (int k = 0; k <= 2 * M; ++k) {
+    const float4 q = *reinterpret_cast<const float4*>(p + (k - M) * 40);
+    z[0][k] = q.x; z[1][k] = q.y; z[2][k] = q.z; z[3][k] = q.w;
+  }
+}
+
+// Σ_k c_k (f[o+k] − f[o−k+1]) (D⁺ numerator) on an array with static indices.
+template <int M>
+__device__ __forceinline__ float sum_plus(const float* f, int o, const float* c) {
+  float acc = fmul(c[0], fsub(f[o + 1], f[o]));
+#pragma unroll
+  for (int k = 2; k <= M; ++k) acc = fadd(acc, fmul(c[k - 1], fsub(f[o + k], f[o - k + 1])));
+  return acc;
+}
+// Σ_k c_k (f[o+k−1] − f[o−k]) (D⁻ numerator).
+template <int M>
+__device__ __forceinline__ float sum_minus(const float* f, int o, const float* c) {
+  float acc = fmul(c[0], fsub(f[o], f[o - 1]));
+#pragma unroll
+  for (int k = 2; k <= M; ++k) acc = fadd(acc, fmul(c[k - 1], fsub(f[o + k - 1], f[o - k])));
+  return acc;
+}
+
+__device__ __forceinline__ float comp(const float4& v, int c) {
+  return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_comp(float4& v, int c, float x) {
+  if (c == 0) v.x = x; else if (c == 1) v.y = x; else if (c == 2) v.z = x; else v.w = x;
+}
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void st4(float* p, const float4& v) { *reinterpret_cast<float4*>(p) = v; }
+
+// Per-column x information for the thread's 4 columns.
+struct ColInfo {
+  bool xin[4];   // x-stencil inside [M, nxp − M)
+  bool ok[4];    // column inside the padded grid
+  int sx[4];     // x-strip index or −1
+  float ax[4], bx[4];
+};
+template <int M>
+__device__ __forceinline__ ColInfo col_info(const Geo& G, int j, const float* axp, const float* bxp) {
+  ColInfo C;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int jc = j + c;
+    C.ok[c] = jc < G.nxp;
+    C.xin[c] = jc >= M && jc < G.nxp - M;
+    C.sx[c] = C.ok[c] ? G.sx(jc) : -1;
+    C.ax[c] = C.sx[c] >= 0 ? axp[jc] : 0.f;
+    C.bx[c] = C.sx[c] >= 0 ? bxp[jc] : 1.f;
+  }
+  return C;
+}
+
 // ---------------------------------------------------------------------------
 // velocity phase
 // ---------------------------------------------------------------------------
 // Acoustic and viscoacoustic: vx += (dt·irx)·(D⁺ₓp + ψ), vz += (dt·irz)·(D⁺_z p + ψ).
-template <int M, int TZ, int BY>
-__global__ void __launch_bounds__(TILE_X* BY)
+template <int M, int BZ, int R>
+__global__ void __launch_bounds__(XT* BZ)
 k_pressure_velocity(const DevProp* __restrict__ props, WorkSet ws) {
+  constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ float sp[T::N];
-  const StepWork w = find_work(ws, blockIdx.x);
+  __shared__ __align__(16) float sp[T::N];
+  const StepWork& w = find_work(ws, blockIdx.x);
   const DevProp& P = props[w.prop];
+  const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
-  const int nzp = P.nzp, nxp = P.nxp, ld = P.ld;
+  float* const vx = P.f[A_VX];
+  float* const vz = P.f[A_VZ];
+  const float* const irx = P.coef[CA_IRX];
+  const float* const irz = P.coef[CA_IRZ];
+  float* const psx = P.psix[0];
+  float* const psz = P.psiz[0];
+  const float* const azp = P.az; const float* const bzp = P.bz;
   if ((w.flags & STEP_PEAK) && blockIdx.x == w.tile0 && threadIdx.x == 0 && threadIdx.y == 0)
     *P.peak = 0.f;  // the stress phase of this step reduces into it
-  stage<M, TZ, TILE_X * BY>(sp, P.f[A_P], nzp, nxp, ld, L.i0, L.j0);
-  __syncthreads();
-  const int j = L.j0 + threadIdx.x;
-  if (j >= nxp) return;
-  float* __restrict__ vx = P.f[A_VX];
-  float* __restrict__ vz = P.f[A_VZ];
-  const float* __restrict__ irx = P.coef[CA_IRX];
-  const float* __restrict__ irz = P.coef[CA_IRZ];
-  const float c[4] = {P.c[0], P.c[1], P.c[2], P.c[3]};
-  const float dt = P.dt, hx = P.hx, hz = P.hz;
-  const bool xin = (j >= M && j < nxp - M);
-  const int sx = strip_x(P, j);
-  const float axj = sx >= 0 ? P.ax[j] : 0.f, bxj = sx >= 0 ? P.bx[j] : 1.f;
+  stage<M, TZ, XT * BZ>(sp, P.f[A_P], G.nzp, G.ld, L.i0, L.j0);
+  cp_async_commit();
+  const int j = L.j0 + 4 * threadIdx.x;
+  float4 r_vx[R], r_vz[R], r_irx[R], r_irz[R];
 #pragma unroll
-  for (int k = 0; k < TZ / BY; ++k) {
-    const int r = threadIdx.y + k * BY;
-    const int i = L.i0 + r;
-    if (i >= nzp) break;
-    const float* s = sp + (r + M) * T::W + threadIdx.x + M;
-    const size_t g = (size_t)i * ld + j;
-    float d = xin ? dplus<M>(s, 1, c, hx) : 0.f;
-    if (sx >= 0) {
-      float* ps = P.psix[0] + (size_t)i * P.wx + sx;
-      float psi = *ps;
-      d = cpml(d, psi, axj, bxj);
-      *ps = psi;
+  for (int r = 0; r < R; ++r) {
+    const int i = L.i0 + threadIdx.y + BZ * r;
+    if (i < G.nzp && j < G.nxp) {
+      const size_t g = (size_t)i * G.ld + j;
+      r_vx[r] = ld4(vx + g); r_vz[r] = ld4(vz + g); r_irx[r] = ldg4(irx + g); r_irz[r] = ldg4(irz + g);
     }
-    vx[g] = fadd(vx[g], fmul(fmul(dt, irx[g]), d));
-    d = (i >= M && i < nzp - M) ? dplus<M>(s, T::W, c, hz) : 0.f;
-    const int sz = strip_z(P, i);
-    if (sz >= 0) {
-      float* ps = P.psiz[0] + (size_t)sz * ld + j;
-      float psi = *ps;
-      d = cpml(d, psi, P.az[i], P.bz[i]);
-      *ps = psi;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (j >= G.nxp) return;
+  const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int rr = threadIdx.y + BZ * r;
+    const int i = L.i0 + rr;
+    if (i >= G.nzp) break;
+    const float* row = sp + (rr + M) * T::W + 4 * threadIdx.x;
+    const size_t g = (size_t)i * G.ld + j;
+    const bool zin = (i >= M && i < G.nzp - M);
+    const int sz = G.sz(i);
+    const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+    float v[12];
+    row12(row, v);
+    float4 ox = r_vx[r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (!C.ok[c]) continue;
+      float d = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+      if (C.sx[c] >= 0) {
+        float* ps = psx + (size_t)i * G.wx + C.sx[c];
+        float psi = *ps; d = cpml(d, psi, C.ax[c], C.bx[c]); *ps = psi;
+      }
+      set_comp(ox, c, fadd(comp(r_vx[r], c), fmul(fmul(G.dt, comp(r_irx[r], c)), d)));
     }
-    vz[g] = fadd(vz[g], fmul(fmul(dt, irz[g]), d));
+    st4(vx + g, ox);
+    float z[4][2 * M + 1];
+    col9<M>(row + 4, z);
+    float4 oz = r_vz[r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (!C.ok[c]) continue;
+      float d = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
+      if (sz >= 0) {
+        float* ps = psz + (size_t)sz * G.ld + j + c;
+        float psi = *ps; d = cpml(d, psi, azi, bzi); *ps = psi;
+      }
+      set_comp(oz, c, fadd(comp(r_vz[r], c), fmul(fmul(G.dt, comp(r_irz[r], c)), d)));
+    }
+    st4(vz + g, oz);
   }
 }
 
 // Elastic: vx += (dt·irx)·(D⁺ₓσxx + D⁻_zσxz), vz += (dt·irz)·(D⁻ₓσxz + D⁺_zσzz).
-template <int M, int TZ, int BY>
-__global__ void __launch_bounds__(TILE_X* BY)
+template <int M, int BZ, int R>
+__global__ void __launch_bounds__(XT* BZ)
 k_elastic_velocity(const DevProp* __restrict__ props, WorkSet ws) {
+  constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ float sxx_s[T::N];
-  __shared__ float szz_s[T::N];
-  __shared__ float sxz_s[T::N];
-  const StepWork w = find_work(ws, blockIdx.x);
+  __shared__ __align__(16) float sxx_s[T::N];
+  __shared__ __align__(16) float szz_s[T::N];
+  __shared__ __align__(16) float sxz_s[T::N];
+  const StepWork& w = find_work(ws, blockIdx.x);
   const DevProp& P = props[w.prop];
+  const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
-  const int nzp = P.nzp, nxp = P.nxp, ld = P.ld;
-  stage<M, TZ, TILE_X * BY>(sxx_s, P.f[E_SXX], nzp, nxp, ld, L.i0, L.j0);
-  stage<M, TZ, TILE_X * BY>(szz_s, P.f[E_SZZ], nzp, nxp, ld, L.i0, L.j0);
-  stage<M, TZ, TILE_X * BY>(sxz_s, P.f[E_SXZ], nzp, nxp, ld, L.i0, L.j0);
-  __syncthreads();
-  const int j = L.j0 + threadIdx.x;
-  if (j >= nxp) return;
-  float* __restrict__ vx = P.f[E_VX];
-  float* __restrict__ vz = P.f[E_VZ];
-  const float* __restrict__ irx = P.coef[CE_IRX];
-  const float* __restrict__ irz = P.coef[CE_IRZ];
-  const float c[4] = {P.c[0], P.c[1], P.c[2], P.c[3]};
-  const float dt = P.dt, hx = P.hx, hz = P.hz;
-  const bool xin = (j >= M && j < nxp - M);
-  const int sx = strip_x(P, j);
-  const float axj = sx >= 0 ? P.ax[j] : 0.f, bxj = sx >= 0 ? P.bx[j] : 1.f;
+  float* const vx = P.f[E_VX];
+  float* const vz = P.f[E_VZ];
+  const float* const irx = P.coef[CE_IRX];
+  const float* const irz = P.coef[CE_IRZ];
+  float* const psx0 = P.psix[0]; float* const psx1 = P.psix[1];
+  float* const psz0 = P.psiz[0]; float* const psz1 = P.psiz[1];
+  const float* const azp = P.az; const float* const bzp = P.bz;
+  stage<M, TZ, XT * BZ>(sxx_s, P.f[E_SXX], G.nzp, G.ld, L.i0, L.j0);
+  stage<M, TZ, XT * BZ>(szz_s, P.f[E_SZZ], G.nzp, G.ld, L.i0, L.j0);
+  stage<M, TZ, XT * BZ>(sxz_s, P.f[E_SXZ], G.nzp, G.ld, L.i0, L.j0);
+  cp_async_commit();
+  const int j = L.j0 + 4 * threadIdx.x;
+  float4 r_vx[R], r_vz[R], r_irx[R], r_irz[R];
 #pragma unroll
-  for (int k = 0; k < TZ / BY; ++k) {
-    const int r = threadIdx.y + k * BY;
-    const int i = L.i0 + r;
-    if (i >= nzp) break;
-    const int so = (r + M) * T::W + threadIdx.x + M;
-    const size_t g = (size_t)i * ld + j;
-    const bool zin = (i >= M && i < nzp - M);
-    const int sz = strip_z(P, i);
-    const float azi = sz >= 0 ? P.az[i] : 0.f, bzi = sz >= 0 ? P.bz[i] : 1.f;
-    // vx_dsxx (x, D⁺) and vx_dsxz (z, D⁻)
-    float a = xin ? dplus<M>(sxx_s + so, 1, c, hx) : 0.f;
-    float b = zin ? dminus<M>(sxz_s + so, T::W, c, hz) : 0.f;
-    if (sx >= 0) {
-      float* ps = P.psix[0] + (size_t)i * P.wx + sx;
-      float psi = *ps; a = cpml(a, psi, axj, bxj); *ps = psi;
+  for (int r = 0; r < R; ++r) {
+    const int i = L.i0 + threadIdx.y + BZ * r;
+    if (i < G.nzp && j < G.nxp) {
+      const size_t g = (size_t)i * G.ld + j;
+      r_vx[r] = ld4(vx + g); r_vz[r] = ld4(vz + g); r_irx[r] = ldg4(irx + g); r_irz[r] = ldg4(irz + g);
     }
-    if (sz >= 0) {
-      float* ps = P.psiz[0] + (size_t)sz * ld + j;
-      float psi = *ps; b = cpml(b, psi, azi, bzi); *ps = psi;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (j >= G.nxp) return;
+  const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int rr = threadIdx.y + BZ * r;
+    const int i = L.i0 + rr;
+    if (i >= G.nzp) break;
+    const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+    const size_t g = (size_t)i * G.ld + j;
+    const bool zin = (i >= M && i < G.nzp - M);
+    const int sz = G.sz(i);
+    const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+    // vx: vx_dsxx (x, D⁺ of σxx) + vx_dsxz (z, D⁻ of σxz)
+    float a[4], b[4];
+    {
+      float v[12];
+      row12(sxx_s + ro, v);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) a[c] = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+      float z[4][2 * M + 1];
+      col9<M>(sxz_s + ro + 4, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
     }
-    vx[g] = fadd(vx[g], fmul(fmul(dt, irx[g]), fadd(a, b)));
-    // vz_dsxz (x, D⁻) and vz_dszz (z, D⁺)
-    a = xin ? dminus<M>(sxz_s + so, 1, c, hx) : 0.f;
-    b = zin ? dplus<M>(szz_s + so, T::W, c, hz) : 0.f;
-    if (sx >= 0) {
-      float* ps = P.psix[1] + (size_t)i * P.wx + sx;
-      float psi = *ps; a = cpml(a, psi, axj, bxj); *ps = psi;
+    float4 ox = r_vx[r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (!C.ok[c]) continue;
+      float av = a[c], bv = b[c];
+      if (C.sx[c] >= 0) {
+        float* ps = psx0 + (size_t)i * G.wx + C.sx[c];
+        float psi = *ps; av = cpml(av, psi, C.ax[c], C.bx[c]); *ps = psi;
+      }
+      if (sz >= 0) {
+        float* ps = psz0 + (size_t)sz * G.ld + j + c;
+        float psi = *ps; bv = cpml(bv, psi, azi, bzi); *ps = psi;
+      }
+      set_comp(ox, c, fadd(comp(r_vx[r], c), fmul(fmul(G.dt, comp(r_irx[r], c)), fadd(av, bv))));
     }
-    if (sz >= 0) {
-      float* ps = P.psiz[1] + (size_t)sz * ld + j;
-      float psi = *ps; b = cpml(b, psi, azi, bzi); *ps = psi;
+    st4(vx + g, ox);
+    // vz: vz_dsxz (x, D⁻ of σxz) + vz_dszz (z, D⁺ of σzz)
+    {
+      float v[12];
+      row12(sxz_s + ro, v);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) a[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+      float z[4][2 * M + 1];
+      col9<M>(szz_s + ro + 4, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
     }
-    vz[g] = fadd(vz[g], fmul(fmul(dt, irz[g]), fadd(a, b)));
+    float4 oz = r_vz[r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (!C.ok[c]) continue;
+      float av = a[c], bv = b[c];
+      if (C.sx[c] >= 0) {
+        float* ps = psx1 + (size_t)i * G.wx + C.sx[c];
+        float psi = *ps; av = cpml(av, psi, C.ax[c], C.bx[c]); *ps = psi;
+      }
+      if (sz >= 0) {
+        float* ps = psz1 + (size_t)sz * G.ld + j + c;
+        float psi = *ps; bv = cpml(bv, psi, azi, bzi); *ps = psi;
+      }
+      set_comp(oz, c, fadd(comp(r_vz[r], c), fmul(fmul(G.dt, comp(r_irz[r], c)), fadd(av, bv))));
+    }
+    st4(vz + g, oz);
   }
 }
 
@@ -184,11 +466,13 @@ __device__ __forceinline__ void block_max_to(float v, float* dst) {
   // v ≥ 0: the float bit pattern orders like the integer.
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   __shared__ float red[32];
-  const int lane = threadIdx.x, wid = threadIdx.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  const int nw = (blockDim.x * blockDim.y + 31) >> 5;
   if (lane == 0) red[wid] = v;
   __syncthreads();
   if (wid == 0) {
-    v = lane < blockDim.y ? red[lane] : 0.f;
+    v = lane < nw ? red[lane] : 0.f;
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (lane == 0) atomicMax(reinterpret_cast<int*>(dst), __float_as_int(v));
   }
@@ -196,73 +480,121 @@ __device__ __forceinline__ void block_max_to(float v, float* dst) {
 
 // Acoustic (VISCO=false): p += (dt·κ)·div.  Viscoacoustic (VISCO=true):
 // ε += dt·div; r_l ← r_l·a_l + b_l·Δε; p = K_R·ε + Σ r_l.
-template <int M, int TZ, int BY, bool VISCO>
-__global__ void __launch_bounds__(TILE_X* BY)
+template <int M, int BZ, int R, bool VISCO>
+__global__ void __launch_bounds__(XT* BZ)
 k_pressure_stress(const DevProp* __restrict__ props, WorkSet ws) {
+  constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ float svx[T::N];
-  __shared__ float svz[T::N];
-  const StepWork w = find_work(ws, blockIdx.x);
+  __shared__ __align__(16) float svx[T::N];
+  __shared__ __align__(16) float svz[T::N];
+  const StepWork& w = find_work(ws, blockIdx.x);
   const DevProp& P = props[w.prop];
+  const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
-  const int nzp = P.nzp, nxp = P.nxp, ld = P.ld;
-  stage<M, TZ, TILE_X * BY>(svx, P.f[A_VX], nzp, nxp, ld, L.i0, L.j0);
-  stage<M, TZ, TILE_X * BY>(svz, P.f[A_VZ], nzp, nxp, ld, L.i0, L.j0);
-  __syncthreads();
-  const int j = L.j0 + threadIdx.x;
-  const bool jok = j < nxp;
-  float* __restrict__ p = P.f[A_P];
-  const float c[4] = {P.c[0], P.c[1], P.c[2], P.c[3]};
-  const float dt = P.dt, hx = P.hx, hz = P.hz;
-  const bool xin = (j >= M && j < nxp - M);
-  const int sx = jok ? strip_x(P, j) : -1;
-  const float axj = sx >= 0 ? P.ax[j] : 0.f, bxj = sx >= 0 ? P.bx[j] : 1.f;
-  float peak = 0.f;
+  float* const p = P.f[A_P];
+  float* const eps = VISCO ? P.f[V_EPS] : nullptr;
+  float* const r0 = VISCO ? P.f[V_R0] : nullptr;
+  const float* const cA = VISCO ? P.coef[CV_KR] : P.coef[CA_KAPPA];   // κ or K_R
+  const float* const b0 = VISCO ? P.coef[CV_B0] : nullptr;
+  const size_t fstride = (size_t)(P.f[1] - P.f[0]);                   // field / coefficient pitch
+  const int nL = VISCO ? P.L : 0;
+  const uint8_t* const qidx = VISCO ? P.qidx : nullptr;
+  const float* const relax_a = VISCO ? P.relax_a : nullptr;
+  float* const psx = P.psix[1];
+  float* const psz = P.psiz[1];
+  const float* const azp = P.az; const float* const bzp = P.bz;
+  stage<M, TZ, XT * BZ>(svx, P.f[A_VX], G.nzp, G.ld, L.i0, L.j0);
+  stage<M, TZ, XT * BZ>(svz, P.f[A_VZ], G.nzp, G.ld, L.i0, L.j0);
+  cp_async_commit();
+  const int j = L.j0 + 4 * threadIdx.x;
+  const bool jok = j < G.nxp;
+  float4 r_a[R], r_b[R];   // acoustic: p, κ; viscoacoustic: ε, K_R
 #pragma unroll
-  for (int k = 0; k < TZ / BY; ++k) {
-    const int r = threadIdx.y + k * BY;
-    const int i = L.i0 + r;
-    if (!jok || i >= nzp) break;
-    const int so = (r + M) * T::W + threadIdx.x + M;
-    const size_t g = (size_t)i * ld + j;
-    float dx = xin ? dminus<M>(svx + so, 1, c, hx) : 0.f;
-    if (sx >= 0) {
-      float* ps = P.psix[1] + (size_t)i * P.wx + sx;
-      float psi = *ps; dx = cpml(dx, psi, axj, bxj); *ps = psi;
+  for (int r = 0; r < R; ++r) {
+    const int i = L.i0 + threadIdx.y + BZ * r;
+    if (i < G.nzp && jok) {
+      const size_t g = (size_t)i * G.ld + j;
+      r_a[r] = ld4(VISCO ? eps + g : p + g);
+      r_b[r] = ldg4(cA + g);
     }
-    float dz = (i >= M && i < nzp - M) ? dminus<M>(svz + so, T::W, c, hz) : 0.f;
-    const int sz = strip_z(P, i);
-    if (sz >= 0) {
-      float* ps = P.psiz[1] + (size_t)sz * ld + j;
-      float psi = *ps; dz = cpml(dz, psi, P.az[i], P.bz[i]); *ps = psi;
-    }
-    const float div = fadd(dx, dz);
-    const bool src = (i == P.src_iz && j == P.src_ix && w.amp != 0.f);
-    if constexpr (!VISCO) {
-      float pv = fadd(p[g], fmul(fmul(dt, P.coef[CA_KAPPA][g]), div));
-      if (src) pv = fadd(pv, w.amp);
-      if (P.free_surface && i == P.pad) pv = 0.f;
-      p[g] = pv;
-    } else {
-      const float inc = fmul(dt, div);
-      float* __restrict__ eps = P.f[V_EPS];
-      float e = fadd(eps[g], inc);
-      float total = 0.f;
-      const uint8_t q = P.qidx[g];
-      for (int l = 0; l < P.L; ++l) {
-        float* __restrict__ rl = P.f[V_R0 + l];
-        const float rv = fadd(fmul(rl[g], P.relax_a[q * P.L + l]), fmul(P.coef[CV_B0 + l][g], inc));
-        rl[g] = rv;
-        total = (l == 0) ? rv : fadd(total, rv);
+  }
+  float amp, amp_eps;
+  source_amps(w, P, amp, amp_eps);
+  cp_async_wait_all();
+  __syncthreads();
+  const size_t npix = (size_t)G.nz * G.nx;
+  float peak = 0.f;
+  if (jok) {
+    const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int rr = threadIdx.y + BZ * r;
+      const int i = L.i0 + rr;
+      if (i >= G.nzp) break;
+      const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+      const size_t g = (size_t)i * G.ld + j;
+      const bool zin = (i >= M && i < G.nzp - M);
+      const int sz = G.sz(i);
+      const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+      float dx[4], dz[4];
+      {
+        float v[12];
+        row12(svx + ro, v);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dx[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+        float z[4][2 * M + 1];
+        col9<M>(svz + ro + 4, z);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
       }
-      float pv = fadd(fmul(P.coef[CV_KR][g], e), total);
-      if (src) {
-        e = fadd(e, w.amp_eps);
-        pv = fadd(pv, w.amp);
+      float4 out = r_a[r];
+      float4 epsv = r_a[r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (!C.ok[c]) continue;
+        const int jc = j + c;
+        float ddx = dx[c], ddz = dz[c];
+        if (C.sx[c] >= 0) {
+          float* ps = psx + (size_t)i * G.wx + C.sx[c];
+          float psi = *ps; ddx = cpml(ddx, psi, C.ax[c], C.bx[c]); *ps = psi;
+        }
+        if (sz >= 0) {
+          float* ps = psz + (size_t)sz * G.ld + jc;
+          float psi = *ps; ddz = cpml(ddz, psi, azi, bzi); *ps = psi;
+        }
+        const float div = fadd(ddx, ddz);
+        const bool src = (i == G.src_iz && jc == G.src_ix && amp != 0.f);
+        float pv;
+        if constexpr (!VISCO) {
+          pv = fadd(comp(r_a[r], c), fmul(fmul(G.dt, comp(r_b[r], c)), div));
+          if (src) pv = fadd(pv, amp);
+          if (G.free_surface && i == G.pad) pv = 0.f;
+        } else {
+          const float inc = fmul(G.dt, div);
+          float e = fadd(comp(r_a[r], c), inc);
+          float total = 0.f;
+          const int q = qidx[g + c];
+          for (int l = 0; l < nL; ++l) {
+            float* rl = r0 + l * fstride;
+            const float rv = fadd(fmul(rl[g + c], __ldg(relax_a + q * nL + l)),
+                                  fmul(__ldg(b0 + l * fstride + g + c), inc));
+            rl[g + c] = rv;
+            total = (l == 0) ? rv : fadd(total, rv);
+          }
+          pv = fadd(fmul(comp(r_b[r], c), e), total);
+          if (src) {
+            e = fadd(e, amp_eps);
+            pv = fadd(pv, amp);
+          }
+          set_comp(epsv, c, e);
+          peak = fmaxf(peak, fabsf(pv));
+        }
+        set_comp(out, c, pv);
+        size_t pc;
+        if (w.epi.kind != EPI_NONE && G.physical(i, jc, pc)) run_epilogue(w.epi, pc, npix, pv, 0.f);
       }
-      eps[g] = e;
-      p[g] = pv;
-      peak = fmaxf(peak, fabsf(pv));
+      st4(p + g, out);
+      if constexpr (VISCO) st4(eps + g, epsv);
     }
   }
   if constexpr (VISCO) {
@@ -272,76 +604,141 @@ k_pressure_stress(const DevProp* __restrict__ props, WorkSet ws) {
 
 // Elastic stress phase:
 //   σxx += dt·(λ2μ·εxx + λ·εzz), σzz += dt·(λ·εxx + λ2μ·εzz),
-//   σxz += (dt·μxz)·(D⁺_z vx + D⁺ₓ vz); source; free surface σzz = σxz = 0.
-template <int M, int TZ, int BY>
-__global__ void __launch_bounds__(TILE_X* BY)
+//   σxz += (dt·μxz)·(D⁺_z vx + D⁺ₓ vz); source; free surface σzz = σxz = 0;
+// then the epilogue with P/S from the stresses (stress separation) or from
+// the raw velocity divergence/curl (divcurl, propagation.py:953-976).
+template <int M, int BZ, int R>
+__global__ void __launch_bounds__(XT* BZ)
 k_elastic_stress(const DevProp* __restrict__ props, WorkSet ws) {
+  constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ float svx[T::N];
-  __shared__ float svz[T::N];
-  const StepWork w = find_work(ws, blockIdx.x);
+  __shared__ __align__(16) float svx[T::N];
+  __shared__ __align__(16) float svz[T::N];
+  const StepWork& w = find_work(ws, blockIdx.x);
   const DevProp& P = props[w.prop];
+  const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
-  const int nzp = P.nzp, nxp = P.nxp, ld = P.ld;
-  stage<M, TZ, TILE_X * BY>(svx, P.f[E_VX], nzp, nxp, ld, L.i0, L.j0);
-  stage<M, TZ, TILE_X * BY>(svz, P.f[E_VZ], nzp, nxp, ld, L.i0, L.j0);
-  __syncthreads();
-  const int j = L.j0 + threadIdx.x;
-  if (j >= nxp) return;
-  float* __restrict__ sxx = P.f[E_SXX];
-  float* __restrict__ szz = P.f[E_SZZ];
-  float* __restrict__ sxz = P.f[E_SXZ];
-  const float c[4] = {P.c[0], P.c[1], P.c[2], P.c[3]};
-  const float dt = P.dt, hx = P.hx, hz = P.hz;
-  const bool xin = (j >= M && j < nxp - M);
-  const int sx = strip_x(P, j);
-  const float axj = sx >= 0 ? P.ax[j] : 0.f, bxj = sx >= 0 ? P.bx[j] : 1.f;
+  float* const sxx = P.f[E_SXX];
+  float* const szz = P.f[E_SZZ];
+  float* const sxz = P.f[E_SXZ];
+  const float* const clam = P.coef[CE_LAM];
+  const float* const cl2m = P.coef[CE_L2M];
+  const float* const cmu = P.coef[CE_MUXZ];
+  float* const psx2 = P.psix[2]; float* const psx3 = P.psix[3];
+  float* const psz2 = P.psiz[2]; float* const psz3 = P.psiz[3];
+  const float* const azp = P.az; const float* const bzp = P.bz;
+  const int mech = P.mech;
+  stage<M, TZ, XT * BZ>(svx, P.f[E_VX], G.nzp, G.ld, L.i0, L.j0);
+  stage<M, TZ, XT * BZ>(svz, P.f[E_VZ], G.nzp, G.ld, L.i0, L.j0);
+  cp_async_commit();
+  const int j = L.j0 + 4 * threadIdx.x;
+  float4 r_xx[R], r_zz[R], r_xz[R], r_lam[R], r_l2m[R], r_mu[R];
 #pragma unroll
-  for (int k = 0; k < TZ / BY; ++k) {
-    const int r = threadIdx.y + k * BY;
-    const int i = L.i0 + r;
-    if (i >= nzp) break;
-    const int so = (r + M) * T::W + threadIdx.x + M;
-    const size_t g = (size_t)i * ld + j;
-    const bool zin = (i >= M && i < nzp - M);
-    const int sz = strip_z(P, i);
-    const float azi = sz >= 0 ? P.az[i] : 0.f, bzi = sz >= 0 ? P.bz[i] : 1.f;
-    float exx = xin ? dminus<M>(svx + so, 1, c, hx) : 0.f;   // sxx_dvx
-    float ezz = zin ? dminus<M>(svz + so, T::W, c, hz) : 0.f; // szz_dvz
-    float f1 = zin ? dplus<M>(svx + so, T::W, c, hz) : 0.f;   // sxz_dvx
-    float f2 = xin ? dplus<M>(svz + so, 1, c, hx) : 0.f;      // sxz_dvz
-    if (sx >= 0) {
-      float* p0 = P.psix[2] + (size_t)i * P.wx + sx;
-      float psi = *p0; exx = cpml(exx, psi, axj, bxj); *p0 = psi;
-      float* p1 = P.psix[3] + (size_t)i * P.wx + sx;
-      psi = *p1; f2 = cpml(f2, psi, axj, bxj); *p1 = psi;
+  for (int r = 0; r < R; ++r) {
+    const int i = L.i0 + threadIdx.y + BZ * r;
+    if (i < G.nzp && j < G.nxp) {
+      const size_t g = (size_t)i * G.ld + j;
+      r_xx[r] = ld4(sxx + g); r_zz[r] = ld4(szz + g); r_xz[r] = ld4(sxz + g);
+      r_lam[r] = ldg4(clam + g); r_l2m[r] = ldg4(cl2m + g); r_mu[r] = ldg4(cmu + g);
     }
-    if (sz >= 0) {
-      float* p0 = P.psiz[2] + (size_t)sz * ld + j;
-      float psi = *p0; ezz = cpml(ezz, psi, azi, bzi); *p0 = psi;
-      float* p1 = P.psiz[3] + (size_t)sz * ld + j;
-      psi = *p1; f1 = cpml(f1, psi, azi, bzi); *p1 = psi;
-    }
-    const float lam = P.coef[CE_LAM][g], l2m = P.coef[CE_L2M][g];
-    float vxx = fadd(sxx[g], fmul(dt, fadd(fmul(l2m, exx), fmul(lam, ezz))));
-    float vzz = fadd(szz[g], fmul(dt, fadd(fmul(lam, exx), fmul(l2m, ezz))));
-    float vxz = fadd(sxz[g], fmul(fmul(dt, P.coef[CE_MUXZ][g]), fadd(f1, f2)));
-    if (i == P.src_iz && j == P.src_ix && w.amp != 0.f) {
-      if (P.mech == MECH_SHEAR) {
-        vxz = fadd(vxz, w.amp);
-      } else if (P.mech == MECH_EXPLOSIVE) {
-        vxx = fadd(vxx, w.amp);
-        vzz = fadd(vzz, w.amp);
+  }
+  float amp, amp_eps;
+  source_amps(w, P, amp, amp_eps);
+  cp_async_wait_all();
+  __syncthreads();
+  if (j >= G.nxp) return;
+  const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
+  const size_t npix = (size_t)G.nz * G.nx;
+  const Epilogue& E = w.epi;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int rr = threadIdx.y + BZ * r;
+    const int i = L.i0 + rr;
+    if (i >= G.nzp) break;
+    const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+    const size_t g = (size_t)i * G.ld + j;
+    const bool zin = (i >= M && i < G.nzp - M);
+    const int sz = G.sz(i);
+    const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+    const bool want_curl = E.kind != EPI_NONE && E.sep == 1 && E.need_s;
+    float exx[4], ezz[4], f1[4], f2[4], curl_a[4], curl_b[4];
+    {
+      float v[12];
+      row12(svx + ro, v);        // vx along x: D⁻ (εxx)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) exx[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+      row12(svz + ro, v);        // vz along x: D⁺ (σxz) and D⁻ (curl)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        f2[c] = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+        curl_b[c] = want_curl ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
       }
-      // force_z adds to vz after this launch (other blocks still read vz here).
+      float z[4][2 * M + 1];
+      col9<M>(svx + ro + 4, z);  // vx along z: D⁺ (σxz) and D⁻ (curl)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        f1[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
+        curl_a[c] = want_curl ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
+      }
+      col9<M>(svz + ro + 4, z);  // vz along z: D⁻ (εzz)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ezz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
     }
-    if (P.free_surface && i == P.pad) {
-      vzz = 0.f;
-      vxz = 0.f;
+    float4 oxx = r_xx[r], ozz = r_zz[r], oxz = r_xz[r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (!C.ok[c]) continue;
+      const int jc = j + c;
+      const float exx_raw = exx[c], ezz_raw = ezz[c];
+      float ex = exx_raw, ez = ezz_raw, g1 = f1[c], g2 = f2[c];
+      if (C.sx[c] >= 0) {
+        float* p0 = psx2 + (size_t)i * G.wx + C.sx[c];
+        float psi = *p0; ex = cpml(ex, psi, C.ax[c], C.bx[c]); *p0 = psi;
+        float* p1 = psx3 + (size_t)i * G.wx + C.sx[c];
+        psi = *p1; g2 = cpml(g2, psi, C.ax[c], C.bx[c]); *p1 = psi;
+      }
+      if (sz >= 0) {
+        float* p0 = psz2 + (size_t)sz * G.ld + jc;
+        float psi = *p0; ez = cpml(ez, psi, azi, bzi); *p0 = psi;
+        float* p1 = psz3 + (size_t)sz * G.ld + jc;
+        psi = *p1; g1 = cpml(g1, psi, azi, bzi); *p1 = psi;
+      }
+      const float lam = comp(r_lam[r], c), l2m = comp(r_l2m[r], c);
+      float vxx = fadd(comp(r_xx[r], c), fmul(G.dt, fadd(fmul(l2m, ex), fmul(lam, ez))));
+      float vzz = fadd(comp(r_zz[r], c), fmul(G.dt, fadd(fmul(lam, ex), fmul(l2m, ez))));
+      float vxz = fadd(comp(r_xz[r], c), fmul(fmul(G.dt, comp(r_mu[r], c)), fadd(g1, g2)));
+      if (i == G.src_iz && jc == G.src_ix && amp != 0.f) {
+        if (mech == MECH_SHEAR) {
+          vxz = fadd(vxz, amp);
+        } else if (mech == MECH_EXPLOSIVE) {
+          vxx = fadd(vxx, amp);
+          vzz = fadd(vzz, amp);
+        }
+        // force_z adds to vz after this launch (other blocks still read vz here).
+      }
+      if (G.free_surface && i == G.pad) {
+        vzz = 0.f;
+        vxz = 0.f;
+      }
+      set_comp(oxx, c, vxx);
+      set_comp(ozz, c, vzz);
+      set_comp(oxz, c, vxz);
+      size_t pc;
+      if (E.kind != EPI_NONE && G.physical(i, jc, pc)) {
+        float pv, sv = 0.f;
+        if (E.sep == 0) {
+          pv = fmul(0.5f, fadd(vxx, vzz));
+          sv = vxz;
+        } else {
+          pv = fadd(exx_raw, ezz_raw);
+          if (E.need_s) sv = fsub(curl_a[c], curl_b[c]);
+        }
+        run_epilogue(E, pc, npix, pv, sv);
+      }
     }
-    sxx[g] = vxx;
-    szz[g] = vzz;
-    sxz[g] = vxz;
+    st4(sxx + g, oxx);
+    st4(szz + g, ozz);
+    st4(sxz + g, oxz);
   }
 }
 

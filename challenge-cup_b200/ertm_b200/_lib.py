@@ -42,7 +42,8 @@ class PropInfo(C.Structure):
         ("nzp", C.c_int32), ("nxp", C.c_int32), ("ld", C.c_int32), ("pad", C.c_int32),
         ("state_bytes", C.c_int64), ("field_bytes", C.c_int64), ("step_index", C.c_int64),
         ("n_fields", C.c_int32), ("clipped", C.c_int32), ("lowpass_steps", C.c_int32),
-        ("n_receivers", C.c_int32),
+        ("n_receivers", C.c_int32), ("fast_div_x", C.c_int32), ("fast_div_z", C.c_int32),
+        ("tile_rows", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -61,6 +62,10 @@ _SIGNATURES = {
     "ertm_last_error": (C.c_char_p, []),
     "ertm_version": (_I32, []),
     "ertm_init": (_I32, [_I32]),
+    "ertm_launch_count": (C.c_int64, []),
+    "ertm_set_tile_rows": (_I32, [_I32]),
+    "ertm_profile_stencil": (_I32, [_I32, _I32]),
+    "ertm_profile_read": (_I32, [C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "ertm_prop_create": (_P, [C.POINTER(PropConfig)] + [_P] * 12 + [_P]),
     "ertm_prop_destroy": (None, [_P]),
     "ertm_prop_info_get": (_I32, [_P, C.POINTER(PropInfo)]),

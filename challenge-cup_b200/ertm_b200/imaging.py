@@ -176,81 +176,8 @@ class RTMImager:
             model.validate()
         except ValueError as exc:
             raise ImagingError(f"invalid imaging input: {exc}") from exc
-        spec = PropagationSpec.from_config(self.solver_config, model)
-        try:
-            check_stability(model, spec)
-        except Exception as exc:
-            raise ImagingError(str(exc)) from exc
-        engine = self.solver_config.engine
-        separation = self.config.separation
-        pairs = [self._resolve_mode(m) for m in modes]
-        if engine in ("acoustic", "viscoacoustic") and any(m.lower() not in _ACOUSTIC_MODES for m in modes):
-            raise ImagingError("acoustic/viscoacoustic engines image PP only; use solver.engine='elastic'")
-        condition = str(self.config.condition).lower()
-        record = self._prepare_record(shot, spec, preprocess)
-        if not record:
-            raise ImagingError("empty shot record; nothing to back-propagate")
-        w = self._prepare_wavelet(shot, spec, wavelet)
-
-        prop = build_propagator(model, spec, engine=engine, q_options=self.q_options(compensation=False))
-        prop.set_source(shot.source)
-        prop.set_receivers(shot.receivers)
-        back = build_propagator(model, spec, engine=engine, q_options=self.q_options(compensation=True))
-        back.set_source(shot.source)
-        back.set_receivers(shot.receivers)
-
-        per_state = max(int(prop.state_bytes()), 1)   # fields only before the first step
-        interval = checkpoint_interval(len(w), per_state, float(self.config.checkpoint_mb))
-        n_states = (len(w) + interval - 1) // interval
-        store = CheckpointStore(interval=interval, bytes_per_state=per_state, n_states=n_states)
-        start_step = int(np.floor((float(shot.source.delay) + float(self.config.start_periods)
-                                   / max(float(shot.source.f0), 1e-6)) / spec.dt))
-        start_step = int(np.clip(start_step, 0, spec.nt))
-
-        names = list(record)
-        codes = []
-        for n in names:
-            tgt = _target_component(n, engine)
-            codes.append(back._check_component(tgt, "inject"))
-        rec = np.ascontiguousarray(np.stack([np.asarray(record[n], dtype=np.float32) for n in names]))
-        cfg = _lib.MigrateConfig()
-        cfg.nt = int(len(w))
-        cfg.nt_spec = int(spec.nt)
-        cfg.interval = int(interval)
-        cfg.condition = _lib.COND[condition]
-        cfg.illumination = int(condition == "normalized" or bool(self.config.receiver_normalization))
-        cfg.start_step = start_step
-        cfg.separation = _lib.SEP[separation]
-        cfg.n_images = len(pairs)
-        for k, (s, r) in enumerate(pairs):
-            cfg.src_wave[k] = _lib.WAVE[s]
-            cfg.rcv_wave[k] = _lib.WAVE[r]
-        cfg.accum = _lib.ACCUM[self.accumulation]
-        cfg.n_comp = len(codes)
-        for k, c in enumerate(codes):
-            cfg.comp[k] = c
-        nz, nx = model.grid.nz, model.grid.nx
-        num_acc = np.zeros((len(pairs), nz, nx))
-        ill_acc = np.zeros((len(pairs), nz, nx))
-        ril_acc = np.zeros((len(pairs), nz, nx))
-        if rec.shape[1] < spec.nt:
-            raise ImagingError("record shorter than nt after preparation")
-        _lib.check(_lib.lib().ertm_migrate(prop.handle, back.handle, cfg, _lib.ptr(w), _lib.ptr(rec),
-                                          _lib.ptr(num_acc), _lib.ptr(ill_acc), _lib.ptr(ril_acc)), "migrate")
-        prop._psi_allocated = back._psi_allocated = True
-        eps = float(self.config.eps)
-        results = []
-        for k, m in enumerate(modes):
-            image = postprocess_image(
-                num_acc[k], ill_acc[k], ril_acc[k], dx=model.grid.dx, dz=model.grid.dz,
-                by_illum=condition == "normalized" and bool(self.config.illumination),
-                by_rillum=bool(self.config.receiver_normalization), eps=eps, laplacian=bool(self.config.laplacian),
-                lowpass_fraction=float(self.config.lowpass_fraction), npml=spec.npml, boundary=spec.boundary)
-            res = ImageResult(image=image, grid=model.grid, mode=m,
-                              meta=self._meta(spec, engine, shot, store, condition, start_step, prop, back, m))
-            res.validate()
-            results.append(res)
-        return results
+        mig = ShotMigrator(self, model)
+        return mig.migrate(shot, wavelet=wavelet, preprocess=preprocess, modes=modes)
 
     def image_condition(self, source_wavefield: np.ndarray, receiver_wavefield: np.ndarray) -> np.ndarray:
         s, r = np.asarray(source_wavefield), np.asarray(receiver_wavefield)
@@ -340,6 +267,148 @@ class RTMImager:
                 "accumulation": self.accumulation}
 
 
+class ShotMigrator:
+    """Device-resident RTM for one model: the forward and backward
+    propagators are built once and reset between shots, so a stream of shots
+    on the same model pays the material set-up once.  ``migrate`` returns
+    ``ImageResult`` objects (host images); ``migrate_device`` takes the record
+    as a device tensor and returns device tensors (torch, float32)."""
+
+    def __init__(self, imager: RTMImager, model: Any) -> None:
+        self.imager = imager
+        self.model = model
+        self.spec = PropagationSpec.from_config(imager.solver_config, model)
+        try:
+            check_stability(model, self.spec)
+        except Exception as exc:
+            raise ImagingError(str(exc)) from exc
+        self.engine = imager.solver_config.engine
+        self.prop = build_propagator(model, self.spec, engine=self.engine,
+                                     q_options=imager.q_options(compensation=False))
+        self.back = build_propagator(model, self.spec, engine=self.engine,
+                                     q_options=imager.q_options(compensation=True))
+        self._receivers_key: tuple | None = None
+        self._used = False
+
+    def _prepare(self, source: Any, receivers: Any, modes: tuple[str, ...], n_steps: int):
+        im = self.imager
+        pairs = [im._resolve_mode(m) for m in modes]
+        if not 1 <= len(pairs) <= 2:
+            raise ImagingError("one or two imaging modes per pass")
+        if self.engine in ("acoustic", "viscoacoustic") and any(m.lower() not in _ACOUSTIC_MODES for m in modes):
+            raise ImagingError("acoustic/viscoacoustic engines image PP only; use solver.engine='elastic'")
+        if self._used:
+            self.prop.reset()
+            self.back.reset()
+        self._used = True
+        self.prop.set_source(source)
+        self.back.set_source(source)
+        key = (np.asarray(receivers.x, dtype=np.float64).tobytes(), np.asarray(receivers.z, dtype=np.float64).tobytes())
+        if key != self._receivers_key:
+            self.prop.set_receivers(receivers)
+            self.back.set_receivers(receivers)
+            self._receivers_key = key
+        else:
+            self.prop._receivers = self.back._receivers = receivers
+        per_state = max(int(self.prop.state_bytes()), 1)   # fields only before the first step
+        interval = checkpoint_interval(n_steps, per_state, float(im.config.checkpoint_mb))
+        store = CheckpointStore(interval=interval, bytes_per_state=per_state,
+                                n_states=(n_steps + interval - 1) // interval)
+        start_step = int(np.floor((float(source.delay) + float(im.config.start_periods)
+                                   / max(float(source.f0), 1e-6)) / self.spec.dt))
+        start_step = int(np.clip(start_step, 0, self.spec.nt))
+        return pairs, store, start_step
+
+    def _config(self, pairs, names, store, start_step, n_steps) -> _lib.MigrateConfig:
+        im = self.imager
+        condition = str(im.config.condition).lower()
+        cfg = _lib.MigrateConfig()
+        cfg.nt = int(n_steps)
+        cfg.nt_spec = int(self.spec.nt)
+        cfg.interval = int(store.interval)
+        cfg.condition = _lib.COND[condition]
+        # bit 0: source illumination (used only by normalized + illumination);
+        # bit 1: receiver illumination (used only by receiver normalisation)
+        cfg.illumination = (int(condition == "normalized" and bool(im.config.illumination))
+                            | (2 if im.config.receiver_normalization else 0))
+        cfg.start_step = start_step
+        cfg.separation = _lib.SEP[im.config.separation]
+        cfg.n_images = len(pairs)
+        for k, (s, r) in enumerate(pairs):
+            cfg.src_wave[k] = _lib.WAVE[s]
+            cfg.rcv_wave[k] = _lib.WAVE[r]
+        cfg.accum = _lib.ACCUM[im.accumulation]
+        codes = [self.back._check_component(_target_component(n, self.engine), "inject") for n in names]
+        if len(codes) > 8:
+            raise ImagingError("at most 8 record components")
+        cfg.n_comp = len(codes)
+        for k, c in enumerate(codes):
+            cfg.comp[k] = c
+        return cfg
+
+    def _post_args(self) -> dict:
+        im = self.imager
+        condition = str(im.config.condition).lower()
+        g = self.model.grid
+        return dict(dx=g.dx, dz=g.dz, by_illum=condition == "normalized" and bool(im.config.illumination),
+                    by_rillum=bool(im.config.receiver_normalization), eps=float(im.config.eps),
+                    laplacian=bool(im.config.laplacian), lowpass_fraction=float(im.config.lowpass_fraction),
+                    npml=self.spec.npml, boundary=self.spec.boundary)
+
+    def migrate(self, shot: Any, *, wavelet: np.ndarray | None = None, preprocess: Callable | None = None,
+                modes: tuple[str, ...] = ("pp",)) -> list[ImageResult]:
+        im = self.imager
+        record = im._prepare_record(shot, self.spec, preprocess)
+        if not record:
+            raise ImagingError("empty shot record; nothing to back-propagate")
+        w = im._prepare_wavelet(shot, self.spec, wavelet)
+        pairs, store, start_step = self._prepare(shot.source, shot.receivers, modes, len(w))
+        names = list(record)
+        cfg = self._config(pairs, names, store, start_step, len(w))
+        rec = np.ascontiguousarray(np.stack([np.asarray(record[n], dtype=np.float32) for n in names]))
+        g = self.model.grid
+        acc = np.zeros((3, len(pairs), g.nz, g.nx))
+        _lib.check(_lib.lib().ertm_migrate(self.prop.handle, self.back.handle, cfg, _lib.ptr(w), _lib.ptr(rec),
+                                          _lib.ptr(acc[0]), _lib.ptr(acc[1]), _lib.ptr(acc[2])), "migrate")
+        self.prop._psi_allocated = self.back._psi_allocated = True
+        condition = str(im.config.condition).lower()
+        results = []
+        for k, m in enumerate(modes):
+            image = postprocess_image(acc[0, k], acc[1, k], acc[2, k], **self._post_args())
+            res = ImageResult(image=image, grid=g, mode=m,
+                              meta=im._meta(self.spec, self.engine, shot, store, condition, start_step, self.prop,
+                                            self.back, m))
+            res.validate()
+            results.append(res)
+        return results
+
+    def migrate_device(self, source: Any, receivers: Any, record, names: list[str], wavelet: np.ndarray, *,
+                       modes: tuple[str, ...] = ("pp",), stream: int | None = None):
+        """Device-resident form: ``record`` is a contiguous device tensor
+        (n_comp, nt, nrec) float32 already aligned to the propagation dt;
+        returns a device tensor (n_modes, nz, nx) float32 of final images."""
+        import torch
+
+        w = np.ascontiguousarray(wavelet, dtype=np.float32)
+        pairs, store, start_step = self._prepare(source, receivers, modes, len(w))
+        cfg = self._config(pairs, names, store, start_step, len(w))
+        g = self.model.grid
+        dev = record.device
+        acc = torch.empty((3, len(pairs), g.nz, g.nx), dtype=torch.float64, device=dev)
+        _lib.check(_lib.lib().ertm_migrate(self.prop.handle, self.back.handle, cfg, _lib.ptr(w), _lib.ptr(record),
+                                          _lib.ptr(acc[0]), _lib.ptr(acc[1]), _lib.ptr(acc[2])), "migrate")
+        self.prop._psi_allocated = self.back._psi_allocated = True
+        out = torch.empty((len(pairs), g.nz, g.nx), dtype=torch.float32, device=dev)
+        a = self._post_args()
+        for k in range(len(pairs)):
+            _lib.check(_lib.lib().ertm_postprocess(
+                g.nz, g.nx, float(a["dx"]), float(a["dz"]), _lib.ptr(acc[0, k]), _lib.ptr(acc[1, k]),
+                _lib.ptr(acc[2, k]), int(a["by_illum"]), int(a["by_rillum"]), a["eps"], int(a["laplacian"]),
+                a["lowpass_fraction"], int(a["npml"]), int(a["boundary"] == "cpml"), _lib.ptr(out[k]), stream),
+                "postprocess")
+        return out
+
+
 def build_imager(config: ImagingConfig, solver_config: SolverConfig | None = None,
                  q_config: QConfig | None = None) -> RTMImager:
     return RTMImager(config, solver_config, q_config)
@@ -347,4 +416,4 @@ def build_imager(config: ImagingConfig, solver_config: SolverConfig | None = Non
 
 __all__ = ["WAVE_MODES", "zero_lag_condition", "normalized_terms", "excitation_terms", "CheckpointStore",
            "checkpoint_interval", "record_source_wavefield", "replay_block", "postprocess_image", "RTMImager",
-           "build_imager", "SolverError"]
+           "ShotMigrator", "build_imager", "SolverError"]

@@ -85,6 +85,8 @@ typedef struct ertm_prop_info {
   int64_t field_bytes;       /* reference field bytes (n_fields · nzp · nxp · 4) */
   int64_t step_index;
   int32_t n_fields, clipped, lowpass_steps, n_receivers;
+  int32_t fast_div_x, fast_div_z;  /* 1: division by dx / dz uses the verified fast form */
+  int32_t tile_rows, reserved;
 } ertm_prop_info;
 
 typedef struct ertm_migrate_config {
@@ -92,10 +94,11 @@ typedef struct ertm_migrate_config {
   int32_t nt_spec;           /* spec.nt: excitation backward loop end (imaging.py:286-288) */
   int32_t interval;          /* checkpoint interval (imaging.py:121-124) */
   int32_t condition;         /* ERTM_COND_* */
-  int32_t illumination;      /* accumulate S² and R² (normalized or receiver normalisation) */
+  int32_t illumination;      /* bit 0: accumulate S² (normalized + illumination);
+                                bit 1: accumulate R² (receiver normalisation) */
   int32_t start_step;        /* cross-correlation starts here (imaging.py:268-277) */
   int32_t separation;        /* ERTM_SEP_* (elastic) */
-  int32_t n_images;          /* 1..4 images sharing one forward/replay/backward pass */
+  int32_t n_images;          /* 1..2 images sharing one forward/replay/backward pass */
   int32_t src_wave[4];       /* ERTM_WAVE_* per image */
   int32_t rcv_wave[4];
   int32_t accum;             /* ERTM_ACCUM_* (excitation is always FP64) */
@@ -108,6 +111,16 @@ const char* ertm_last_error(void);
 int32_t ertm_version(void);
 /* Select the device and check it is sm_100 (no reference counterpart). */
 int32_t ertm_init(int32_t device);
+/* Instrumentation (no reference counterpart): kernels launched so far, and
+ * CUDA-event timing of the stencil phases of every `every`-th step on the
+ * stream they run on; ertm_profile_read returns the summed milliseconds and
+ * the number of timed steps since the last ertm_profile_stencil call. */
+int64_t ertm_launch_count(void);
+/* Pin the stencil tile height (8, 16 or 32 rows; 0 = automatic) for
+ * propagators created afterwards — the autotuner's knob (order 8 only). */
+int32_t ertm_set_tile_rows(int32_t rows);
+int32_t ertm_profile_stencil(int32_t enable, int32_t every);
+int32_t ertm_profile_read(double* total_ms, int64_t* samples);
 
 /* propagators ------------------------------------------------------------ */
 /* Replaces AcousticPropagator/ViscoacousticPropagator/ElasticPropagator
