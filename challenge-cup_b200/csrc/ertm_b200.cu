@@ -923,6 +923,51 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
   CK(cudaStreamSynchronize(st));
 }
 
+// --------------------------------------------------------------------------
+// Allocation-free stacking (ertm_stack_noalloc)
+// --------------------------------------------------------------------------
+// Callers that cannot allocate device memory — a serving process whose whole
+// device memory is carved up by its own pool at start-up, a host framework
+// that owns every allocation, or code that must not trigger the implicit
+// device synchronisation cudaMalloc/cudaFree can cause — still need the
+// per-shot-normalised stack.  This variant keeps its scratch in file-scope
+// device arrays: one chunk of float64 sums (the image is stacked chunk by
+// chunk) and one max|·| word per image.  Every GPU that loads this library
+// holds these 2 MiB + 4 KiB until the process exits.
+constexpr int64_t kStackChunk = 1 << 18;     // pixels per pass
+constexpr int kStackMaxImages = 1024;
+static __device__ __align__(256) double g_stack_sum[kStackChunk];
+static __device__ __align__(256) unsigned int g_stack_scale[kStackMaxImages];
+
+struct StackScratch {
+  double* sum = nullptr;
+  unsigned int* scale = nullptr;
+};
+std::map<int, StackScratch> g_stack_scratch;
+std::mutex g_stack_mutex;
+
+// Device addresses of the scratch arrays for the current device; looked up
+// once per device (the host-side names are not device addresses).
+StackScratch stack_scratch() {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_stack_mutex);
+  auto it = g_stack_scratch.find(dev);
+  if (it != g_stack_scratch.end()) return it->second;
+  StackScratch s;
+  CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&s.sum), g_stack_sum));
+  CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&s.scale), g_stack_scale));
+  g_stack_scratch[dev] = s;
+  return s;
+}
+
+void require_device_pointer(const void* p, const char* what) {
+  cudaPointerAttributes a{};
+  CK(cudaPointerGetAttributes(&a, p));
+  REQUIRE(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged,
+          std::string(what) + " must be device memory (ertm_stack_noalloc copies nothing through the host)");
+}
+
 }  // namespace
 
 // ==========================================================================
@@ -1342,6 +1387,38 @@ int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int3
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
     CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_stack_noalloc(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
+                           void* stream) {
+  return guarded([&] {
+    REQUIRE(n_images >= 1 && n >= 1 && images && out, "bad arguments");
+    REQUIRE(n_images <= kStackMaxImages,
+            "ertm_stack_noalloc stacks at most " + std::to_string(kStackMaxImages) + " images per call");
+    require_device_pointer(out, "out");
+    for (int k = 0; k < n_images; ++k) require_device_pointer(images[k], "every image");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n_images == 1) {
+      CK(cudaMemcpyAsync(out, images[0], n * 4, cudaMemcpyDeviceToDevice, st));
+      return;
+    }
+    const StackScratch S = stack_scratch();
+    // the scratch keeps the previous call's contents: clear what must start at zero
+    CK(cudaMemsetAsync(S.scale, 0, sizeof(unsigned int) * n_images, st));
+    if (normalize) {
+      const unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 1184);
+      for (int k = 0; k < n_images; ++k) k_absmax_f32<<<g, 256, 0, st>>>(images[k], n, S.scale + k);
+    }
+    for (int64_t off = 0; off < n; off += kStackChunk) {
+      const int64_t len = std::min<int64_t>(kStackChunk, n - off);
+      const unsigned g = (unsigned)((len + 255) / 256);
+      CK(cudaMemsetAsync(S.sum, 0, sizeof(double) * len, st));
+      for (int k = 0; k < n_images; ++k)
+        k_stack_add<<<g, 256, 0, st>>>(images[k] + off, len, S.scale + k, normalize, S.sum);
+      k_stack_finish<<<g, 256, 0, st>>>(S.sum, len, n_images, out + off);
+    }
+    CK(cudaGetLastError());
   });
 }
 

@@ -88,6 +88,7 @@ _SIGNATURES = {
     "ertm_postprocess": (_I32, [_I32, _I32, C.c_double, C.c_double, _P, _P, _P, _I32, _I32, C.c_double,
                                 _I32, C.c_double, _I32, _I32, _P, _P]),
     "ertm_stack": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
+    "ertm_stack_noalloc": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -185,6 +185,21 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream);
 
+/* No counterpart in the reference.  Same result as ertm_stack, but it
+ * allocates nothing, for callers that cannot allocate device memory: a
+ * serving process that carves all device memory into its own pool at start-up,
+ * a host framework that owns every allocation, or code that must avoid the
+ * device-wide synchronisation cudaMalloc/cudaFree may cause.  images (a host
+ * array of n_images device pointers) and out must be device memory; more
+ * than 1024 images per call is rejected with an error.  Scratch lives in
+ * static device arrays (2 MiB of float64 sums + 4 KiB), held by every GPU that
+ * loads the library until the process exits; the first call on a device looks
+ * up their addresses (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  Work is enqueued on `stream`; calls that overlap on the GPU
+ * share the scratch and race, so order them on one stream. */
+int32_t ertm_stack_noalloc(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif
