@@ -277,97 +277,112 @@ def run_reference(args, dist: Dist) -> None:
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args, dist: Dist) -> None:
+    import ctypes as C
+
     import torch
 
     from ertm_b200 import _lib
+    from ertm_b200.batch import migrate_device_batch
     from ertm_b200.imaging import ShotMigrator
+    from ertm_b200.propagation import source_wavelet
     from ertm_b200.stacking import stack_images
     from ertm_b200.types import ShotRecord
 
     dev = dist.local
     torch.cuda.set_device(dev)
-    _lib.lib(dev)
     L = _lib.lib(dev)
     wl = build_workload(args, dist.rank)
     imager, solver = imager_for(wl)
     shots = synthesize(wl, solver)
     names = list(wl.components)
     rec_dev = [torch.from_numpy(np.stack([s.components[n] for n in names])).cuda() for s in shots]
-    from ertm_b200.propagation import source_wavelet
     wavelets = [source_wavelet(s, wl.dt, wl.nt) for s in wl.sources]
-    mig = ShotMigrator(imager, wl.model)
     g = wl.model.grid
     n_modes = len(wl.modes)
-    stack_out = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float32, device="cuda")
+    n_shots = len(wl.sources)
+    plain_mig = ShotMigrator(imager, wl.model)                       # one propagator pair, reused
+    batch_migs = [ShotMigrator(imager, wl.model) for _ in range(n_shots)]  # one pair per shot
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
 
-    import ctypes as C
-
-    def device_job():
-        imgs = [mig.migrate_device(src, wl.receivers, rec_dev[i], names, wavelets[i], modes=wl.modes)
-                for i, src in enumerate(wl.sources)]
+    def stack(imgs, out):
         for k in range(n_modes):
             ptrs = (C.c_void_p * len(imgs))(*[im[k].data_ptr() for im in imgs])
-            _lib.check(L.ertm_stack(len(imgs), g.nz * g.nx, C.cast(ptrs, C.c_void_p), 1, stack_out[k].data_ptr(),
-                                    None), "stack")
-        return stack_out
+            _lib.check(L.ertm_stack(len(imgs), g.nz * g.nx, C.cast(ptrs, C.c_void_p), 1, out[k].data_ptr(), None),
+                       "stack")
+        return out
 
-    for _ in range(args.warmup):
-        device_job()
-    torch.cuda.synchronize()
-    clocks = Clocks(dev)
-    _lib.check(L.ertm_profile_stencil(1, 8), "profile")
-    launches0 = L.ertm_launch_count()
-    times = []
-    dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        device_job()
-        e1.record()
+    out_plain = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float32, device="cuda")
+    out_batch = torch.empty_like(out_plain)
+
+    def plain_job():
+        imgs = [plain_mig.migrate_device(src, wl.receivers, rec_dev[i], names, wavelets[i], modes=wl.modes)
+                for i, src in enumerate(wl.sources)]
+        return stack(imgs, out_plain)
+
+    def batch_job():
+        imgs = migrate_device_batch(imager, batch_migs, wl.sources, [wl.receivers] * n_shots, rec_dev, names,
+                                    wavelets, modes=wl.modes)
+        return stack(imgs, out_batch)
+
+    def timed(job, steps, profile: bool):
+        for _ in range(args.warmup):
+            job()
         torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
-    dist.barrier()
-    torch.cuda.synchronize()
+        if profile:
+            _lib.check(L.ertm_profile_stencil(1, 4), "profile")
+        launches0 = L.ertm_launch_count()
+        times = []
+        dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            job()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        dist.barrier()
+        torch.cuda.synchronize()
+        return times, int(L.ertm_launch_count() - launches0)
+
+    # plain one-shot path (reported beside the batched form)
+    plain_times, _ = timed(plain_job, args.steps, False)
+    clocks = Clocks(dev)
+    clocks.start()
+    times, launches = timed(batch_job, args.steps, True)
     clk = clocks.stop()
-    launches = int(L.ertm_launch_count() - launches0)
-    tot, cnt = C.c_double(), C.c_int64()
-    _lib.check(L.ertm_profile_read(C.byref(tot), C.byref(cnt)), "profile read")
+    tot, cnt, byt = C.c_double(), C.c_int64(), C.c_double()
+    _lib.check(L.ertm_profile_read(C.byref(tot), C.byref(cnt), C.byref(byt)), "profile read")
     _lib.check(L.ertm_profile_stencil(0, 1), "profile off")
-    step_ms = float(tot.value) / max(int(cnt.value), 1)
+    same = bool(torch.equal(out_plain, out_batch))
 
     total_ms = dist.max(float(sum(times)))
-    shots_total = len(wl.sources) * dist.world * args.steps
+    plain_ms = dist.max(float(sum(plain_times)))
+    shots_total = n_shots * dist.world * args.steps
     value = shots_total / (total_ms / 1e3)
+    plain_value = shots_total / (plain_ms / 1e3)
     cell_updates = 3 * wl.nt * wl.cells * shots_total
-    # combined stack across ranks: the only collective
     if dist.world > 1:
-        dist.sum_(stack_out)
-        stack_out /= dist.world
+        dist.sum_(out_batch)      # the only collective: the stacks of all ranks
+        out_batch /= dist.world
 
     # end to end through the public API: pinned host records in, host image out
     pinned = [{n: torch.from_numpy(s.components[n]).pin_memory().numpy() for n in names} for s in shots]
     e2e_times = []
-    h2d = d2h = 0
     for _ in range(args.e2e_steps):
         dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        per_mode = {m: [] for m in wl.modes}
-        for i, s in enumerate(shots):
-            shot = ShotRecord(data=pinned[i][names[0]], dt=s.dt, t=s.t, receivers=s.receivers, source=s.source,
-                              components=pinned[i])
-            for res in imager.migrate_modes(shot, wl.model, modes=wl.modes):
-                per_mode[res.mode].append(res)
-        stacked = {m: stack_images(v, normalize=True).image for m, v in per_mode.items()}
+        from ertm_b200.batch import BatchMigrator
+        host_shots = [ShotRecord(data=pinned[i][names[0]], dt=s.dt, t=s.t, receivers=s.receivers, source=s.source,
+                                 components=pinned[i]) for i, s in enumerate(shots)]
+        per_shot = BatchMigrator(imager).migrate_shots(host_shots, wl.model, modes=wl.modes)
+        stacked = {m: stack_images([r[k] for r in per_shot], normalize=True).image for k, m in enumerate(wl.modes)}
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
         assert all(np.isfinite(v).all() for v in stacked.values())
     npix = g.nx * g.nz
-    n_shots = len(shots)
     comp_bytes = len(names) * wl.nt * wl.receivers.nrec * 4
     model_bytes = 3 * npix * 4 * 2                      # vp, vs, rho per propagator, two propagators
     h2d = n_shots * (comp_bytes + model_bytes + 3 * n_modes * npix * 8 + wl.nt * 4)
@@ -376,8 +391,8 @@ def run_ours(args, dist: Dist) -> None:
     e2e_value = n_shots * dist.world / e2e_s
 
     peak, peak_kind = measured_hbm_peak()
-    bytes_step = step_bytes(mig.prop)
-    achieved = bytes_step / (step_ms * 1e-3) / 1e9
+    step_ms = float(tot.value) / max(int(cnt.value), 1)
+    achieved = float(byt.value) / (float(tot.value) * 1e-3) / 1e9 if tot.value > 0 else 0.0
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cs = cpu_sample(args.config, args.cpu_sample_steps)
@@ -392,16 +407,22 @@ def run_ours(args, dist: Dist) -> None:
         "data": "synthetic: seeded layered model with cavities and a fault; records from the GPU forward model",
         "config": {"workload": wl.name, "config": args.config, "nx": g.nx, "nz": g.nz, "dx": g.dx, "nt": wl.nt,
                    "dt": wl.dt, "engine": wl.engine, "modes": list(wl.modes), "condition": wl.condition,
-                   "separation": wl.separation, "shots_per_rank": len(wl.sources), "receivers": wl.receivers.nrec,
+                   "separation": wl.separation, "shots_per_rank": n_shots, "receivers": wl.receivers.nrec,
                    "components": names, "accumulation": "fp64", "l2": "flushed between steps (256 MiB write)",
-                   "path": "plain: one shot at a time, PP and PS from one pass", "parallelism": f"shots x{dist.world}"},
+                   "path": "batched: all shots of the job in lockstep ticks (form b)",
+                   "parallelism": f"shots x{dist.world}"},
         "gcell_updates_per_s": cell_updates / (total_ms / 1e3) / 1e9,
+        "plain": {"value": plain_value, "unit": "shots/s", "ms_per_step": plain_ms / args.steps,
+                  "gcell_updates_per_s": cell_updates / (plain_ms / 1e3) / 1e9,
+                  "path": "one shot at a time, PP and PS from one pass"},
+        "batched_over_plain": value / plain_value,
+        "batched_equals_plain": same,
         "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": committed_traffic(f"{wl.engine}_step"),
-                     "kernel": f"{wl.engine} step (velocity + stress kernels)",
-                     "bytes_per_step": bytes_step, "step_us": step_ms * 1e3, "timed_steps": int(cnt.value),
-                     "peak_source": peak_kind},
+                     "kernel": f"{wl.engine} velocity + stress launches of a batched tick",
+                     "bytes_per_tick": float(byt.value) / max(int(cnt.value), 1), "tick_us": step_ms * 1e3,
+                     "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,

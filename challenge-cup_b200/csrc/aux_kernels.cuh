@@ -176,6 +176,41 @@ __global__ void k_inject(const DevProp* props, int pi, InjectPlanDev plan, const
   *f = acc;
 }
 
+// Injection for many propagators in one launch (batched ticks): item k owns
+// global cells [cell0, cell0 + n_cells).
+struct InjectItem {
+  InjectPlanDev plan;
+  const DevProp* prop;
+  const float* record;
+  int64_t time_offset;
+  int32_t cell0;
+  int32_t pad_;
+};
+struct InjectBatch {
+  int32_t n;
+  int32_t pad_;
+  InjectItem it[MAX_BATCH_WORKS];
+};
+
+__global__ void k_inject_batch(InjectBatch B) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  int lo = 0, hi = B.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (B.it[mid].cell0 <= u) lo = mid; else hi = mid - 1;
+  }
+  const InjectItem& I = B.it[lo];
+  const int v = u - I.cell0;
+  if (v < 0 || v >= I.plan.n_cells) return;
+  float* f = I.prop->f[I.plan.cell_field[v]] + I.plan.cell_index[v];
+  float acc = *f;
+  for (int k = I.plan.start[v]; k < I.plan.start[v + 1]; ++k) {
+    const double val = (double)I.record[I.plan.src[k] + I.time_offset];
+    acc = __double2float_rn(dadd((double)acc, dmul(dmul(val, I.plan.wa[k]), I.plan.wb[k])));
+  }
+  *f = acc;
+}
+
 // Single-cell add (elastic force_z source lands on vz after the stress phase,
 // propagation.py:872-873).
 __global__ void k_point_add(float* f, int64_t idx, float amp) {

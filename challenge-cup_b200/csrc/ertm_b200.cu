@@ -73,9 +73,13 @@ struct StencilProfile {
   bool on = false;
   int every = 8;
   int64_t counter = 0;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  struct Sample {
+    cudaEvent_t e0, e1;
+    double bytes;
+  };
+  std::vector<Sample> pending;
   std::vector<cudaEvent_t> pool;
-  double total_ms = 0.0;
+  double total_ms = 0.0, total_bytes = 0.0;
   int64_t samples = 0;
   cudaEvent_t get() {
     if (!pool.empty()) {
@@ -90,14 +94,27 @@ struct StencilProfile {
   void drain() {
     for (auto& pr : pending) {
       float ms = 0.f;
-      CK(cudaEventSynchronize(pr.second));
-      CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      CK(cudaEventSynchronize(pr.e1));
+      CK(cudaEventElapsedTime(&ms, pr.e0, pr.e1));
       total_ms += ms;
+      total_bytes += pr.bytes;
       ++samples;
-      pool.push_back(pr.first);
-      pool.push_back(pr.second);
+      pool.push_back(pr.e0);
+      pool.push_back(pr.e1);
     }
     pending.clear();
+  }
+  // Bracket the stencil launches of one step or tick (every `every`-th call).
+  bool begin(cudaStream_t st, cudaEvent_t& e0) {
+    if (!on || (counter++ % every) != 0) return false;
+    e0 = get();
+    CK(cudaEventRecord(e0, st));
+    return true;
+  }
+  void end(cudaStream_t st, cudaEvent_t e0, double bytes) {
+    cudaEvent_t e1 = get();
+    CK(cudaEventRecord(e1, st));
+    pending.push_back({e0, e1, bytes});
   }
 };
 StencilProfile g_prof;
@@ -415,27 +432,28 @@ InjectPlanHost& inject_plan(Prop& P, const std::vector<int>& comps, int64_t nt) 
 // --------------------------------------------------------------------------
 // stepping
 // --------------------------------------------------------------------------
-template <int M, int BZ, int R>
-void launch_step_shape(int engine, const DevProp* d, const WorkSet& ws, int blocks, cudaStream_t st) {
+template <int M, int BZ, int R, class WS>
+void launch_step_shape(int engine, const DevProp* d, const WS& ws, int blocks, cudaStream_t st) {
   const dim3 blk(XT, BZ);
   switch (engine) {
     case ENGINE_ACOUSTIC:
-      k_pressure_velocity<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
-      k_pressure_stress<M, BZ, R, false><<<blocks, blk, 0, st>>>(d, ws);
+      k_pressure_velocity<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
+      k_pressure_stress<M, BZ, R, false, WS><<<blocks, blk, 0, st>>>(d, ws);
       break;
     case ENGINE_VISCO:
-      k_pressure_velocity<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
-      k_pressure_stress<M, BZ, R, true><<<blocks, blk, 0, st>>>(d, ws);
+      k_pressure_velocity<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
+      k_pressure_stress<M, BZ, R, true, WS><<<blocks, blk, 0, st>>>(d, ws);
       break;
     default:
-      k_elastic_velocity<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
-      k_elastic_stress<M, BZ, R><<<blocks, blk, 0, st>>>(d, ws);
+      k_elastic_velocity<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
+      k_elastic_stress<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
   }
 }
 
 // Both phases of one step for every work in ws (one tile height for all):
 // TZ 8 = 8×8 threads, 16 = 8×16 threads, 32 = 8×16 threads × 2 rows.
-void launch_step(int M, int tz, int engine, const DevProp* d, const WorkSet& ws, int blocks, cudaStream_t st) {
+template <class WS>
+void launch_step(int M, int tz, int engine, const DevProp* d, const WS& ws, int blocks, cudaStream_t st) {
   if (M == 4) {
     if (tz == 32) launch_step_shape<4, 16, 2>(engine, d, ws, blocks, st);
     else if (tz == 16) launch_step_shape<4, 16, 1>(engine, d, ws, blocks, st);
@@ -515,10 +533,22 @@ void lowpass_field(Prop& P, float* f, double cutoff) {
   k_f64_to_f32<<<g2, b2, 0, P.st>>>(P.fft_real.as<double>(), f, P.h.ld, nz, nx);
 }
 
-// One step of one propagator.  Amplitude: wavelet[t] from device memory when
+// Algorithmic HBM bytes of one propagator step: each state array read and
+// written once, each per-cell coefficient read once, CPML strips read and
+// written (SURVEY-style accounting; the viscoacoustic a_l count as per-cell
+// coefficients although they are read from a per-Q table here).
+double step_bytes(const Prop& P) {
+  const double npad = (double)P.h.nzp * P.h.nxp;
+  const int n_state = P.h.n_fields;
+  const int n_coef = P.h.engine == ENGINE_ACOUSTIC ? 3 : (P.h.engine == ENGINE_ELASTIC ? 5 : 3 + 2 * P.h.L);
+  const double strips = (double)P.n_psi * ((double)P.h.wx * P.h.nzp + (double)P.h.hz_rows * P.h.nxp);
+  return npad * (8.0 * n_state + 4.0 * n_coef) + 8.0 * strips;
+}
+
+// The StepWork of one step.  Amplitude: wavelet[t] from device memory when
 // `wave` is given, else amp64 (float32 for the field, float32(amp64/K_R) for
 // the viscoacoustic strain).  `epi` is fused into the stress phase.
-void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, const Epilogue* epi = nullptr) {
+StepWork make_work(const Prop& P, double amp64, const float* wave, int t, const Epilogue* epi) {
   StepWork w{};
   w.prop = 0;
   w.tile0 = 0;
@@ -534,19 +564,13 @@ void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, co
   const bool comp = P.h.engine == ENGINE_VISCO && P.cfg.compensation;
   w.flags = comp ? STEP_PEAK : 0;
   if (epi) w.epi = *epi;
-  WorkSet ws{nullptr, 0, w};
-  const bool timed = g_prof.on && (g_prof.counter++ % g_prof.every == 0);
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (timed) {
-    e0 = g_prof.get();
-    e1 = g_prof.get();
-    CK(cudaEventRecord(e0, P.st));
-  }
-  launch_step(P.M, P.tz, P.h.engine, P.dp(), ws, P.tiles, P.st);
-  if (timed) {
-    CK(cudaEventRecord(e1, P.st));
-    g_prof.pending.emplace_back(e0, e1);
-  }
+  return w;
+}
+
+// What follows the stress phase of a step: the force_z source on vz, the
+// compensated viscoacoustic amplitude cap / low-pass (propagation.py:726-749,
+// evaluated with the step index before its increment), and the increment.
+void after_step(Prop& P, double amp64, const float* wave, int t) {
   const bool force_z = P.h.engine == ENGINE_ELASTIC && P.h.mech == MECH_FORCE_Z && P.h.src_iz >= 0;
   if (force_z && (wave || amp64 != 0.0)) {
     const int64_t idx = (int64_t)P.h.src_iz * P.h.ld + P.h.src_ix;
@@ -554,8 +578,7 @@ void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, co
     else k_point_add<<<1, 32, 0, P.st>>>(P.field(E_VZ), idx, (float)amp64);
     ++g_launches;
   }
-  if (comp) {
-    // propagation.py:726-749, evaluated with the step index before the increment
+  if (P.h.engine == ENGINE_VISCO && P.cfg.compensation) {
     const int64_t s = P.step_index;
     ++g_launches;
     if (s < 30) {
@@ -574,6 +597,15 @@ void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, co
   }
   CK(cudaGetLastError());
   ++P.step_index;
+}
+
+void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, const Epilogue* epi = nullptr) {
+  WorkSet1 ws{make_work(P, amp64, wave, t, epi)};
+  cudaEvent_t e0 = nullptr;
+  const bool timed = g_prof.begin(P.st, e0);
+  launch_step(P.M, P.tz, P.h.engine, P.dp(), ws, P.tiles, P.st);
+  if (timed) g_prof.end(P.st, e0, step_bytes(P));
+  after_step(P, amp64, wave, t);
 }
 
 void image_field(Prop& P, int wave, int sep, float* out) {
@@ -736,8 +768,37 @@ void launch_epilogue(const Prop& P, const Epilogue& E) {
   ++g_launches;
 }
 
-void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wavelet, const float* record,
-             double* num_out, double* illum_out, double* rillum_out) {
+// Per-shot state of one migration: device buffers, epilogue template and
+// the position in the schedule (used by the plain and the batched drivers).
+struct ShotRun {
+  Prop* F = nullptr;
+  Prop* B = nullptr;
+  ertm_migrate_config cfg{};
+  int fi = 0, bi = 0;          // indices of F and B in the launch's DevProp table
+  int nt = 0, iv = 1, n_states = 0;
+  int64_t nrec = 0;
+  size_t npix = 0;
+  bool excitation = false, kahan = false, want_ill = false, want_ril = false;
+  bool need_src[2] = {false, false}, need_rcv_s = false;
+  bool bwd_unfused = false, fwd_unfused = false;
+  DevBuf wave, rec, acc, ck, rbuf[2], running, peak;
+  std::vector<int64_t> ck_step;
+  InjectPlanHost* plan = nullptr;
+  double* num[MAX_EPI_IMAGES] = {};
+  double* ril[MAX_EPI_IMAGES] = {};
+  double* ill_slot[2] = {};
+  Epilogue base{};
+  double* out[3] = {};
+  // schedule: 0 forward, 1 replay/backward, 2 excitation map, 3 excitation backward, 4 done
+  int phase = 0;
+  int t_f = 0, rp_block = -1, rp_t = 0, bk_block = -1, bk_t = 0, replayed_below = 0;
+  int s_of(int b) const { return b * iv; }
+  int e_of(int b) const { return std::min((b + 1) * iv, nt); }
+};
+
+void prepare_run(ShotRun& R, Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wavelet,
+                 const float* record, double* num_out, double* illum_out, double* rillum_out, cudaStream_t st,
+                 int n_buffers) {
   REQUIRE(F.h.engine == B.h.engine && F.h.nz == B.h.nz && F.h.nx == B.h.nx, "fwd/back mismatch");
   REQUIRE(cfg.nt >= 1 && cfg.interval >= 1 && cfg.nt_spec >= 1, "bad nt/interval");
   REQUIRE(cfg.n_images >= 1 && cfg.n_images <= MAX_EPI_IMAGES, "n_images must be 1..2");
@@ -747,180 +808,428 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
     REQUIRE((cfg.src_wave[k] == 0 || cfg.src_wave[k] == 1) && (cfg.rcv_wave[k] == 0 || cfg.rcv_wave[k] == 1) &&
                 (F.h.engine == ENGINE_ELASTIC || (cfg.src_wave[k] == 0 && cfg.rcv_wave[k] == 0)),
             "wave not available for this engine");
-  const bool excitation = cfg.condition == ERTM_COND_EXCITATION;
-  cudaStream_t st = F.st;
-  if (B.st != st) {
-    CK(cudaStreamSynchronize(B.st));
-    B.st = st;
-  }
-  const int nt = cfg.nt, iv = cfg.interval;
-  const int n_states = (nt + iv - 1) / iv;
-  const size_t npix = (size_t)F.h.nz * F.h.nx;
-  const int nimg = cfg.n_images;
-  const bool kahan = cfg.accum == ERTM_ACCUM_KAHAN && !excitation;
-  const bool want_ill = (cfg.illumination & 1) && !excitation;
-  const bool want_ril = (cfg.illumination & 2) != 0;
-  // accumulators
-  DevBuf acc(npix * 8 * (2 * nimg + 2), st);
-  CK(cudaMemsetAsync(acc.p, 0, acc.bytes, st));
-  double* num[MAX_EPI_IMAGES] = {};
-  double* ril[MAX_EPI_IMAGES] = {};
-  double* ill_slot[2] = {acc.as<double>() + 2 * nimg * npix, acc.as<double>() + (2 * nimg + 1) * npix};
-  for (int k = 0; k < nimg; ++k) {
-    num[k] = acc.as<double>() + k * npix;
-    ril[k] = acc.as<double>() + (nimg + k) * npix;
-  }
-  // wavelet on the device; record + injection plan on the backward propagator
-  DevBuf dwave((size_t)nt * 4, st);
-  upload(dwave.p, wavelet, (size_t)nt * 4, st);
-  std::vector<int> comps(cfg.comp, cfg.comp + cfg.n_comp);
-  const int64_t nrec = (int64_t)B.rx.size();
-  DevBuf rec((size_t)cfg.n_comp * cfg.nt_spec * nrec * 4, st);
-  upload(rec.p, record, rec.bytes, st);
-  InjectPlanHost* plan = comps.empty() ? nullptr : &inject_plan(B, comps, cfg.nt_spec);
-  auto inject = [&](int t) {
-    if (!plan || plan->n_cells == 0) return;
-    ++g_launches;
-    k_inject<<<(plan->n_cells + 127) / 128, 128, 0, st>>>(B.dp(), 0, plan->dev(), rec.as<float>(),
-                                                          (int64_t)t * nrec);
-  };
-  // forward with checkpoints (imaging.py:113-137)
-  DevBuf ck((size_t)n_states * F.state_floats * 4, st);
-  std::vector<int64_t> ck_step(n_states);
-  for (int t = 0; t < nt; ++t) {
-    step_once(F, 0.0, dwave.as<float>(), t);
-    if (t % iv == 0) {
-      CK(cudaMemcpyAsync(ck.as<float>() + (size_t)(t / iv) * F.state_floats, F.state.p, F.state_floats * 4,
-                         cudaMemcpyDeviceToDevice, st));
-      ck_step[t / iv] = F.step_index;
+  for (Prop* P : {&F, &B})
+    if (P->st != st) {
+      CK(cudaStreamSynchronize(P->st));
+      P->st = st;
     }
-  }
-  auto restore = [&](int b) {
-    CK(cudaMemcpyAsync(F.state.p, ck.as<float>() + (size_t)b * F.state_floats, F.state_floats * 4,
-                       cudaMemcpyDeviceToDevice, st));
-    F.step_index = ck_step[b];
-  };
-  // epilogue templates
-  Epilogue base{};
-  base.sep = cfg.separation;
-  base.n_images = nimg;
-  base.kahan = kahan ? 1 : 0;
-  bool need_src[2] = {false, false}, need_rcv_s = false;
+  R.F = &F;
+  R.B = &B;
+  R.cfg = cfg;
+  R.nt = cfg.nt;
+  R.iv = cfg.interval;
+  R.n_states = (cfg.nt + cfg.interval - 1) / cfg.interval;
+  R.npix = (size_t)F.h.nz * F.h.nx;
+  R.excitation = cfg.condition == ERTM_COND_EXCITATION;
+  R.kahan = cfg.accum == ERTM_ACCUM_KAHAN && !R.excitation;
+  R.want_ill = (cfg.illumination & 1) && !R.excitation;
+  R.want_ril = (cfg.illumination & 2) != 0;
+  R.out[0] = num_out;
+  R.out[1] = illum_out;
+  R.out[2] = rillum_out;
+  const size_t npix = R.npix;
+  const int nimg = cfg.n_images;
+  R.acc = DevBuf(npix * 8 * (2 * nimg + 2), st);
+  CK(cudaMemsetAsync(R.acc.p, 0, R.acc.bytes, st));
+  R.ill_slot[0] = R.acc.as<double>() + 2 * nimg * npix;
+  R.ill_slot[1] = R.acc.as<double>() + (2 * nimg + 1) * npix;
   for (int k = 0; k < nimg; ++k) {
-    base.src_slot[k] = cfg.src_wave[k];
-    base.rcv_wave[k] = cfg.rcv_wave[k];
-    base.num[k] = num[k];
-    base.ril[k] = want_ril ? ril[k] : nullptr;
-    need_src[cfg.src_wave[k]] = true;
-    need_rcv_s |= cfg.rcv_wave[k] == 1;
+    R.num[k] = R.acc.as<double>() + k * npix;
+    R.ril[k] = R.acc.as<double>() + (nimg + k) * npix;
+  }
+  R.wave = DevBuf((size_t)R.nt * 4, st);
+  upload(R.wave.p, wavelet, (size_t)R.nt * 4, st);
+  std::vector<int> comps(cfg.comp, cfg.comp + cfg.n_comp);
+  R.nrec = (int64_t)B.rx.size();
+  R.rec = DevBuf((size_t)cfg.n_comp * cfg.nt_spec * R.nrec * 4, st);
+  upload(R.rec.p, record, R.rec.bytes, st);
+  R.plan = comps.empty() ? nullptr : &inject_plan(B, comps, cfg.nt_spec);
+  if (R.plan && R.plan->n_cells == 0) R.plan = nullptr;
+  R.ck = DevBuf((size_t)R.n_states * F.state_floats * 4, st);
+  R.ck_step.assign(R.n_states, 0);
+  Epilogue& E = R.base;
+  E = Epilogue{};
+  E.sep = cfg.separation;
+  E.n_images = nimg;
+  E.kahan = R.kahan ? 1 : 0;
+  for (int k = 0; k < nimg; ++k) {
+    E.src_slot[k] = cfg.src_wave[k];
+    E.rcv_wave[k] = cfg.rcv_wave[k];
+    E.num[k] = R.num[k];
+    E.ril[k] = R.want_ril ? R.ril[k] : nullptr;
+    R.need_src[cfg.src_wave[k]] = true;
+    R.need_rcv_s |= cfg.rcv_wave[k] == 1;
   }
   // each distinct source wave's illumination is accumulated once
   for (int k = 0; k < nimg; ++k) {
     bool first = true;
     for (int q = 0; q < k; ++q) first &= cfg.src_wave[q] != cfg.src_wave[k];
-    base.ill[k] = (want_ill && first) ? ill_slot[cfg.src_wave[k]] : nullptr;
+    E.ill[k] = (R.want_ill && first) ? R.ill_slot[cfg.src_wave[k]] : nullptr;
   }
-  // The fused epilogue sees the fields right after the stress phase; it is
-  // run stand-alone when something still changes them afterwards.
-  const bool bwd_unfused = B.h.engine == ENGINE_VISCO && B.cfg.compensation;
-  const bool fwd_force_z = F.h.engine == ENGINE_ELASTIC && F.h.mech == MECH_FORCE_Z && cfg.separation == 1;
-  auto fwd_step = [&](int t, const Epilogue& e) {
-    if (fwd_force_z) {
-      step_once(F, 0.0, dwave.as<float>(), t);
-      launch_epilogue(F, e);
-    } else {
-      step_once(F, 0.0, dwave.as<float>(), t, &e);
-    }
-  };
-  auto bwd_step = [&](const Epilogue& e) {
-    if (e.kind == EPI_NONE) {
-      step_once(B, 0.0);
-    } else if (bwd_unfused) {
-      step_once(B, 0.0);
-      launch_epilogue(B, e);
-    } else {
-      step_once(B, 0.0, nullptr, 0, &e);
-    }
-  };
-  if (!excitation) {
-    DevBuf rbuf((size_t)iv * 2 * npix * 4, st);
-    Epilogue store = base;
-    store.kind = EPI_STORE;
-    store.need_s = need_src[1] ? 1 : 0;
-    Epilogue image = base;
-    image.kind = EPI_IMAGE;
-    image.need_s = need_rcv_s ? 1 : 0;
-    image.illum = want_ill ? 1 : 0;
-    image.rillum = want_ril ? 1 : 0;
-    for (int b = n_states - 1; b >= 0; --b) {
-      const int s0 = b * iv, e0 = std::min((b + 1) * iv, nt);
-      restore(b);
-      for (int t = s0; t < e0; ++t) {
-        float* slot = rbuf.as<float>() + (size_t)(t - s0) * 2 * npix;
-        store.out[0] = need_src[0] ? slot : nullptr;
-        store.out[1] = need_src[1] ? slot + npix : nullptr;
-        fwd_step(t, store);
-      }
-      for (int t = e0 - 1; t >= s0; --t) {
-        inject(t);
-        const float* slot = rbuf.as<float>() + (size_t)(t - s0) * 2 * npix;
-        image.src[0] = slot;
-        image.src[1] = slot + npix;
-        image.cross = t >= cfg.start_step ? 1 : 0;
-        Epilogue e = image;
-        if (!e.cross && !e.illum && !e.rillum) e.kind = EPI_NONE;
-        bwd_step(e);
-      }
-    }
+  // The fused epilogue sees the fields right after the stress phase; it runs
+  // stand-alone when something still changes them afterwards.
+  R.bwd_unfused = B.h.engine == ENGINE_VISCO && B.cfg.compensation;
+  R.fwd_unfused = F.h.engine == ENGINE_ELASTIC && F.h.mech == MECH_FORCE_Z && cfg.separation == 1;
+  if (!R.excitation) {
+    for (int k = 0; k < n_buffers; ++k) R.rbuf[k] = DevBuf((size_t)R.iv * 2 * npix * 4, st);
   } else {
-    DevBuf running(npix * 4, st), peak((size_t)npix * 4, st);
-    CK(cudaMemsetAsync(running.p, 0, npix * 4, st));
-    CK(cudaMemsetAsync(peak.p, 0xff, npix * 4, st));  // −1
-    Epilogue track = base;
-    track.kind = EPI_EXC_TRACK;
-    track.running = running.as<float>();
-    track.peak_step = peak.as<int32_t>();
-    Epilogue image = track;
-    image.kind = EPI_EXC_IMAGE;
-    image.need_s = need_rcv_s ? 1 : 0;
-    for (int b = 0; b < n_states; ++b) {
-      const int s0 = b * iv, e0 = std::min((b + 1) * iv, nt);
-      restore(b);
-      for (int t = s0; t < e0; ++t) {
-        track.step = t;
-        fwd_step(t, track);
-      }
-    }
-    for (int b = n_states - 1; b >= 0; --b) {
-      const int s0 = b * iv, e0 = (b + 1 < n_states) ? (b + 1) * iv : cfg.nt_spec;
-      for (int t = e0 - 1; t >= s0; --t) {
-        inject(t);
-        Epilogue e = image;
-        e.step = t;
-        if (t < cfg.start_step) e.kind = EPI_NONE;
-        bwd_step(e);
-      }
-    }
-    // illumination = A² is set but never used by this condition (imaging.py:304, 328)
+    R.running = DevBuf(npix * 4, st);
+    R.peak = DevBuf(npix * 4, st);
+    CK(cudaMemsetAsync(R.running.p, 0, npix * 4, st));
+    CK(cudaMemsetAsync(R.peak.p, 0xff, npix * 4, st));  // −1
   }
-  CK(cudaGetLastError());
-  // outputs: per image, num/illum/rillum as float64
-  DevBuf tmp(kahan ? npix * 8 : 0, st);
-  auto out = [&](double* dst, const double* src) {
+}
+
+void save_checkpoint(ShotRun& R, int b, cudaStream_t st) {
+  CK(cudaMemcpyAsync(R.ck.as<float>() + (size_t)b * R.F->state_floats, R.F->state.p, R.F->state_floats * 4,
+                     cudaMemcpyDeviceToDevice, st));
+  R.ck_step[b] = R.F->step_index;
+}
+
+void restore_checkpoint(ShotRun& R, int b, cudaStream_t st) {
+  CK(cudaMemcpyAsync(R.F->state.p, R.ck.as<float>() + (size_t)b * R.F->state_floats, R.F->state_floats * 4,
+                     cudaMemcpyDeviceToDevice, st));
+  R.F->step_index = R.ck_step[b];
+}
+
+// Epilogues of the replay step at time t of block b and of the backward step at t.
+Epilogue replay_epilogue(const ShotRun& R, int b, int t) {
+  Epilogue e = R.base;
+  if (R.excitation) {
+    e.kind = EPI_EXC_TRACK;
+    e.running = R.running.as<float>();
+    e.peak_step = R.peak.as<int32_t>();
+    e.step = t;
+    return e;
+  }
+  float* slot = R.rbuf[b & (R.rbuf[1].p ? 1 : 0)].as<float>() + (size_t)(t - R.s_of(b)) * 2 * R.npix;
+  e.kind = EPI_STORE;
+  e.need_s = R.need_src[1] ? 1 : 0;
+  e.out[0] = R.need_src[0] ? slot : nullptr;
+  e.out[1] = R.need_src[1] ? slot + R.npix : nullptr;
+  return e;
+}
+
+Epilogue backward_epilogue(const ShotRun& R, int b, int t) {
+  Epilogue e = R.base;
+  if (R.excitation) {
+    e.kind = t >= R.cfg.start_step ? EPI_EXC_IMAGE : EPI_NONE;
+    e.need_s = R.need_rcv_s ? 1 : 0;
+    e.running = R.running.as<float>();
+    e.peak_step = R.peak.as<int32_t>();
+    e.step = t;
+    return e;
+  }
+  const float* slot = R.rbuf[b & (R.rbuf[1].p ? 1 : 0)].as<float>() + (size_t)(t - R.s_of(b)) * 2 * R.npix;
+  e.kind = EPI_IMAGE;
+  e.need_s = R.need_rcv_s ? 1 : 0;
+  e.illum = R.want_ill ? 1 : 0;
+  e.rillum = R.want_ril ? 1 : 0;
+  e.src[0] = slot;
+  e.src[1] = slot + R.npix;
+  e.cross = t >= R.cfg.start_step ? 1 : 0;
+  if (!e.cross && !e.illum && !e.rillum) e.kind = EPI_NONE;
+  return e;
+}
+
+void finish_run(ShotRun& R, cudaStream_t st) {
+  const size_t npix = R.npix;
+  DevBuf tmp(R.kahan ? npix * 8 : 0, st);
+  auto copy_out = [&](double* dst, const double* src) {
     const double* from = src;
-    if (kahan) {
+    if (R.kahan) {
       const float* s = reinterpret_cast<const float*>(src);
       k_kahan_to_f64<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(s, s + npix, tmp.as<double>(), (int64_t)npix);
       from = tmp.as<double>();
     }
     CK(cudaMemcpyAsync(dst, from, npix * 8, cudaMemcpyDefault, st));
   };
-  for (int k = 0; k < nimg; ++k) {
-    if (num_out) out(num_out + (size_t)k * npix, num[k]);
-    if (illum_out) out(illum_out + (size_t)k * npix, ill_slot[cfg.src_wave[k]]);
-    if (rillum_out) out(rillum_out + (size_t)k * npix, ril[k]);
+  for (int k = 0; k < R.cfg.n_images; ++k) {
+    if (R.out[0]) copy_out(R.out[0] + (size_t)k * npix, R.num[k]);
+    if (R.out[1]) copy_out(R.out[1] + (size_t)k * npix, R.ill_slot[R.cfg.src_wave[k]]);
+    if (R.out[2]) copy_out(R.out[2] + (size_t)k * npix, R.ril[k]);
   }
   CK(cudaStreamSynchronize(st));
+}
+
+void inject_one(ShotRun& R, int t, cudaStream_t st) {
+  if (!R.plan) return;
+  ++g_launches;
+  k_inject<<<(R.plan->n_cells + 127) / 128, 128, 0, st>>>(R.B->dp(), 0, R.plan->dev(), R.rec.as<float>(),
+                                                            (int64_t)t * R.nrec);
+}
+
+// Plain driver: one shot, steps one after the other (imaging.py:255-331).
+void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wavelet, const float* record,
+             double* num_out, double* illum_out, double* rillum_out) {
+  cudaStream_t st = F.st;
+  ShotRun R;
+  prepare_run(R, F, B, cfg, wavelet, record, num_out, illum_out, rillum_out, st, 1);
+  const float* dw = R.wave.as<float>();
+  auto fwd_step = [&](int t, const Epilogue& e) {
+    if (R.fwd_unfused) {
+      step_once(F, 0.0, dw, t);
+      launch_epilogue(F, e);
+    } else {
+      step_once(F, 0.0, dw, t, &e);
+    }
+  };
+  auto bwd_step = [&](const Epilogue& e) {
+    if (e.kind == EPI_NONE) {
+      step_once(B, 0.0);
+    } else if (R.bwd_unfused) {
+      step_once(B, 0.0);
+      launch_epilogue(B, e);
+    } else {
+      step_once(B, 0.0, nullptr, 0, &e);
+    }
+  };
+  // forward with checkpoints (imaging.py:113-137)
+  for (int t = 0; t < R.nt; ++t) {
+    step_once(F, 0.0, dw, t);
+    if (t % R.iv == 0) save_checkpoint(R, t / R.iv, st);
+  }
+  if (!R.excitation) {
+    for (int b = R.n_states - 1; b >= 0; --b) {
+      restore_checkpoint(R, b, st);
+      for (int t = R.s_of(b); t < R.e_of(b); ++t) fwd_step(t, replay_epilogue(R, b, t));
+      for (int t = R.e_of(b) - 1; t >= R.s_of(b); --t) {
+        inject_one(R, t, st);
+        bwd_step(backward_epilogue(R, b, t));
+      }
+    }
+  } else {
+    for (int b = 0; b < R.n_states; ++b) {
+      restore_checkpoint(R, b, st);
+      for (int t = R.s_of(b); t < R.e_of(b); ++t) fwd_step(t, replay_epilogue(R, b, t));
+    }
+    // backward over [0, nt_spec) (imaging.py:283-303); A² illumination is unused
+    for (int t = cfg.nt_spec - 1; t >= 0; --t) {
+      inject_one(R, t, st);
+      bwd_step(backward_epilogue(R, 0, t));
+    }
+  }
+  CK(cudaGetLastError());
+  finish_run(R, st);
+}
+
+// --------------------------------------------------------------------------
+// Batched driver (form (b)): many shots advance in lockstep ticks.  A tick
+// gives every unfinished shot at most one forward/replay step and one
+// backward step; all steps of a tick share one velocity and one stress launch
+// per (engine, order) group.  During the replay/backward phase the replay of
+// block b−1 (into one replay buffer) overlaps the backward pass over block b
+// (reading the other), so a shot needs ≈ 2·nt ticks instead of 3·nt steps.
+// Every propagator performs exactly the steps of the plain driver in the same
+// order, so the results are identical.
+// --------------------------------------------------------------------------
+struct TickItem {
+  ShotRun* run;
+  bool fwd;          // replay/forward propagator (else backward)
+  StepWork w;
+  bool unfused;      // epilogue runs after after_step
+  Epilogue epi;      // the epilogue (fused into w, or stand-alone)
+};
+
+void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStream_t st, double& bytes) {
+  if (items.empty()) return;
+  const Prop& P0 = items[0]->fwd ? *items[0]->run->F : *items[0]->run->B;
+  const int M = P0.M, engine = P0.h.engine;
+  for (size_t c0 = 0; c0 < items.size(); c0 += MAX_BATCH_WORKS) {
+    const size_t c1 = std::min(items.size(), c0 + MAX_BATCH_WORKS);
+    int64_t t32 = 0, t16 = 0, t8 = 0;
+    for (size_t k = c0; k < c1; ++k) {
+      const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
+      t32 += tiles_for(P.h, 32);
+      t16 += tiles_for(P.h, 16);
+      t8 += tiles_for(P.h, 8);
+    }
+    const int tz = choose_tz(M, 0, t32, t16, t8);
+    WorkSetB ws{};
+    ws.n = (int)(c1 - c0);
+    int tile0 = 0;
+    for (size_t k = c0; k < c1; ++k) {
+      const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
+      StepWork w = items[k]->w;
+      w.tile0 = tile0;
+      w.tiles_x = (P.h.nxp + TILE_X - 1) / TILE_X;
+      w.tiles = tiles_for(P.h, tz);
+      tile0 += w.tiles;
+      ws.w[k - c0] = w;
+      bytes += step_bytes(P);
+    }
+    launch_step(M, tz, engine, table, ws, tile0, st);
+  }
+}
+
+void migrate_batch(std::vector<ShotRun>& runs, cudaStream_t st) {
+  static_assert(sizeof(WorkSetB) < 30000, "kernel parameter block too large");
+  static_assert(sizeof(InjectBatch) < 30000, "kernel parameter block too large");
+  // one DevProp table for every propagator of the batch
+  std::vector<DevProp> table;
+  for (ShotRun& R : runs) {
+    R.fi = (int)table.size();
+    table.push_back(R.F->h);
+    R.bi = (int)table.size();
+    table.push_back(R.B->h);
+  }
+  DevBuf dtable(table.size() * sizeof(DevProp), st);
+  upload(dtable.p, table.data(), dtable.bytes, st);
+  const DevProp* dt = dtable.as<DevProp>();
+  std::vector<TickItem> items;
+  items.reserve(2 * runs.size());
+  while (true) {
+    items.clear();
+    std::vector<std::pair<ShotRun*, int>> restores, injections;
+    for (ShotRun& R : runs) {
+      switch (R.phase) {
+        case 0: {  // forward with checkpoints
+          TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.t_f, nullptr), false, {}};
+          it.w.prop = R.fi;
+          items.push_back(it);
+          break;
+        }
+        case 1: {  // replay of block rp_block overlapped with the backward over bk_block
+          const bool do_rp = R.rp_block >= 0 && R.bk_block <= R.rp_block + 1;
+          const bool do_bk = R.bk_block >= 0 && R.replayed_below <= R.bk_block;
+          if (do_rp) {
+            if (R.rp_t == R.s_of(R.rp_block)) restores.push_back({&R, R.rp_block});
+            Epilogue e = replay_epilogue(R, R.rp_block, R.rp_t);
+            TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.rp_t, R.fwd_unfused ? nullptr : &e),
+                        R.fwd_unfused, e};
+            it.w.prop = R.fi;
+            items.push_back(it);
+          }
+          if (do_bk) {
+            injections.push_back({&R, R.bk_t});
+            Epilogue e = backward_epilogue(R, R.bk_block, R.bk_t);
+            const bool unf = R.bwd_unfused && e.kind != EPI_NONE;
+            TickItem it{&R, false, make_work(*R.B, 0.0, nullptr, 0, unf ? nullptr : &e), unf, e};
+            it.w.prop = R.bi;
+            items.push_back(it);
+          }
+          break;
+        }
+        case 2: {  // excitation map: replay every block forward
+          if (R.rp_t == R.s_of(R.rp_block)) restores.push_back({&R, R.rp_block});
+          Epilogue e = replay_epilogue(R, R.rp_block, R.rp_t);
+          TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.rp_t, R.fwd_unfused ? nullptr : &e),
+                      R.fwd_unfused, e};
+          it.w.prop = R.fi;
+          items.push_back(it);
+          break;
+        }
+        case 3: {  // excitation backward over [0, nt_spec)
+          injections.push_back({&R, R.bk_t});
+          Epilogue e = backward_epilogue(R, 0, R.bk_t);
+          const bool unf = R.bwd_unfused && e.kind != EPI_NONE;
+          TickItem it{&R, false, make_work(*R.B, 0.0, nullptr, 0, unf ? nullptr : &e), unf, e};
+          it.w.prop = R.bi;
+          items.push_back(it);
+          break;
+        }
+        default:
+          break;
+      }
+    }
+    if (items.empty()) break;
+    for (auto& r : restores) restore_checkpoint(*r.first, r.second, st);
+    // time-reversed record injection of this tick's backward steps
+    for (size_t c0 = 0; c0 < injections.size(); c0 += MAX_BATCH_WORKS) {
+      InjectBatch ib{};
+      int cells = 0;
+      for (size_t k = c0; k < std::min(injections.size(), c0 + MAX_BATCH_WORKS); ++k) {
+        ShotRun& R = *injections[k].first;
+        if (!R.plan) continue;
+        InjectItem& I = ib.it[ib.n++];
+        I.plan = R.plan->dev();
+        I.prop = dt + R.bi;
+        I.record = R.rec.as<float>();
+        I.time_offset = (int64_t)injections[k].second * R.nrec;
+        I.cell0 = cells;
+        cells += R.plan->n_cells;
+      }
+      if (cells > 0) {
+        k_inject_batch<<<(cells + 127) / 128, 128, 0, st>>>(ib);
+        ++g_launches;
+      }
+    }
+    // stencil launches, grouped by (engine, order)
+    std::map<std::pair<int, int>, std::vector<TickItem*>> groups;
+    for (TickItem& it : items) {
+      const Prop& P = it.fwd ? *it.run->F : *it.run->B;
+      groups[{P.h.engine, P.M}].push_back(&it);
+    }
+    cudaEvent_t e0 = nullptr;
+    const bool timed = g_prof.begin(st, e0);
+    double bytes = 0.0;
+    for (auto& g : groups) launch_group(g.second, dt, st, bytes);
+    if (timed) g_prof.end(st, e0, bytes);
+    // after the stress phase: sources on vz, stabilisation, stand-alone epilogues, checkpoints
+    for (TickItem& it : items) {
+      ShotRun& R = *it.run;
+      Prop& P = it.fwd ? *R.F : *R.B;
+      after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t);
+      if (it.unfused) launch_epilogue(P, it.epi);
+      if (R.phase == 0 && R.t_f % R.iv == 0) save_checkpoint(R, R.t_f / R.iv, st);
+    }
+    CK(cudaGetLastError());
+    // advance the schedules
+    for (ShotRun& R : runs) {
+      switch (R.phase) {
+        case 0:
+          if (++R.t_f == R.nt) {
+            if (!R.excitation) {
+              R.phase = 1;
+              R.rp_block = R.bk_block = R.n_states - 1;
+              R.rp_t = R.s_of(R.rp_block);
+              R.bk_t = R.e_of(R.bk_block) - 1;
+              R.replayed_below = R.n_states;
+            } else {
+              R.phase = 2;
+              R.rp_block = 0;
+              R.rp_t = 0;
+            }
+          }
+          break;
+        case 1: {
+          const bool did_rp = R.rp_block >= 0 && R.bk_block <= R.rp_block + 1;
+          const bool did_bk = R.bk_block >= 0 && R.replayed_below <= R.bk_block;
+          if (did_bk) {
+            if (--R.bk_t < R.s_of(R.bk_block)) {
+              --R.bk_block;
+              if (R.bk_block >= 0) R.bk_t = R.e_of(R.bk_block) - 1;
+            }
+          }
+          if (did_rp) {
+            if (++R.rp_t == R.e_of(R.rp_block)) {
+              R.replayed_below = R.rp_block;
+              --R.rp_block;
+              if (R.rp_block >= 0) R.rp_t = R.s_of(R.rp_block);
+            }
+          }
+          if (R.bk_block < 0) R.phase = 4;
+          break;
+        }
+        case 2:
+          if (++R.rp_t == R.e_of(R.rp_block)) {
+            if (++R.rp_block == R.n_states) {
+              R.phase = 3;
+              R.bk_t = R.cfg.nt_spec - 1;
+            } else {
+              R.rp_t = R.s_of(R.rp_block);
+            }
+          }
+          break;
+        case 3:
+          if (--R.bk_t < 0) R.phase = 4;
+          break;
+        default:
+          break;
+      }
+    }
+  }
+  for (ShotRun& R : runs) finish_run(R, st);
 }
 
 // --------------------------------------------------------------------------
@@ -995,16 +1304,18 @@ int32_t ertm_profile_stencil(int32_t enable, int32_t every) {
     g_prof.every = every > 0 ? every : 1;
     g_prof.counter = 0;
     g_prof.total_ms = 0.0;
+    g_prof.total_bytes = 0.0;
     g_prof.samples = 0;
   });
 }
 
-int32_t ertm_profile_read(double* total_ms, int64_t* samples) {
+int32_t ertm_profile_read(double* total_ms, int64_t* samples, double* total_bytes) {
   return guarded([&] {
     REQUIRE(total_ms && samples, "null argument");
     g_prof.drain();
     *total_ms = g_prof.total_ms;
     *samples = g_prof.samples;
+    if (total_bytes) *total_bytes = g_prof.total_bytes;
   });
 }
 
@@ -1311,6 +1622,25 @@ int32_t ertm_migrate(void* fwd, void* back, const ertm_migrate_config* cfg, cons
     REQUIRE(fwd && back && cfg && wavelet, "bad arguments");
     REQUIRE(cfg->n_comp == 0 || record, "record missing");
     migrate(*static_cast<Prop*>(fwd), *static_cast<Prop*>(back), *cfg, wavelet, record, num, illum, rillum);
+  });
+}
+
+int32_t ertm_migrate_batch(int32_t n_shots, const ertm_batch_shot* shots) {
+  return guarded([&] {
+    REQUIRE(n_shots >= 1 && shots, "bad arguments");
+    cudaStream_t st = static_cast<Prop*>(shots[0].fwd)->st;
+    std::vector<ShotRun> runs(n_shots);
+    for (int k = 0; k < n_shots; ++k) {
+      const ertm_batch_shot& S = shots[k];
+      REQUIRE(S.fwd && S.back && S.wavelet, "shot " + std::to_string(k) + ": missing propagator or wavelet");
+      REQUIRE(S.cfg.n_comp == 0 || S.record, "shot " + std::to_string(k) + ": record missing");
+      for (int q = 0; q < k; ++q)
+        REQUIRE(shots[q].fwd != S.fwd && shots[q].back != S.back && shots[q].fwd != S.back && shots[q].back != S.fwd,
+                "every shot needs its own pair of propagators");
+      prepare_run(runs[k], *static_cast<Prop*>(S.fwd), *static_cast<Prop*>(S.back), S.cfg, S.wavelet, S.record,
+                  S.num, S.illum, S.rillum, st, 2);
+    }
+    migrate_batch(runs, st);
   });
 }
 

@@ -117,11 +117,30 @@ struct StepWork {
 };
 constexpr int STEP_PEAK = 1;        // visco: reduce max|p| into DevProp::peak
 
-struct WorkSet {
-  const StepWork* table;  // device table (batched); nullptr → single
-  int32_t n;
-  StepWork single;
+// The works of one launch, passed by value in the kernel parameters: one work
+// (plain stepping) or up to N (batched ticks; blocks find their work by binary
+// search over the tile offsets).
+struct WorkSet1 {
+  StepWork w;
+  __device__ __forceinline__ const StepWork& get(int) const { return w; }
 };
+
+template <int N>
+struct WorkSetN {
+  int32_t n;
+  int32_t pad_;
+  StepWork w[N];
+  __device__ __forceinline__ const StepWork& get(int block) const {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (w[mid].tile0 <= block) lo = mid; else hi = mid - 1;
+    }
+    return w[lo];
+  }
+};
+constexpr int MAX_BATCH_WORKS = 32;
+using WorkSetB = WorkSetN<MAX_BATCH_WORKS>;
 
 // ---------------------------------------------------------------------------
 // exact-order float helpers
@@ -187,14 +206,5 @@ __device__ __forceinline__ int strip_z(const DevProp& P, int i) {
   return -1;
 }
 
-__device__ __forceinline__ const StepWork& find_work(const WorkSet& ws, int block) {
-  if (ws.table == nullptr) return ws.single;
-  int lo = 0, hi = ws.n - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (ws.table[mid].tile0 <= block) lo = mid; else hi = mid - 1;
-  }
-  return ws.table[lo];
-}
 
 }  // namespace ertm

@@ -277,13 +277,13 @@ __device__ __forceinline__ ColInfo col_info(const Geo& G, int j, const float* ax
 // velocity phase
 // ---------------------------------------------------------------------------
 // Acoustic and viscoacoustic: vx += (dt·irx)·(D⁺ₓp + ψ), vz += (dt·irz)·(D⁺_z p + ψ).
-template <int M, int BZ, int R>
+template <int M, int BZ, int R, class WS>
 __global__ void __launch_bounds__(XT* BZ)
-k_pressure_velocity(const DevProp* __restrict__ props, WorkSet ws) {
+k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
   __shared__ __align__(16) float sp[T::N];
-  const StepWork& w = find_work(ws, blockIdx.x);
+  const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
@@ -354,15 +354,15 @@ k_pressure_velocity(const DevProp* __restrict__ props, WorkSet ws) {
 }
 
 // Elastic: vx += (dt·irx)·(D⁺ₓσxx + D⁻_zσxz), vz += (dt·irz)·(D⁻ₓσxz + D⁺_zσzz).
-template <int M, int BZ, int R>
+template <int M, int BZ, int R, class WS>
 __global__ void __launch_bounds__(XT* BZ)
-k_elastic_velocity(const DevProp* __restrict__ props, WorkSet ws) {
+k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
   __shared__ __align__(16) float sxx_s[T::N];
   __shared__ __align__(16) float szz_s[T::N];
   __shared__ __align__(16) float sxz_s[T::N];
-  const StepWork& w = find_work(ws, blockIdx.x);
+  const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
@@ -480,14 +480,14 @@ __device__ __forceinline__ void block_max_to(float v, float* dst) {
 
 // Acoustic (VISCO=false): p += (dt·κ)·div.  Viscoacoustic (VISCO=true):
 // ε += dt·div; r_l ← r_l·a_l + b_l·Δε; p = K_R·ε + Σ r_l.
-template <int M, int BZ, int R, bool VISCO>
+template <int M, int BZ, int R, bool VISCO, class WS>
 __global__ void __launch_bounds__(XT* BZ)
-k_pressure_stress(const DevProp* __restrict__ props, WorkSet ws) {
+k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
   __shared__ __align__(16) float svx[T::N];
   __shared__ __align__(16) float svz[T::N];
-  const StepWork& w = find_work(ws, blockIdx.x);
+  const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);
@@ -607,14 +607,14 @@ k_pressure_stress(const DevProp* __restrict__ props, WorkSet ws) {
 //   σxz += (dt·μxz)·(D⁺_z vx + D⁺ₓ vz); source; free surface σzz = σxz = 0;
 // then the epilogue with P/S from the stresses (stress separation) or from
 // the raw velocity divergence/curl (divcurl, propagation.py:953-976).
-template <int M, int BZ, int R>
+template <int M, int BZ, int R, class WS>
 __global__ void __launch_bounds__(XT* BZ)
-k_elastic_stress(const DevProp* __restrict__ props, WorkSet ws) {
+k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
   __shared__ __align__(16) float svx[T::N];
   __shared__ __align__(16) float svz[T::N];
-  const StepWork& w = find_work(ws, blockIdx.x);
+  const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
   const TileLoc L = tile_of(w, blockIdx.x, TZ);

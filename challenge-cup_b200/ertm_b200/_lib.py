@@ -56,6 +56,13 @@ class MigrateConfig(C.Structure):
     ]
 
 
+class BatchShot(C.Structure):
+    _fields_ = [
+        ("fwd", C.c_void_p), ("back", C.c_void_p), ("cfg", MigrateConfig), ("wavelet", C.c_void_p),
+        ("record", C.c_void_p), ("num", C.c_void_p), ("illum", C.c_void_p), ("rillum", C.c_void_p),
+    ]
+
+
 _P = C.c_void_p
 _I32 = C.c_int32
 _SIGNATURES = {
@@ -65,7 +72,7 @@ _SIGNATURES = {
     "ertm_launch_count": (C.c_int64, []),
     "ertm_set_tile_rows": (_I32, [_I32]),
     "ertm_profile_stencil": (_I32, [_I32, _I32]),
-    "ertm_profile_read": (_I32, [C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "ertm_profile_read": (_I32, [C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "ertm_prop_create": (_P, [C.POINTER(PropConfig)] + [_P] * 12 + [_P]),
     "ertm_prop_destroy": (None, [_P]),
     "ertm_prop_info_get": (_I32, [_P, C.POINTER(PropInfo)]),
@@ -85,6 +92,7 @@ _SIGNATURES = {
     "ertm_prop_load_state": (_I32, [_P, _P]),
     "ertm_forward": (_I32, [_P, _I32, _P, _I32, _P, _P]),
     "ertm_migrate": (_I32, [_P, _P, C.POINTER(MigrateConfig), _P, _P, _P, _P, _P]),
+    "ertm_migrate_batch": (_I32, [_I32, C.POINTER(BatchShot)]),
     "ertm_postprocess": (_I32, [_I32, _I32, C.c_double, C.c_double, _P, _P, _P, _I32, _I32, C.c_double,
                                 _I32, C.c_double, _I32, _I32, _P, _P]),
     "ertm_stack": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),

@@ -1,0 +1,188 @@
+"""Batched migration (form b): many shots per device call.
+
+``BatchMigrator.migrate_shots`` runs a list of shots — possibly on different
+models, grids, engines and lengths — through ``ertm_migrate_batch``: all
+shots advance together in ticks that share one velocity and one stress
+launch per (engine, order) group, and inside each shot the replay of block
+b−1 overlaps the backward pass over block b.  Every propagator performs the
+same steps in the same order as the plain one-shot path, so each image equals
+the plain path's image bit for bit.
+
+Shots are grouped so that a group's device memory (two propagators, the
+checkpoints, two replay buffers and the accumulators per shot) stays within a
+budget; groups run one after another.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Any, Sequence
+
+import numpy as np
+
+from . import _lib
+from .exceptions import ImagingError
+from .imaging import RTMImager, ShotMigrator, postprocess_image
+from .types import ImageResult
+
+
+@dataclass
+class _Prepared:
+    mig: ShotMigrator
+    shot: Any
+    pairs: list
+    store: Any
+    start_step: int
+    cfg: _lib.MigrateConfig
+    record: np.ndarray
+    wavelet: np.ndarray
+    modes: tuple[str, ...]
+    acc: Any = None
+
+
+def shot_device_bytes(mig: ShotMigrator, n_steps: int, n_images: int, n_buffers: int = 2) -> int:
+    """Device memory one shot of a batch holds while it runs."""
+    info = mig.prop.info()
+    state = int(info.state_bytes)
+    g = mig.model.grid
+    npix = g.nx * g.nz
+    coef = 12 * info.nzp * info.ld * 4          # upper bound on the coefficient block
+    interval = max(1, mig.interval_for(n_steps))
+    n_states = (n_steps + interval - 1) // interval
+    replay = n_buffers * interval * 2 * npix * 4
+    acc = (2 * n_images + 2) * npix * 8
+    return 2 * (state + coef) + n_states * state + replay + acc
+
+
+class BatchMigrator:
+    """Migrate many shots per device call with the same imaging settings."""
+
+    def __init__(self, imager: RTMImager, *, memory_budget: int | None = None) -> None:
+        self.imager = imager
+        self.memory_budget = memory_budget
+
+    def _budget(self) -> int:
+        if self.memory_budget is not None:
+            return int(self.memory_budget)
+        import torch
+        free, _ = torch.cuda.mem_get_info()
+        return int(0.8 * free)
+
+    def migrate_shots(self, shots: Sequence[Any], models: Any, *, modes: tuple[str, ...] | None = None,
+                      wavelets: Sequence[np.ndarray] | None = None) -> list[list[ImageResult]]:
+        """Returns, per shot, one ImageResult per mode."""
+        modes = tuple(modes or (self.imager.config.mode,))
+        model_list = list(models) if isinstance(models, (list, tuple)) else [models] * len(shots)
+        if len(model_list) != len(shots):
+            raise ImagingError("one model per shot (or one model for all)")
+        results: list[list[ImageResult] | None] = [None] * len(shots)
+        group: list[tuple[int, _Prepared]] = []
+        used = 0
+        budget = self._budget()
+        for k, (shot, model) in enumerate(zip(shots, model_list)):
+            try:
+                shot.validate()
+                model.validate()
+            except ValueError as exc:
+                raise ImagingError(f"invalid imaging input: {exc}") from exc
+            mig = ShotMigrator(self.imager, model)
+            w = None if wavelets is None else wavelets[k]
+            need = shot_device_bytes(mig, mig.spec.nt if w is None else len(w), len(modes))
+            if group and used + need > budget:
+                self._run(group, results)
+                group, used = [], 0
+            group.append((k, self._prepare(mig, shot, modes, w)))
+            used += need
+        if group:
+            self._run(group, results)
+        return [r for r in results]  # type: ignore[misc]
+
+    def _prepare(self, mig: ShotMigrator, shot: Any, modes, wavelet) -> _Prepared:
+        im = self.imager
+        record = im._prepare_record(shot, mig.spec, None)
+        if not record:
+            raise ImagingError("empty shot record; nothing to back-propagate")
+        w = im._prepare_wavelet(shot, mig.spec, wavelet)
+        pairs, store, start = mig._prepare(shot.source, shot.receivers, modes, len(w))
+        names = list(record)
+        cfg = mig._config(pairs, names, store, start, len(w))
+        rec = np.ascontiguousarray(np.stack([np.asarray(record[n], dtype=np.float32) for n in names]))
+        return _Prepared(mig, shot, pairs, store, start, cfg, rec, w, modes)
+
+    def _run(self, group: list[tuple[int, _Prepared]], results: list) -> None:
+        import torch
+
+        shots = (_lib.BatchShot * len(group))()
+        keep = []
+        for i, (_, p) in enumerate(group):
+            g = p.mig.model.grid
+            p.acc = torch.zeros((3, len(p.pairs), g.nz, g.nx), dtype=torch.float64, device="cuda")
+            rec = torch.from_numpy(p.record).cuda()
+            keep.append(rec)
+            s = shots[i]
+            s.fwd = p.mig.prop.handle
+            s.back = p.mig.back.handle
+            s.cfg = p.cfg
+            s.wavelet = _lib.ptr(p.wavelet)
+            s.record = _lib.ptr(rec)
+            s.num = _lib.ptr(p.acc[0])
+            s.illum = _lib.ptr(p.acc[1])
+            s.rillum = _lib.ptr(p.acc[2])
+        _lib.check(_lib.lib().ertm_migrate_batch(len(group), shots), "migrate_batch")
+        for k, p in group:
+            p.mig.prop._psi_allocated = p.mig.back._psi_allocated = True
+            im = self.imager
+            cond = str(im.config.condition).lower()
+            out = []
+            acc = p.acc.cpu().numpy()
+            for j, m in enumerate(p.modes):
+                image = postprocess_image(acc[0, j], acc[1, j], acc[2, j], **p.mig._post_args())
+                res = ImageResult(image=image, grid=p.mig.model.grid, mode=m,
+                                  meta=im._meta(p.mig.spec, p.mig.engine, p.shot, p.store, cond, p.start_step,
+                                                p.mig.prop, p.mig.back, m))
+                res.meta["batched"] = True
+                res.validate()
+                out.append(res)
+            results[k] = out
+
+
+def migrate_device_batch(imager: RTMImager, migrators: Sequence[ShotMigrator], sources: Sequence[Any],
+                         receivers: Sequence[Any], records: Sequence[Any], names: Sequence[str],
+                         wavelets: Sequence[np.ndarray], *, modes: tuple[str, ...] = ("pp",)):
+    """Device-resident batched form: one migrator (propagator pair) per shot,
+    built beforehand and reused; ``records[k]`` is a contiguous device tensor
+    (n_comp, nt, nrec) aligned to the propagation dt.  Returns a list of
+    device tensors (n_modes, nz, nx) float32 of final images."""
+    import torch
+
+    n = len(migrators)
+    shots = (_lib.BatchShot * n)()
+    accs = []
+    for k, mig in enumerate(migrators):
+        w = np.ascontiguousarray(wavelets[k], dtype=np.float32)
+        pairs, store, start = mig._prepare(sources[k], receivers[k], modes, len(w))
+        cfg = mig._config(pairs, list(names), store, start, len(w))
+        g = mig.model.grid
+        acc = torch.empty((3, len(pairs), g.nz, g.nx), dtype=torch.float64, device=records[k].device)
+        accs.append((acc, w))
+        s = shots[k]
+        s.fwd, s.back, s.cfg = mig.prop.handle, mig.back.handle, cfg
+        s.wavelet = _lib.ptr(w)
+        s.record = _lib.ptr(records[k])
+        s.num, s.illum, s.rillum = _lib.ptr(acc[0]), _lib.ptr(acc[1]), _lib.ptr(acc[2])
+    _lib.check(_lib.lib().ertm_migrate_batch(n, shots), "migrate_batch")
+    out = []
+    for k, mig in enumerate(migrators):
+        mig.prop._psi_allocated = mig.back._psi_allocated = True
+        acc = accs[k][0]
+        g = mig.model.grid
+        imgs = torch.empty((len(modes), g.nz, g.nx), dtype=torch.float32, device=acc.device)
+        a = mig._post_args()
+        for j in range(len(modes)):
+            _lib.check(_lib.lib().ertm_postprocess(
+                g.nz, g.nx, float(a["dx"]), float(a["dz"]), _lib.ptr(acc[0, j]), _lib.ptr(acc[1, j]),
+                _lib.ptr(acc[2, j]), int(a["by_illum"]), int(a["by_rillum"]), a["eps"], int(a["laplacian"]),
+                a["lowpass_fraction"], int(a["npml"]), int(a["boundary"] == "cpml"), _lib.ptr(imgs[j]), None),
+                "postprocess")
+        out.append(imgs)
+    return out

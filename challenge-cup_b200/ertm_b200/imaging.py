@@ -290,6 +290,11 @@ class ShotMigrator:
         self._receivers_key: tuple | None = None
         self._used = False
 
+    def interval_for(self, n_steps: int) -> int:
+        """Checkpoint interval of a fresh run (state bytes before the first step)."""
+        return checkpoint_interval(n_steps, max(int(self.prop.info().field_bytes), 1),
+                                   float(self.imager.config.checkpoint_mb))
+
     def _prepare(self, source: Any, receivers: Any, modes: tuple[str, ...], n_steps: int):
         im = self.imager
         pairs = [im._resolve_mode(m) for m in modes]

@@ -112,15 +112,16 @@ int32_t ertm_version(void);
 /* Select the device and check it is sm_100 (no reference counterpart). */
 int32_t ertm_init(int32_t device);
 /* Instrumentation (no reference counterpart): kernels launched so far, and
- * CUDA-event timing of the stencil phases of every `every`-th step on the
- * stream they run on; ertm_profile_read returns the summed milliseconds and
- * the number of timed steps since the last ertm_profile_stencil call. */
+ * CUDA-event timing of the stencil launches of every `every`-th step (or
+ * batched tick) on the stream they run on; ertm_profile_read returns the
+ * summed milliseconds, the number of timed samples and the algorithmic HBM
+ * bytes of the timed launches since the last ertm_profile_stencil call. */
 int64_t ertm_launch_count(void);
 /* Pin the stencil tile height (8, 16 or 32 rows; 0 = automatic) for
  * propagators created afterwards — the autotuner's knob (order 8 only). */
 int32_t ertm_set_tile_rows(int32_t rows);
 int32_t ertm_profile_stencil(int32_t enable, int32_t every);
-int32_t ertm_profile_read(double* total_ms, int64_t* samples);
+int32_t ertm_profile_read(double* total_ms, int64_t* samples, double* total_bytes);
 
 /* propagators ------------------------------------------------------------ */
 /* Replaces AcousticPropagator/ViscoacousticPropagator/ElasticPropagator
@@ -174,6 +175,24 @@ int32_t ertm_forward(void* prop, int32_t nt, const float* amps, int32_t n_comp, 
  * accumulators are n_images × (nz, nx) float64 (num, illum, rillum). */
 int32_t ertm_migrate(void* fwd, void* back, const ertm_migrate_config* cfg, const float* wavelet,
                      const float* record, double* num, double* illum, double* rillum);
+/* One shot of a batched migration. */
+typedef struct ertm_batch_shot {
+  void* fwd;                 /* forward/replay propagator of this shot */
+  void* back;                /* backward propagator of this shot */
+  ertm_migrate_config cfg;
+  const float* wavelet;      /* cfg.nt samples */
+  const float* record;       /* cfg.n_comp × cfg.nt_spec × nrec */
+  double* num;               /* outputs as in ertm_migrate */
+  double* illum;
+  double* rillum;
+} ertm_batch_shot;
+
+/* Batched form of ertm_migrate (the pipeline's shot loop, pipeline.py:277-283):
+ * all shots advance together in ticks that share one velocity and one stress
+ * launch per (engine, order) group; within a shot the replay of block b−1
+ * overlaps the backward pass over block b.  Shots may differ in grid, engine,
+ * length and condition.  Results equal n_shots separate ertm_migrate calls. */
+int32_t ertm_migrate_batch(int32_t n_shots, const ertm_batch_shot* shots);
 /* Normalisation and _postprocess (imaging.py:326-333, 476-502): image =
  * num/(illum+eps)/(rillum+eps) as selected, Laplacian, wavenumber low-pass
  * (lowpass < 1), PML mask of width npml (top too when top_mask). */
