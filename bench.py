@@ -420,7 +420,9 @@ def run_ours(args, dist: Dist) -> None:
         "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": committed_traffic(f"{wl.engine}_step"),
-                     "kernel": f"{wl.engine} velocity + stress launches of a batched tick",
+                     "kernel": f"{wl.engine} velocity + stress launches of a batched tick (imaging epilogue fused)",
+                     "bytes_definition": "per propagator step: Npad*(8*n_state + 4*n_coef) + 8*CPML strip cells*terms;"
+                                         " per fused imaging epilogue: 16 B per accumulator, 4 B per replayed field",
                      "bytes_per_tick": float(byt.value) / max(int(cnt.value), 1), "tick_us": step_ms * 1e3,
                      "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,

@@ -80,15 +80,16 @@ __global__ void k_setup_materials(DevProp* props, int pi, SetupArgs A) {
 }
 
 // Exhaustive check of divh() against __fdiv_rn for a fixed divisor h: all
-// 2^32 float inputs; mismatches are counted (NaNs compare equal to NaNs).
-__global__ void k_verify_division(float h, double r, unsigned long long* mismatches) {
+// 2^32 float inputs; value mismatches are counted (+0 == −0, NaN == NaN).
+__global__ void k_verify_division(float h, double r64, float r32, float rl, int mode,
+                                  unsigned long long* mismatches) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   unsigned long long bad = 0;
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < (1ull << 32); k += stride) {
     const float a = __uint_as_float((uint32_t)k);
-    const float q = divh(a, h, r, 1);
+    const float q = divh(a, h, r64, r32, rl, mode);
     const float ref = __fdiv_rn(a, h);
-    const bool same = (__float_as_uint(q) == __float_as_uint(ref)) || (q != q && ref != ref);
+    const bool same = (q == ref) || (q != q && ref != ref);
     bad += same ? 0ull : 1ull;
   }
   if (bad) atomicAdd(mismatches, bad);

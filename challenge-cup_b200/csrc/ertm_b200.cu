@@ -468,30 +468,53 @@ void launch_step(int M, int tz, int engine, const DevProp* d, const WS& ws, int 
   g_launches += 2;
 }
 
-// Fast exact division by a grid spacing: verified once per float value of h
-// over all 2^32 inputs (k_verify_division), then cached for the process.
-std::map<uint32_t, bool> g_div_ok;
+// Division mode for a grid spacing h (see divh): the cheapest form that the
+// device reproduces __fdiv_rn(a, h) with for all 2^32 inputs, checked once per
+// float value of h and cached for the process.
+std::map<uint32_t, int> g_div_mode;
 std::mutex g_div_mutex;
 
-bool division_verified(float h, double r, cudaStream_t st) {
-  uint32_t key;
-  std::memcpy(&key, &h, 4);
-  {
-    std::lock_guard<std::mutex> lock(g_div_mutex);
-    auto it = g_div_ok.find(key);
-    if (it != g_div_ok.end()) return it->second;
-  }
+// Reciprocal pieces of a spacing: RN64(1/h), RN32(1/h) and RN32(1/h − RN32(1/h))
+// (the last from the float64 difference, accurate to far below one ulp of it).
+void reciprocals(float h, double& r64, float& r32, float& rl) {
+  r64 = 1.0 / (double)h;               // IEEE double division on the host
+  r32 = 1.0f / h;                      // IEEE single division on the host
+  rl = (float)(r64 - (double)r32);
+}
+
+unsigned long long division_mismatches(float h, int mode, cudaStream_t st) {
+  double r64;
+  float r32, rl;
+  reciprocals(h, r64, r32, rl);
   DevBuf bad(8, st);
   CK(cudaMemsetAsync(bad.p, 0, 8, st));
-  k_verify_division<<<148 * 8, 256, 0, st>>>(h, r, bad.as<unsigned long long>());
+  k_verify_division<<<148 * 8, 256, 0, st>>>(h, r64, r32, rl, mode, bad.as<unsigned long long>());
   ++g_launches;
   CK(cudaGetLastError());
   unsigned long long n = 1;
   CK(cudaMemcpyAsync(&n, bad.p, 8, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  return n;
+}
+
+int division_mode(float h, cudaStream_t st) {
+  uint32_t key;
+  std::memcpy(&key, &h, 4);
+  {
+    std::lock_guard<std::mutex> lock(g_div_mutex);
+    auto it = g_div_mode.find(key);
+    if (it != g_div_mode.end()) return it->second;
+  }
+  int mode = 0;
+  for (int m : {1, 3, 2}) {
+    if (division_mismatches(h, m, st) == 0) {
+      mode = m;
+      break;
+    }
+  }
   std::lock_guard<std::mutex> lock(g_div_mutex);
-  g_div_ok[key] = (n == 0);
-  return n == 0;
+  g_div_mode[key] = mode;
+  return mode;
 }
 
 // Tile height for a launch: the tallest tile that still gives ≥ 4 blocks per
@@ -543,6 +566,35 @@ double step_bytes(const Prop& P) {
   const int n_coef = P.h.engine == ENGINE_ACOUSTIC ? 3 : (P.h.engine == ENGINE_ELASTIC ? 5 : 3 + 2 * P.h.L);
   const double strips = (double)P.n_psi * ((double)P.h.wx * P.h.nzp + (double)P.h.hz_rows * P.h.nxp);
   return npad * (8.0 * n_state + 4.0 * n_coef) + 8.0 * strips;
+}
+
+// Algorithmic bytes of a fused epilogue over the physical cells (SURVEY §8d:
+// each imaging accumulator is read and written once per step, 16 B; the
+// replayed source field is written once and read once, 4 B each).
+double epilogue_bytes(const Epilogue& e, size_t npix) {
+  double per = 0.0;
+  switch (e.kind) {
+    case EPI_STORE:
+      per = 4.0 * ((e.out[0] ? 1 : 0) + (e.out[1] ? 1 : 0));
+      break;
+    case EPI_IMAGE:
+      for (int k = 0; k < e.n_images; ++k) {
+        if (e.cross) per += 16.0;
+        if (e.illum && e.ill[k]) per += 16.0;
+        if (e.rillum && e.ril[k]) per += 16.0;
+      }
+      per += 4.0 * ((e.src[0] ? 1 : 0) + (e.src[1] ? 1 : 0));
+      break;
+    case EPI_EXC_TRACK:
+      per = 8.0;   // running |P| read and (when larger) written
+      break;
+    case EPI_EXC_IMAGE:
+      per = 4.0;   // peak-step read; the few matching cells add 24 B each
+      break;
+    default:
+      break;
+  }
+  return per * (double)npix;
 }
 
 // The StepWork of one step.  Amplitude: wavelet[t] from device memory when
@@ -604,7 +656,7 @@ void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, co
   cudaEvent_t e0 = nullptr;
   const bool timed = g_prof.begin(P.st, e0);
   launch_step(P.M, P.tz, P.h.engine, P.dp(), ws, P.tiles, P.st);
-  if (timed) g_prof.end(P.st, e0, step_bytes(P));
+  if (timed) g_prof.end(P.st, e0, step_bytes(P) + (epi ? epilogue_bytes(*epi, (size_t)P.h.nz * P.h.nx) : 0.0));
   after_step(P, amp64, wave, t);
 }
 
@@ -649,10 +701,15 @@ Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, cons
   h.hx = (float)cfg->dx;
   h.hz = (float)cfg->dz;
   h.dt = (float)cfg->dt;
-  h.rx = 1.0 / (double)h.hx;   // IEEE double division on the host: RN64(1/hx)
+  h.rx = 1.0 / (double)h.hx;
   h.rz = 1.0 / (double)h.hz;
-  h.fast_x = division_verified(h.hx, h.rx, P->st) ? 1 : 0;
-  h.fast_z = division_verified(h.hz, h.rz, P->st) ? 1 : 0;
+  {
+    double d;
+    reciprocals(h.hx, d, h.rx32, h.rxl);
+    reciprocals(h.hz, d, h.rz32, h.rzl);
+  }
+  h.fast_x = division_mode(h.hx, P->st);
+  h.fast_z = division_mode(h.hz, P->st);
   h.npx_l = cfg->npml_x_left;
   h.npx_r = cfg->npml_x_right;
   h.npz_t = cfg->npml_z_top;
@@ -1056,7 +1113,7 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
       w.tiles = tiles_for(P.h, tz);
       tile0 += w.tiles;
       ws.w[k - c0] = w;
-      bytes += step_bytes(P);
+      bytes += step_bytes(P) + epilogue_bytes(w.epi, (size_t)P.h.nz * P.h.nx);
     }
     launch_step(M, tz, engine, table, ws, tile0, st);
   }
@@ -1289,6 +1346,13 @@ const char* ertm_last_error(void) { return g_error.c_str(); }
 int32_t ertm_version(void) { return 1; }
 
 int64_t ertm_launch_count(void) { return g_launches.load(); }
+
+int32_t ertm_division_check(float h, int32_t mode, uint64_t* mismatches) {
+  return guarded([&] {
+    REQUIRE(mismatches && mode >= 0 && mode <= 3 && h > 0.f, "bad arguments");
+    *mismatches = division_mismatches(h, mode, 0);
+  });
+}
 
 int32_t ertm_set_tile_rows(int32_t rows) {
   return guarded([&] {

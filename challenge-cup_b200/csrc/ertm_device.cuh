@@ -51,8 +51,10 @@ struct DevProp {
   int32_t n_fields;
   float c[4];           // float32 stencil coefficients (unused ones = 0)
   float hx, hz, dt;     // float32 spacing and time step
-  double rx, rz;        // RN64(1/hx), RN64(1/hz) for the verified fast division
-  int32_t fast_x, fast_z;  // 1: divh() by hx / hz was verified equal to __fdiv_rn for all inputs
+  double rx, rz;        // RN64(1/hx), RN64(1/hz)
+  float rx32, rz32;     // RN32(1/hx), RN32(1/hz)
+  float rxl, rzl;       // RN32(1/h − RN32(1/h)) for the one-FMA form
+  int32_t fast_x, fast_z;  // division mode by hx / hz (see divh)
   int32_t npx_l, npx_r; // x-strip widths (0 when absent)
   int32_t npz_t, npz_b; // z-strip widths (top is 0 under a free surface)
   int32_t wx;           // npx_l + npx_r
@@ -175,14 +177,27 @@ __device__ __forceinline__ float dminus(const float* s, int stride, const float*
   return fdiv(acc, h);
 }
 
-// a / h rounded to nearest.  Fast form: float32(RN64(double(a) · R)) with
-// R = RN64(1/h): the float64 product is within 2^-52 relative of a/h, so the
-// single rounding to float32 matches RN32(a/h) unless a/h lies that close to
-// a float32 rounding midpoint.  Whether that ever happens for a given h is
-// decided by the host, which compares this form with __fdiv_rn(a, h) for all
-// 2^32 float inputs a (k_verify_division) and only then sets `fast`.
-__device__ __forceinline__ float divh(float a, float h, double r64, int fast) {
-  if (fast) return __double2float_rn(__dmul_rn((double)a, r64));
+// a / h rounded to nearest, in one of four forms; the host picks the first
+// of forms 1, 3, 2 whose value equals __fdiv_rn(a, h) for all 2^32 float
+// inputs a (+0 and −0 count as equal, NaN as equal to NaN; k_verify_division)
+// and otherwise keeps form 0.
+//   3: RN(a·z_h + RN(a·z_l)) with one FMA, z_h = RN32(1/h), z_l = RN32(1/h − z_h)
+//      — division by a constant known in advance, Brisebarre, Muller & Raina,
+//      "Accelerating correctly rounded floating-point division when the
+//      divisor is known in advance", IEEE Trans. Computers 53(8), 2004;
+//   2: q = RN(a·r), e = a − q·h (exact FMA residual), RN(q + e·r), r = RN32(1/h)
+//      — the one-step correction of Markstein, IBM J. Res. Dev. 34(1), 1990;
+//   1: float32(RN64(double(a)·R)) with R = RN64(1/h);
+//   0: __fdiv_rn(a, h).
+__device__ __forceinline__ float div_bmr(float a, float zh, float zl) { return __fmaf_rn(a, zh, __fmul_rn(a, zl)); }
+__device__ __forceinline__ float div_fma(float a, float h, float r) {
+  const float q = __fmul_rn(a, r);
+  return __fmaf_rn(__fmaf_rn(-q, h, a), r, q);
+}
+__device__ __forceinline__ float divh(float a, float h, double r64, float r32, float rl, int mode) {
+  if (mode == 3) return div_bmr(a, r32, rl);
+  if (mode == 2) return div_fma(a, h, r32);
+  if (mode == 1) return __double2float_rn(__dmul_rn((double)a, r64));
   return __fdiv_rn(a, h);
 }
 

@@ -68,6 +68,24 @@ __device__ __forceinline__ void stage(float* s, const float* __restrict__ g, int
   }
 }
 
+// Issue the asynchronous copy of one per-cell operand tile (no halo): rows
+// [i0, i0+TZ) × columns [j0, j0+32) into a TZ × 32 shared array; rows past
+// the grid are zero-filled (j0 + 32 ≤ ld always holds).
+template <int TZ, int NT>
+__device__ __forceinline__ void stage_cells(float* s, const float* __restrict__ g, int nzp, int ld, int i0, int j0) {
+  constexpr int CH = TZ * 8;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (CH + NT - 1) / NT; ++it) {
+    const int idx = tid + it * NT;
+    if (CH % NT != 0 && idx >= CH) break;
+    const int r = idx >> 3, ch = idx & 7;
+    const int gi = i0 + r;
+    const bool ok = gi < nzp;
+    cp_async16(s + r * 32 + 4 * ch, ok ? g + (size_t)gi * ld + j0 + 4 * ch : g, ok);
+  }
+}
+
 struct TileLoc {
   int i0, j0;
 };
@@ -166,15 +184,29 @@ __device__ __forceinline__ void run_epilogue(const Epilogue& E, size_t c, size_t
 struct Geo {
   int nzp, nxp, ld, wx, npx_l, npx_r, npz_t, npz_b, pad, nz, nx, src_iz, src_ix, free_surface, fast_x, fast_z;
   float c[4];
-  float dt, hx, hz;
+  float dt, hx, hz, rx32, rz32, rxl, rzl;
   double rx, rz;
   __device__ __forceinline__ explicit Geo(const DevProp& P)
       : nzp(P.nzp), nxp(P.nxp), ld(P.ld), wx(P.wx), npx_l(P.npx_l), npx_r(P.npx_r), npz_t(P.npz_t),
         npz_b(P.npz_b), pad(P.pad), nz(P.nz), nx(P.nx), src_iz(P.src_iz), src_ix(P.src_ix),
         free_surface(P.free_surface), fast_x(P.fast_x), fast_z(P.fast_z), c{P.c[0], P.c[1], P.c[2], P.c[3]},
-        dt(P.dt), hx(P.hx), hz(P.hz), rx(P.rx), rz(P.rz) {}
-  __device__ __forceinline__ float dx_(float a) const { return divh(a, hx, rx, fast_x); }
-  __device__ __forceinline__ float dz_(float a) const { return divh(a, hz, rz, fast_z); }
+        dt(P.dt), hx(P.hx), hz(P.hz), rx32(P.rx32), rz32(P.rz32), rxl(P.rxl), rzl(P.rzl), rx(P.rx), rz(P.rz) {}
+  __device__ __forceinline__ float dx_(float a) const { return divh(a, hx, rx, rx32, rxl, fast_x); }
+  __device__ __forceinline__ float dz_(float a) const { return divh(a, hz, rz, rz32, rzl, fast_z); }
+  // Straight-line interior form (only used when the float64-product form was verified).
+  __device__ __forceinline__ float dxf(float a) const { return __double2float_rn(__dmul_rn((double)a, rx)); }
+  __device__ __forceinline__ float dzf(float a) const { return __double2float_rn(__dmul_rn((double)a, rz)); }
+  // A tile whose cells are all physical, away from every CPML strip, the
+  // free-surface row and the source node, with the FMA division verified:
+  // its stencils run without per-cell branches.
+  __device__ __forceinline__ bool interior(int i0, int j0, int tz) const {
+    const int i1 = i0 + tz, j1 = j0 + 32;
+    const bool phys = i0 >= pad && i1 <= pad + nz && j0 >= pad && j1 <= pad + nx;
+    const bool strips = i0 >= npz_t && i1 <= nzp - npz_b && j0 >= npx_l && j1 <= nxp - npx_r;
+    const bool fs = !free_surface || i0 > pad;
+    const bool src = !(src_iz >= i0 && src_iz < i1 && src_ix >= j0 && src_ix < j1);
+    return phys && strips && fs && src && fast_x == 1 && fast_z == 1;
+  }
   __device__ __forceinline__ int sx(int j) const {
     if (j < npx_l) return j;
     if (j >= nxp - npx_r) return npx_l + (j - (nxp - npx_r));
@@ -296,21 +328,41 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   const float* const azp = P.az; const float* const bzp = P.bz;
   if ((w.flags & STEP_PEAK) && blockIdx.x == w.tile0 && threadIdx.x == 0 && threadIdx.y == 0)
     *P.peak = 0.f;  // the stress phase of this step reduces into it
+  __shared__ __align__(16) float c_vx[TZ * 32], c_vz[TZ * 32], c_irx[TZ * 32], c_irz[TZ * 32];
   stage<M, TZ, XT * BZ>(sp, P.f[A_P], G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_vx, vx, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_vz, vz, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_irx, irx, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_irz, irz, G.nzp, G.ld, L.i0, L.j0);
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
-  float4 r_vx[R], r_vz[R], r_irx[R], r_irz[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int i = L.i0 + threadIdx.y + BZ * r;
-    if (i < G.nzp && j < G.nxp) {
-      const size_t g = (size_t)i * G.ld + j;
-      r_vx[r] = ld4(vx + g); r_vz[r] = ld4(vz + g); r_irx[r] = ldg4(irx + g); r_irz[r] = ldg4(irz + g);
-    }
-  }
+#define CELL(arr, rr) ld4(arr + (rr) * 32 + 4 * threadIdx.x)
   cp_async_wait_all();
   __syncthreads();
   if (j >= G.nxp) return;
+  if (G.interior(L.i0, L.j0, TZ)) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int rr = threadIdx.y + BZ * r;
+      const float* row = sp + (rr + M) * T::W + 4 * threadIdx.x;
+      const size_t g = (size_t)(L.i0 + rr) * G.ld + j;
+      float v[12];
+      row12(row, v);
+      float z[4][2 * M + 1];
+      col9<M>(row + 4, z);
+      float4 ox, oz;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float dx = G.dxf(sum_plus<M>(v, 4 + c, G.c));
+        const float dz = G.dzf(sum_plus<M>(z[c], M, G.c));
+        set_comp(ox, c, fadd(comp(CELL(c_vx, rr), c), fmul(fmul(G.dt, comp(CELL(c_irx, rr), c)), dx)));
+        set_comp(oz, c, fadd(comp(CELL(c_vz, rr), c), fmul(fmul(G.dt, comp(CELL(c_irz, rr), c)), dz)));
+      }
+      st4(vx + g, ox);
+      st4(vz + g, oz);
+    }
+    return;
+  }
   const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -324,7 +376,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
     const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
     float v[12];
     row12(row, v);
-    float4 ox = r_vx[r];
+    float4 ox = CELL(c_vx, rr);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
@@ -333,12 +385,12 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
         float* ps = psx + (size_t)i * G.wx + C.sx[c];
         float psi = *ps; d = cpml(d, psi, C.ax[c], C.bx[c]); *ps = psi;
       }
-      set_comp(ox, c, fadd(comp(r_vx[r], c), fmul(fmul(G.dt, comp(r_irx[r], c)), d)));
+      set_comp(ox, c, fadd(comp(CELL(c_vx, rr), c), fmul(fmul(G.dt, comp(CELL(c_irx, rr), c)), d)));
     }
     st4(vx + g, ox);
     float z[4][2 * M + 1];
     col9<M>(row + 4, z);
-    float4 oz = r_vz[r];
+    float4 oz = CELL(c_vz, rr);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
@@ -347,7 +399,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
         float* ps = psz + (size_t)sz * G.ld + j + c;
         float psi = *ps; d = cpml(d, psi, azi, bzi); *ps = psi;
       }
-      set_comp(oz, c, fadd(comp(r_vz[r], c), fmul(fmul(G.dt, comp(r_irz[r], c)), d)));
+      set_comp(oz, c, fadd(comp(CELL(c_vz, rr), c), fmul(fmul(G.dt, comp(CELL(c_irz, rr), c)), d)));
     }
     st4(vz + g, oz);
   }
@@ -376,20 +428,45 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   stage<M, TZ, XT * BZ>(sxx_s, P.f[E_SXX], G.nzp, G.ld, L.i0, L.j0);
   stage<M, TZ, XT * BZ>(szz_s, P.f[E_SZZ], G.nzp, G.ld, L.i0, L.j0);
   stage<M, TZ, XT * BZ>(sxz_s, P.f[E_SXZ], G.nzp, G.ld, L.i0, L.j0);
+  __shared__ __align__(16) float c_vx[TZ * 32], c_vz[TZ * 32], c_irx[TZ * 32], c_irz[TZ * 32];
+  stage_cells<TZ, XT * BZ>(c_vx, vx, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_vz, vz, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_irx, irx, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_irz, irz, G.nzp, G.ld, L.i0, L.j0);
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
-  float4 r_vx[R], r_vz[R], r_irx[R], r_irz[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int i = L.i0 + threadIdx.y + BZ * r;
-    if (i < G.nzp && j < G.nxp) {
-      const size_t g = (size_t)i * G.ld + j;
-      r_vx[r] = ld4(vx + g); r_vz[r] = ld4(vz + g); r_irx[r] = ldg4(irx + g); r_irz[r] = ldg4(irz + g);
-    }
-  }
   cp_async_wait_all();
   __syncthreads();
   if (j >= G.nxp) return;
+  if (G.interior(L.i0, L.j0, TZ)) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int rr = threadIdx.y + BZ * r;
+      const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+      const size_t g = (size_t)(L.i0 + rr) * G.ld + j;
+      float v[12], z[4][2 * M + 1];
+      float4 ox, oz;
+      row12(sxx_s + ro, v);
+      col9<M>(sxz_s + ro + 4, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float a = G.dxf(sum_plus<M>(v, 4 + c, G.c));
+        const float b = G.dzf(sum_minus<M>(z[c], M, G.c));
+        set_comp(ox, c, fadd(comp(CELL(c_vx, rr), c), fmul(fmul(G.dt, comp(CELL(c_irx, rr), c)), fadd(a, b))));
+      }
+      st4(vx + g, ox);
+      row12(sxz_s + ro, v);
+      col9<M>(szz_s + ro + 4, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float a = G.dxf(sum_minus<M>(v, 4 + c, G.c));
+        const float b = G.dzf(sum_plus<M>(z[c], M, G.c));
+        set_comp(oz, c, fadd(comp(CELL(c_vz, rr), c), fmul(fmul(G.dt, comp(CELL(c_irz, rr), c)), fadd(a, b))));
+      }
+      st4(vz + g, oz);
+    }
+    return;
+  }
   const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -413,7 +490,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) b[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
     }
-    float4 ox = r_vx[r];
+    float4 ox = CELL(c_vx, rr);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
@@ -426,7 +503,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
         float* ps = psz0 + (size_t)sz * G.ld + j + c;
         float psi = *ps; bv = cpml(bv, psi, azi, bzi); *ps = psi;
       }
-      set_comp(ox, c, fadd(comp(r_vx[r], c), fmul(fmul(G.dt, comp(r_irx[r], c)), fadd(av, bv))));
+      set_comp(ox, c, fadd(comp(CELL(c_vx, rr), c), fmul(fmul(G.dt, comp(CELL(c_irx, rr), c)), fadd(av, bv))));
     }
     st4(vx + g, ox);
     // vz: vz_dsxz (x, D⁻ of σxz) + vz_dszz (z, D⁺ of σzz)
@@ -440,7 +517,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) b[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
     }
-    float4 oz = r_vz[r];
+    float4 oz = CELL(c_vz, rr);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
@@ -453,7 +530,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
         float* ps = psz1 + (size_t)sz * G.ld + j + c;
         float psi = *ps; bv = cpml(bv, psi, azi, bzi); *ps = psi;
       }
-      set_comp(oz, c, fadd(comp(r_vz[r], c), fmul(fmul(G.dt, comp(r_irz[r], c)), fadd(av, bv))));
+      set_comp(oz, c, fadd(comp(CELL(c_vz, rr), c), fmul(fmul(G.dt, comp(CELL(c_irz, rr), c)), fadd(av, bv))));
     }
     st4(vz + g, oz);
   }
@@ -505,26 +582,62 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   const float* const azp = P.az; const float* const bzp = P.bz;
   stage<M, TZ, XT * BZ>(svx, P.f[A_VX], G.nzp, G.ld, L.i0, L.j0);
   stage<M, TZ, XT * BZ>(svz, P.f[A_VZ], G.nzp, G.ld, L.i0, L.j0);
+  __shared__ __align__(16) float c_a[TZ * 32], c_b[TZ * 32];   // acoustic: p, κ; viscoacoustic: ε, K_R
+  stage_cells<TZ, XT * BZ>(c_a, VISCO ? eps : p, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_b, cA, G.nzp, G.ld, L.i0, L.j0);
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
   const bool jok = j < G.nxp;
-  float4 r_a[R], r_b[R];   // acoustic: p, κ; viscoacoustic: ε, K_R
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int i = L.i0 + threadIdx.y + BZ * r;
-    if (i < G.nzp && jok) {
-      const size_t g = (size_t)i * G.ld + j;
-      r_a[r] = ld4(VISCO ? eps + g : p + g);
-      r_b[r] = ldg4(cA + g);
-    }
-  }
   float amp, amp_eps;
   source_amps(w, P, amp, amp_eps);
   cp_async_wait_all();
   __syncthreads();
   const size_t npix = (size_t)G.nz * G.nx;
   float peak = 0.f;
-  if (jok) {
+  if (jok && G.interior(L.i0, L.j0, TZ)) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int rr = threadIdx.y + BZ * r;
+      const int i = L.i0 + rr;
+      const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+      const size_t g = (size_t)i * G.ld + j;
+      float v[12], z[4][2 * M + 1];
+      row12(svx + ro, v);
+      col9<M>(svz + ro + 4, z);
+      float4 out, epsv;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float div = fadd(G.dxf(sum_minus<M>(v, 4 + c, G.c)), G.dzf(sum_minus<M>(z[c], M, G.c)));
+        float pv;
+        if constexpr (!VISCO) {
+          pv = fadd(comp(CELL(c_a, rr), c), fmul(fmul(G.dt, comp(CELL(c_b, rr), c)), div));
+        } else {
+          const float inc = fmul(G.dt, div);
+          const float e = fadd(comp(CELL(c_a, rr), c), inc);
+          float total = 0.f;
+          const int q = qidx[g + c];
+          for (int l = 0; l < nL; ++l) {
+            float* rl = r0 + l * fstride;
+            const float rv = fadd(fmul(rl[g + c], __ldg(relax_a + q * nL + l)),
+                                  fmul(__ldg(b0 + l * fstride + g + c), inc));
+            rl[g + c] = rv;
+            total = (l == 0) ? rv : fadd(total, rv);
+          }
+          pv = fadd(fmul(comp(CELL(c_b, rr), c), e), total);
+          set_comp(epsv, c, e);
+          peak = fmaxf(peak, fabsf(pv));
+        }
+        set_comp(out, c, pv);
+      }
+      st4(p + g, out);
+      if constexpr (VISCO) st4(eps + g, epsv);
+      if (w.epi.kind != EPI_NONE) {
+        const size_t pc = (size_t)(i - G.pad) * G.nx + (j - G.pad);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) run_epilogue(w.epi, pc + c, npix, comp(out, c), 0.f);
+      }
+    }
+  } else if (jok) {
     const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -547,8 +660,8 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) dz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
       }
-      float4 out = r_a[r];
-      float4 epsv = r_a[r];
+      float4 out = CELL(c_a, rr);
+      float4 epsv = out;
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (!C.ok[c]) continue;
@@ -566,12 +679,12 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
         const bool src = (i == G.src_iz && jc == G.src_ix && amp != 0.f);
         float pv;
         if constexpr (!VISCO) {
-          pv = fadd(comp(r_a[r], c), fmul(fmul(G.dt, comp(r_b[r], c)), div));
+          pv = fadd(comp(CELL(c_a, rr), c), fmul(fmul(G.dt, comp(CELL(c_b, rr), c)), div));
           if (src) pv = fadd(pv, amp);
           if (G.free_surface && i == G.pad) pv = 0.f;
         } else {
           const float inc = fmul(G.dt, div);
-          float e = fadd(comp(r_a[r], c), inc);
+          float e = fadd(comp(CELL(c_a, rr), c), inc);
           float total = 0.f;
           const int q = qidx[g + c];
           for (int l = 0; l < nL; ++l) {
@@ -581,7 +694,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
             rl[g + c] = rv;
             total = (l == 0) ? rv : fadd(total, rv);
           }
-          pv = fadd(fmul(comp(r_b[r], c), e), total);
+          pv = fadd(fmul(comp(CELL(c_b, rr), c), e), total);
           if (src) {
             e = fadd(e, amp_eps);
             pv = fadd(pv, amp);
@@ -630,26 +743,83 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   const int mech = P.mech;
   stage<M, TZ, XT * BZ>(svx, P.f[E_VX], G.nzp, G.ld, L.i0, L.j0);
   stage<M, TZ, XT * BZ>(svz, P.f[E_VZ], G.nzp, G.ld, L.i0, L.j0);
+  __shared__ __align__(16) float c_xx[TZ * 32], c_zz[TZ * 32], c_xz[TZ * 32], c_lam[TZ * 32], c_l2m[TZ * 32],
+      c_mu[TZ * 32];
+  stage_cells<TZ, XT * BZ>(c_xx, sxx, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_zz, szz, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_xz, sxz, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_lam, clam, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_l2m, cl2m, G.nzp, G.ld, L.i0, L.j0);
+  stage_cells<TZ, XT * BZ>(c_mu, cmu, G.nzp, G.ld, L.i0, L.j0);
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
-  float4 r_xx[R], r_zz[R], r_xz[R], r_lam[R], r_l2m[R], r_mu[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int i = L.i0 + threadIdx.y + BZ * r;
-    if (i < G.nzp && j < G.nxp) {
-      const size_t g = (size_t)i * G.ld + j;
-      r_xx[r] = ld4(sxx + g); r_zz[r] = ld4(szz + g); r_xz[r] = ld4(sxz + g);
-      r_lam[r] = ldg4(clam + g); r_l2m[r] = ldg4(cl2m + g); r_mu[r] = ldg4(cmu + g);
-    }
-  }
   float amp, amp_eps;
   source_amps(w, P, amp, amp_eps);
   cp_async_wait_all();
   __syncthreads();
   if (j >= G.nxp) return;
-  const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
   const size_t npix = (size_t)G.nz * G.nx;
   const Epilogue& E = w.epi;
+  if (G.interior(L.i0, L.j0, TZ)) {
+    const bool want_curl = E.kind != EPI_NONE && E.sep == 1 && E.need_s;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int rr = threadIdx.y + BZ * r;
+      const int i = L.i0 + rr;
+      const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+      const size_t g = (size_t)i * G.ld + j;
+      float v[12], z[4][2 * M + 1];
+      float exx[4], ezz[4], f1[4], f2[4], ca[4], cb[4];
+      row12(svx + ro, v);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) exx[c] = G.dxf(sum_minus<M>(v, 4 + c, G.c));
+      row12(svz + ro, v);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) f2[c] = G.dxf(sum_plus<M>(v, 4 + c, G.c));
+      if (want_curl) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cb[c] = G.dxf(sum_minus<M>(v, 4 + c, G.c));
+      }
+      col9<M>(svx + ro + 4, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) f1[c] = G.dzf(sum_plus<M>(z[c], M, G.c));
+      if (want_curl) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ca[c] = G.dzf(sum_minus<M>(z[c], M, G.c));
+      }
+      col9<M>(svz + ro + 4, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ezz[c] = G.dzf(sum_minus<M>(z[c], M, G.c));
+      float4 oxx, ozz, oxz;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float lam = comp(CELL(c_lam, rr), c), l2m = comp(CELL(c_l2m, rr), c);
+        set_comp(oxx, c, fadd(comp(CELL(c_xx, rr), c), fmul(G.dt, fadd(fmul(l2m, exx[c]), fmul(lam, ezz[c])))));
+        set_comp(ozz, c, fadd(comp(CELL(c_zz, rr), c), fmul(G.dt, fadd(fmul(lam, exx[c]), fmul(l2m, ezz[c])))));
+        set_comp(oxz, c, fadd(comp(CELL(c_xz, rr), c), fmul(fmul(G.dt, comp(CELL(c_mu, rr), c)), fadd(f1[c], f2[c]))));
+      }
+      st4(sxx + g, oxx);
+      st4(szz + g, ozz);
+      st4(sxz + g, oxz);
+      if (E.kind != EPI_NONE) {
+        const size_t pc = (size_t)(i - G.pad) * G.nx + (j - G.pad);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          float pv, sv = 0.f;
+          if (E.sep == 0) {
+            pv = fmul(0.5f, fadd(comp(oxx, c), comp(ozz, c)));
+            sv = comp(oxz, c);
+          } else {
+            pv = fadd(exx[c], ezz[c]);
+            if (want_curl) sv = fsub(ca[c], cb[c]);
+          }
+          run_epilogue(E, pc + c, npix, pv, sv);
+        }
+      }
+    }
+    return;
+  }
+  const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int rr = threadIdx.y + BZ * r;
@@ -684,7 +854,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) ezz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
     }
-    float4 oxx = r_xx[r], ozz = r_zz[r], oxz = r_xz[r];
+    float4 oxx = CELL(c_xx, rr), ozz = CELL(c_zz, rr), oxz = CELL(c_xz, rr);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
@@ -703,10 +873,10 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
         float* p1 = psz3 + (size_t)sz * G.ld + jc;
         psi = *p1; g1 = cpml(g1, psi, azi, bzi); *p1 = psi;
       }
-      const float lam = comp(r_lam[r], c), l2m = comp(r_l2m[r], c);
-      float vxx = fadd(comp(r_xx[r], c), fmul(G.dt, fadd(fmul(l2m, ex), fmul(lam, ez))));
-      float vzz = fadd(comp(r_zz[r], c), fmul(G.dt, fadd(fmul(lam, ex), fmul(l2m, ez))));
-      float vxz = fadd(comp(r_xz[r], c), fmul(fmul(G.dt, comp(r_mu[r], c)), fadd(g1, g2)));
+      const float lam = comp(CELL(c_lam, rr), c), l2m = comp(CELL(c_l2m, rr), c);
+      float vxx = fadd(comp(CELL(c_xx, rr), c), fmul(G.dt, fadd(fmul(l2m, ex), fmul(lam, ez))));
+      float vzz = fadd(comp(CELL(c_zz, rr), c), fmul(G.dt, fadd(fmul(lam, ex), fmul(l2m, ez))));
+      float vxz = fadd(comp(CELL(c_xz, rr), c), fmul(fmul(G.dt, comp(CELL(c_mu, rr), c)), fadd(g1, g2)));
       if (i == G.src_iz && jc == G.src_ix && amp != 0.f) {
         if (mech == MECH_SHEAR) {
           vxz = fadd(vxz, amp);
@@ -741,5 +911,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
     st4(sxz + g, oxz);
   }
 }
+
+#undef CELL
 
 }  // namespace ertm

@@ -120,6 +120,10 @@ int64_t ertm_launch_count(void);
 /* Pin the stencil tile height (8, 16 or 32 rows; 0 = automatic) for
  * propagators created afterwards — the autotuner's knob (order 8 only). */
 int32_t ertm_set_tile_rows(int32_t rows);
+/* Count, over all 2^32 float inputs a, where the fast division form `mode`
+ * (3 one-FMA, 2 FMA correction, 1 float64 product) differs in value from
+ * __fdiv_rn(a, h) (no reference counterpart; diagnostics). */
+int32_t ertm_division_check(float h, int32_t mode, uint64_t* mismatches);
 int32_t ertm_profile_stencil(int32_t enable, int32_t every);
 int32_t ertm_profile_read(double* total_ms, int64_t* samples, double* total_bytes);
 
