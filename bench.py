@@ -8,8 +8,9 @@ benchmark step migrates all shots of the job (PP and PS from one
 forward/replay/backward pass per shot) and stacks them.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-    torchrun --nproc-per-node N bench.py --gpus N ...   (weak scaling: every
-        rank migrates its own 8 shots; the stacks are summed with NCCL)
+    torchrun --nproc-per-node N bench.py --gpus N ...   (weak scaling: a job
+        of 8·N shots sharded over the ranks; one NCCL all-reduce of the
+        float64 stack per job)
 
 One JSON line is printed by rank 0.
 """
@@ -46,6 +47,7 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=48)
+    ap.add_argument("--serve-jobs", type=int, default=24, help="jobs in the serving run (0: no serving run)")
     return ap.parse_args()
 
 
@@ -53,12 +55,12 @@ def parse_args() -> argparse.Namespace:
 # distributed plumbing
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self) -> None:
+    def __init__(self, join: bool = True) -> None:
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
-        if self.world > 1:
+        if self.world > 1 and join:
             import datetime
 
             import torch
@@ -159,18 +161,27 @@ def committed_traffic(name: str) -> float | None:
 # ---------------------------------------------------------------------------
 # workload helpers
 # ---------------------------------------------------------------------------
-def build_workload(args, rank: int):
+def build_workload(args, world: int):
+    """The job's workload: the configuration's shots per GPU times the world
+    size (weak scaling), every rank building the same seeded job."""
     from ertm_b200 import workloads
-    wl = workloads.WORKLOADS[args.config](seed=0, **({"n_shots": args.shots} if args.shots else {}),
-                                          **({"nt": args.nt} if args.nt else {}))
-    if rank:
-        # weak scaling: same model, a different seeded shot set per rank
-        rng = np.random.default_rng(1000 + rank)
-        g = wl.model.grid
-        from ertm_b200.types import SourceSpec
-        wl.sources = [SourceSpec(x=float(x), z=s.z, f0=s.f0, delay=s.delay)
-                      for x, s in zip(np.sort(rng.uniform(0.05, 0.95, len(wl.sources)) * g.x_max), wl.sources)]
+    kw = {"nt": args.nt} if args.nt else {}
+    make = workloads.WORKLOADS[args.config]
+    wl = make(seed=0, **kw, **({"n_shots": args.shots} if args.shots else {}))
+    if world > 1:
+        wl = make(seed=0, n_shots=len(wl.sources) * world, **kw)
     return wl
+
+
+def job_config(wl, args, world: int) -> dict:
+    g = wl.model.grid
+    return {"workload": wl.name, "config": args.config, "nx": g.nx, "nz": g.nz, "dx": g.dx, "nt": wl.nt,
+            "dt": wl.dt, "engine": wl.engine, "modes": list(wl.modes), "condition": wl.condition,
+            "separation": wl.separation, "shots_per_job": len(wl.sources), "receivers": wl.receivers.nrec,
+            "components": list(wl.components), "accumulation": "fp64",
+            "l2": "flushed between steps (256 MiB write)",
+            "path": "batched: all shots of a rank in lockstep ticks (form b)",
+            "parallelism": f"shots sharded over {world} GPU(s), one float64 all-reduce of the stack per job"}
 
 
 def imager_for(wl):
@@ -183,11 +194,11 @@ def imager_for(wl):
     return RTMImager(imaging, solver, q), solver
 
 
-def synthesize(wl, solver):
+def synthesize(wl, solver, sources):
     """Shot records from the GPU forward model (untimed set-up)."""
     from ertm_b200.solver import FiniteDifferenceSolver
     fd = FiniteDifferenceSolver(solver)
-    return [fd.forward(wl.model, s, wl.receivers, components=wl.components) for s in wl.sources]
+    return [fd.forward(wl.model, s, wl.receivers, components=wl.components) for s in sources]
 
 
 def step_bytes(prop) -> float:
@@ -266,11 +277,58 @@ def run_reference(args, dist: Dist) -> None:
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": args.config},
+            "config": job_config(build_workload(args, dist.world), args, dist.world),
             "gcell_updates_per_s": value * 3 * nt * cells * times[0][1][0]["migrates_per_shot"] / 1e9,
             "cpu_baseline": {"value": value, "unit": "shots/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# serving (form c)
+# ---------------------------------------------------------------------------
+def serving_run(n_jobs: int) -> dict:
+    """The serving loop on a stream of mixed jobs: once with every job queued
+    at t=0 (saturation), then with Poisson arrivals at 50 % and 80 % of the
+    saturated job rate; per-shot latency = shot completion - job submission."""
+    from ertm_b200 import workloads
+    from ertm_b200.serving import RTMServer, percentile
+    spec = dict(max_scale=(4.0, 2.0), nt_range=(500, 2000), max_shots=4)
+    jobs = workloads.serving_jobs(seed=1, n_jobs=n_jobs, **spec)
+    n_shots = sum(len(j.shots) for j in jobs)
+    cells = sum(3 * j.model.grid.nx * j.model.grid.nz * j.imager.solver_config.nt * len(j.shots) for j in jobs)
+
+    def run(arrivals):
+        with RTMServer() as srv:
+            t0 = time.perf_counter()
+            futs = []
+            for job, at in zip(jobs, arrivals):
+                delay = t0 + at - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                futs.append(srv.submit(job))
+            res = [f.result() for f in futs]
+            wall = max(r.finished for r in res) - t0
+        lat = [x for r in res for x in r.shot_latencies]
+        return {"shots_per_s": n_shots / wall, "wall_s": wall, "shot_latency_p50_s": percentile(lat, 50),
+                "shot_latency_p99_s": percentile(lat, 99),
+                "job_latency_p50_s": percentile([r.latency for r in res], 50),
+                "job_latency_p99_s": percentile([r.latency for r in res], 99),
+                "peak_active_shots": srv.stats["peak_active"], "peak_bytes": srv.stats["peak_bytes"]}
+
+    run([0.0] * len(jobs))                      # warm-up (division checks, FFT plans, memory pool)
+    sat = run([0.0] * len(jobs))
+    job_rate = len(jobs) / sat["wall_s"]
+    rng = np.random.default_rng(7)
+    out = {"workload": (f"{n_jobs} jobs, engine uniform over acoustic/elastic/viscoacoustic, grid 256x256..1024x512 "
+                        f"log-uniform at 5-10 m, nt 500-2000, 1-4 shots, normalized, seeded noise records"),
+           "shots": n_shots, "gcell_updates": cells / 1e9, "saturation": sat,
+           "saturation_gcell_updates_per_s": cells / sat["wall_s"] / 1e9}
+    for frac in (0.5, 0.8):
+        lam = frac * job_rate
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, len(jobs)))
+        out[f"poisson_{int(frac * 100)}pct"] = {"lambda_jobs_per_s": lam, **run(list(arrivals))}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -284,31 +342,43 @@ def run_ours(args, dist: Dist) -> None:
     from ertm_b200 import _lib
     from ertm_b200.batch import migrate_device_batch
     from ertm_b200.imaging import ShotMigrator
+    from ertm_b200.parallel import ShotParallelMigrator, plan_shards, reduce_partial_sums, shot_cost
     from ertm_b200.propagation import source_wavelet
-    from ertm_b200.stacking import stack_images
     from ertm_b200.types import ShotRecord
 
     dev = dist.local
     torch.cuda.set_device(dev)
     L = _lib.lib(dev)
-    wl = build_workload(args, dist.rank)
+    wl = build_workload(args, dist.world)
     imager, solver = imager_for(wl)
-    shots = synthesize(wl, solver)
+    g = wl.model.grid
+    n_total = len(wl.sources)
+    mine = plan_shards([shot_cost(g.nx, g.nz, wl.nt, wl.engine)] * n_total, dist.world)[dist.rank]
+    sources = [wl.sources[i] for i in mine]
+    shots = synthesize(wl, solver, sources)
     names = list(wl.components)
     rec_dev = [torch.from_numpy(np.stack([s.components[n] for n in names])).cuda() for s in shots]
-    wavelets = [source_wavelet(s, wl.dt, wl.nt) for s in wl.sources]
-    g = wl.model.grid
+    wavelets = [source_wavelet(s, wl.dt, wl.nt) for s in sources]
     n_modes = len(wl.modes)
-    n_shots = len(wl.sources)
+    n_shots = len(sources)
+    npix = g.nx * g.nz
     plain_mig = ShotMigrator(imager, wl.model)                       # one propagator pair, reused
     batch_migs = [ShotMigrator(imager, wl.model) for _ in range(n_shots)]  # one pair per shot
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
+    partial = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float64, device="cuda")
 
     def stack(imgs, out):
+        """This rank's float64 partial stack, the job's one all-reduce, finish."""
+        partial.zero_()
         for k in range(n_modes):
             ptrs = (C.c_void_p * len(imgs))(*[im[k].data_ptr() for im in imgs])
-            _lib.check(L.ertm_stack(len(imgs), g.nz * g.nx, C.cast(ptrs, C.c_void_p), 1, out[k].data_ptr(), None),
-                       "stack")
+            _lib.check(L.ertm_stack_partial(len(imgs), npix, C.cast(ptrs, C.c_void_p), int(n_total > 1),
+                                            partial[k].data_ptr(), None), "stack partial")
+        if dist.world > 1:
+            reduce_partial_sums(partial)
+        for k in range(n_modes):
+            _lib.check(L.ertm_stack_finish(npix, partial[k].data_ptr(), n_total, out[k].data_ptr(), None),
+                       "stack finish")
         return out
 
     out_plain = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float32, device="cuda")
@@ -316,11 +386,11 @@ def run_ours(args, dist: Dist) -> None:
 
     def plain_job():
         imgs = [plain_mig.migrate_device(src, wl.receivers, rec_dev[i], names, wavelets[i], modes=wl.modes)
-                for i, src in enumerate(wl.sources)]
+                for i, src in enumerate(sources)]
         return stack(imgs, out_plain)
 
     def batch_job():
-        imgs = migrate_device_batch(imager, batch_migs, wl.sources, [wl.receivers] * n_shots, rec_dev, names,
+        imgs = migrate_device_batch(imager, batch_migs, sources, [wl.receivers] * n_shots, rec_dev, names,
                                     wavelets, modes=wl.modes)
         return stack(imgs, out_batch)
 
@@ -359,36 +429,47 @@ def run_ours(args, dist: Dist) -> None:
 
     total_ms = dist.max(float(sum(times)))
     plain_ms = dist.max(float(sum(plain_times)))
-    shots_total = n_shots * dist.world * args.steps
+    shots_total = n_total * args.steps
     value = shots_total / (total_ms / 1e3)
     plain_value = shots_total / (plain_ms / 1e3)
     cell_updates = 3 * wl.nt * wl.cells * shots_total
-    if dist.world > 1:
-        dist.sum_(out_batch)      # the only collective: the stacks of all ranks
-        out_batch /= dist.world
 
-    # end to end through the public API: pinned host records in, host image out
+    # end to end through the public API: every rank is handed the whole job as
+    # host shot records (pinned), migrates its shard and gets the stacked host
+    # images back; host<->device copies are inside the timed region
     pinned = [{n: torch.from_numpy(s.components[n]).pin_memory().numpy() for n in names} for s in shots]
+    host_shots = [None] * n_total
+    for j, i in enumerate(mine):
+        s = shots[j]
+        host_shots[i] = ShotRecord(data=pinned[j][names[0]], dt=s.dt, t=s.t, receivers=s.receivers, source=s.source,
+                                   components=pinned[j])
+    for i in range(n_total):        # other ranks' shots: only their shape enters the shard plan here
+        if host_shots[i] is None:
+            host_shots[i] = ShotRecord(data=np.zeros((wl.nt, wl.receivers.nrec), np.float32), dt=wl.dt,
+                                       t=np.arange(wl.nt) * wl.dt, receivers=wl.receivers, source=wl.sources[i],
+                                       components={n: np.zeros((wl.nt, wl.receivers.nrec), np.float32)
+                                                   for n in names})
+    spm = ShotParallelMigrator(imager, group=None)
     e2e_times = []
     for _ in range(args.e2e_steps):
         dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        from ertm_b200.batch import BatchMigrator
-        host_shots = [ShotRecord(data=pinned[i][names[0]], dt=s.dt, t=s.t, receivers=s.receivers, source=s.source,
-                                 components=pinned[i]) for i, s in enumerate(shots)]
-        per_shot = BatchMigrator(imager).migrate_shots(host_shots, wl.model, modes=wl.modes)
-        stacked = {m: stack_images([r[k] for r in per_shot], normalize=True).image for k, m in enumerate(wl.modes)}
+        stacked = spm.migrate_job(host_shots, wl.model, modes=wl.modes)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-        assert all(np.isfinite(v).all() for v in stacked.values())
-    npix = g.nx * g.nz
+        assert all(np.isfinite(r.image).all() for r in stacked)
     comp_bytes = len(names) * wl.nt * wl.receivers.nrec * 4
     model_bytes = 3 * npix * 4 * 2                      # vp, vs, rho per propagator, two propagators
-    h2d = n_shots * (comp_bytes + model_bytes + 3 * n_modes * npix * 8 + wl.nt * 4)
-    d2h = n_shots * (3 * n_modes * npix * 8 + n_modes * npix * 4) + n_modes * npix * 4
-    e2e_s = dist.max(statistics.mean(e2e_times))
-    e2e_value = n_shots * dist.world / e2e_s
+    # summed over the job's ranks: records, models, accumulators and wavelets in; accumulators, images out
+    h2d = n_total * (comp_bytes + model_bytes + 3 * n_modes * npix * 8 + wl.nt * 4 + n_modes * npix * 4)
+    d2h = n_total * (3 * n_modes * npix * 8 + n_modes * npix * 4) + dist.world * n_modes * npix * 4
+    e2e_s = dist.max(statistics.mean(e2e_times)) if e2e_times else float("nan")
+    e2e_value = n_total / e2e_s
+
+    serving = None
+    if dist.world == 1 and args.serve_jobs > 0:
+        serving = serving_run(args.serve_jobs)
 
     peak, peak_kind = measured_hbm_peak()
     step_ms = float(tot.value) / max(int(cnt.value), 1)
@@ -405,12 +486,7 @@ def run_ours(args, dist: Dist) -> None:
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded layered model with cavities and a fault; records from the GPU forward model",
-        "config": {"workload": wl.name, "config": args.config, "nx": g.nx, "nz": g.nz, "dx": g.dx, "nt": wl.nt,
-                   "dt": wl.dt, "engine": wl.engine, "modes": list(wl.modes), "condition": wl.condition,
-                   "separation": wl.separation, "shots_per_rank": n_shots, "receivers": wl.receivers.nrec,
-                   "components": names, "accumulation": "fp64", "l2": "flushed between steps (256 MiB write)",
-                   "path": "batched: all shots of the job in lockstep ticks (form b)",
-                   "parallelism": f"shots x{dist.world}"},
+        "config": job_config(wl, args, dist.world),
         "gcell_updates_per_s": cell_updates / (total_ms / 1e3) / 1e9,
         "plain": {"value": plain_value, "unit": "shots/s", "ms_per_step": plain_ms / args.steps,
                   "gcell_updates_per_s": cell_updates / (plain_ms / 1e3) / 1e9,
@@ -426,6 +502,7 @@ def run_ours(args, dist: Dist) -> None:
                      "bytes_per_tick": float(byt.value) / max(int(cnt.value), 1), "tick_us": step_ms * 1e3,
                      "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,
+        "serving": serving,
         "clocks": clk,
         "gpu_launches": launches,
     }
@@ -435,7 +512,9 @@ def run_ours(args, dist: Dist) -> None:
 
 def main() -> None:
     args = parse_args()
-    dist = Dist()
+    # the reference arm is a CPU run on rank 0 alone: no process group, so the
+    # other ranks exit at once instead of waiting for rank 0 in a collective
+    dist = Dist(join=args.impl != "reference")
     try:
         if args.impl == "reference":
             run_reference(args, dist)

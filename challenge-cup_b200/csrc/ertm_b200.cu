@@ -1119,175 +1119,205 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
   }
 }
 
-void migrate_batch(std::vector<ShotRun>& runs, cudaStream_t st) {
+// DevProp table of every propagator of `runs` (uploaded when the set changes).
+void upload_table(std::vector<ShotRun*>& runs, std::vector<DevProp>& table, DevBuf& dtable, cudaStream_t st) {
+  table.clear();
+  for (ShotRun* R : runs) {
+    R->fi = (int)table.size();
+    table.push_back(R->F->h);
+    R->bi = (int)table.size();
+    table.push_back(R->B->h);
+  }
+  const size_t bytes = std::max<size_t>(1, table.size()) * sizeof(DevProp);
+  if (dtable.bytes < bytes) dtable = DevBuf(bytes, st);
+  upload(dtable.p, table.data(), table.size() * sizeof(DevProp), st);
+}
+
+// One tick of the batched schedule: every unfinished shot of `runs` gets at
+// most one forward/replay step and one backward step.  Returns false when no
+// shot had work left.
+bool batch_tick(std::vector<ShotRun*>& runs, const DevProp* dt, cudaStream_t st) {
   static_assert(sizeof(WorkSetB) < 30000, "kernel parameter block too large");
   static_assert(sizeof(InjectBatch) < 30000, "kernel parameter block too large");
-  // one DevProp table for every propagator of the batch
-  std::vector<DevProp> table;
-  for (ShotRun& R : runs) {
-    R.fi = (int)table.size();
-    table.push_back(R.F->h);
-    R.bi = (int)table.size();
-    table.push_back(R.B->h);
-  }
-  DevBuf dtable(table.size() * sizeof(DevProp), st);
-  upload(dtable.p, table.data(), dtable.bytes, st);
-  const DevProp* dt = dtable.as<DevProp>();
   std::vector<TickItem> items;
   items.reserve(2 * runs.size());
-  while (true) {
-    items.clear();
-    std::vector<std::pair<ShotRun*, int>> restores, injections;
-    for (ShotRun& R : runs) {
-      switch (R.phase) {
-        case 0: {  // forward with checkpoints
-          TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.t_f, nullptr), false, {}};
-          it.w.prop = R.fi;
-          items.push_back(it);
-          break;
-        }
-        case 1: {  // replay of block rp_block overlapped with the backward over bk_block
-          const bool do_rp = R.rp_block >= 0 && R.bk_block <= R.rp_block + 1;
-          const bool do_bk = R.bk_block >= 0 && R.replayed_below <= R.bk_block;
-          if (do_rp) {
-            if (R.rp_t == R.s_of(R.rp_block)) restores.push_back({&R, R.rp_block});
-            Epilogue e = replay_epilogue(R, R.rp_block, R.rp_t);
-            TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.rp_t, R.fwd_unfused ? nullptr : &e),
-                        R.fwd_unfused, e};
-            it.w.prop = R.fi;
-            items.push_back(it);
-          }
-          if (do_bk) {
-            injections.push_back({&R, R.bk_t});
-            Epilogue e = backward_epilogue(R, R.bk_block, R.bk_t);
-            const bool unf = R.bwd_unfused && e.kind != EPI_NONE;
-            TickItem it{&R, false, make_work(*R.B, 0.0, nullptr, 0, unf ? nullptr : &e), unf, e};
-            it.w.prop = R.bi;
-            items.push_back(it);
-          }
-          break;
-        }
-        case 2: {  // excitation map: replay every block forward
+  std::vector<std::pair<ShotRun*, int>> restores, injections;
+  for (ShotRun* Rp : runs) {
+    ShotRun& R = *Rp;
+    switch (R.phase) {
+      case 0: {  // forward with checkpoints
+        TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.t_f, nullptr), false, {}};
+        it.w.prop = R.fi;
+        items.push_back(it);
+        break;
+      }
+      case 1: {  // replay of block rp_block overlapped with the backward over bk_block
+        const bool do_rp = R.rp_block >= 0 && R.bk_block <= R.rp_block + 1;
+        const bool do_bk = R.bk_block >= 0 && R.replayed_below <= R.bk_block;
+        if (do_rp) {
           if (R.rp_t == R.s_of(R.rp_block)) restores.push_back({&R, R.rp_block});
           Epilogue e = replay_epilogue(R, R.rp_block, R.rp_t);
           TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.rp_t, R.fwd_unfused ? nullptr : &e),
                       R.fwd_unfused, e};
           it.w.prop = R.fi;
           items.push_back(it);
-          break;
         }
-        case 3: {  // excitation backward over [0, nt_spec)
+        if (do_bk) {
           injections.push_back({&R, R.bk_t});
-          Epilogue e = backward_epilogue(R, 0, R.bk_t);
+          Epilogue e = backward_epilogue(R, R.bk_block, R.bk_t);
           const bool unf = R.bwd_unfused && e.kind != EPI_NONE;
           TickItem it{&R, false, make_work(*R.B, 0.0, nullptr, 0, unf ? nullptr : &e), unf, e};
           it.w.prop = R.bi;
           items.push_back(it);
-          break;
         }
-        default:
-          break;
+        break;
       }
-    }
-    if (items.empty()) break;
-    for (auto& r : restores) restore_checkpoint(*r.first, r.second, st);
-    // time-reversed record injection of this tick's backward steps
-    for (size_t c0 = 0; c0 < injections.size(); c0 += MAX_BATCH_WORKS) {
-      InjectBatch ib{};
-      int cells = 0;
-      for (size_t k = c0; k < std::min(injections.size(), c0 + MAX_BATCH_WORKS); ++k) {
-        ShotRun& R = *injections[k].first;
-        if (!R.plan) continue;
-        InjectItem& I = ib.it[ib.n++];
-        I.plan = R.plan->dev();
-        I.prop = dt + R.bi;
-        I.record = R.rec.as<float>();
-        I.time_offset = (int64_t)injections[k].second * R.nrec;
-        I.cell0 = cells;
-        cells += R.plan->n_cells;
+      case 2: {  // excitation map: replay every block forward
+        if (R.rp_t == R.s_of(R.rp_block)) restores.push_back({&R, R.rp_block});
+        Epilogue e = replay_epilogue(R, R.rp_block, R.rp_t);
+        TickItem it{&R, true, make_work(*R.F, 0.0, R.wave.as<float>(), R.rp_t, R.fwd_unfused ? nullptr : &e),
+                    R.fwd_unfused, e};
+        it.w.prop = R.fi;
+        items.push_back(it);
+        break;
       }
-      if (cells > 0) {
-        k_inject_batch<<<(cells + 127) / 128, 128, 0, st>>>(ib);
-        ++g_launches;
+      case 3: {  // excitation backward over [0, nt_spec)
+        injections.push_back({&R, R.bk_t});
+        Epilogue e = backward_epilogue(R, 0, R.bk_t);
+        const bool unf = R.bwd_unfused && e.kind != EPI_NONE;
+        TickItem it{&R, false, make_work(*R.B, 0.0, nullptr, 0, unf ? nullptr : &e), unf, e};
+        it.w.prop = R.bi;
+        items.push_back(it);
+        break;
       }
+      default:
+        break;
     }
-    // stencil launches, grouped by (engine, order)
-    std::map<std::pair<int, int>, std::vector<TickItem*>> groups;
-    for (TickItem& it : items) {
-      const Prop& P = it.fwd ? *it.run->F : *it.run->B;
-      groups[{P.h.engine, P.M}].push_back(&it);
+  }
+  if (items.empty()) return false;
+  for (auto& r : restores) restore_checkpoint(*r.first, r.second, st);
+  // time-reversed record injection of this tick's backward steps
+  for (size_t c0 = 0; c0 < injections.size(); c0 += MAX_BATCH_WORKS) {
+    InjectBatch ib{};
+    int cells = 0;
+    for (size_t k = c0; k < std::min(injections.size(), c0 + MAX_BATCH_WORKS); ++k) {
+      ShotRun& R = *injections[k].first;
+      if (!R.plan) continue;
+      InjectItem& I = ib.it[ib.n++];
+      I.plan = R.plan->dev();
+      I.prop = dt + R.bi;
+      I.record = R.rec.as<float>();
+      I.time_offset = (int64_t)injections[k].second * R.nrec;
+      I.cell0 = cells;
+      cells += R.plan->n_cells;
     }
-    cudaEvent_t e0 = nullptr;
-    const bool timed = g_prof.begin(st, e0);
-    double bytes = 0.0;
-    for (auto& g : groups) launch_group(g.second, dt, st, bytes);
-    if (timed) g_prof.end(st, e0, bytes);
-    // after the stress phase: sources on vz, stabilisation, stand-alone epilogues, checkpoints
-    for (TickItem& it : items) {
-      ShotRun& R = *it.run;
-      Prop& P = it.fwd ? *R.F : *R.B;
-      after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t);
-      if (it.unfused) launch_epilogue(P, it.epi);
-      if (R.phase == 0 && R.t_f % R.iv == 0) save_checkpoint(R, R.t_f / R.iv, st);
+    if (cells > 0) {
+      k_inject_batch<<<(cells + 127) / 128, 128, 0, st>>>(ib);
+      ++g_launches;
     }
-    CK(cudaGetLastError());
-    // advance the schedules
-    for (ShotRun& R : runs) {
-      switch (R.phase) {
-        case 0:
-          if (++R.t_f == R.nt) {
-            if (!R.excitation) {
-              R.phase = 1;
-              R.rp_block = R.bk_block = R.n_states - 1;
-              R.rp_t = R.s_of(R.rp_block);
-              R.bk_t = R.e_of(R.bk_block) - 1;
-              R.replayed_below = R.n_states;
-            } else {
-              R.phase = 2;
-              R.rp_block = 0;
-              R.rp_t = 0;
-            }
+  }
+  // stencil launches, grouped by (engine, order)
+  std::map<std::pair<int, int>, std::vector<TickItem*>> groups;
+  for (TickItem& it : items) {
+    const Prop& P = it.fwd ? *it.run->F : *it.run->B;
+    groups[{P.h.engine, P.M}].push_back(&it);
+  }
+  cudaEvent_t e0 = nullptr;
+  const bool timed = g_prof.begin(st, e0);
+  double bytes = 0.0;
+  for (auto& g : groups) launch_group(g.second, dt, st, bytes);
+  if (timed) g_prof.end(st, e0, bytes);
+  // after the stress phase: sources on vz, stabilisation, stand-alone epilogues, checkpoints
+  for (TickItem& it : items) {
+    ShotRun& R = *it.run;
+    Prop& P = it.fwd ? *R.F : *R.B;
+    after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t);
+    if (it.unfused) launch_epilogue(P, it.epi);
+    if (R.phase == 0 && R.t_f % R.iv == 0) save_checkpoint(R, R.t_f / R.iv, st);
+  }
+  CK(cudaGetLastError());
+  // advance the schedules
+  for (ShotRun* Rp : runs) {
+    ShotRun& R = *Rp;
+    switch (R.phase) {
+      case 0:
+        if (++R.t_f == R.nt) {
+          if (!R.excitation) {
+            R.phase = 1;
+            R.rp_block = R.bk_block = R.n_states - 1;
+            R.rp_t = R.s_of(R.rp_block);
+            R.bk_t = R.e_of(R.bk_block) - 1;
+            R.replayed_below = R.n_states;
+          } else {
+            R.phase = 2;
+            R.rp_block = 0;
+            R.rp_t = 0;
           }
-          break;
-        case 1: {
-          const bool did_rp = R.rp_block >= 0 && R.bk_block <= R.rp_block + 1;
-          const bool did_bk = R.bk_block >= 0 && R.replayed_below <= R.bk_block;
-          if (did_bk) {
-            if (--R.bk_t < R.s_of(R.bk_block)) {
-              --R.bk_block;
-              if (R.bk_block >= 0) R.bk_t = R.e_of(R.bk_block) - 1;
-            }
-          }
-          if (did_rp) {
-            if (++R.rp_t == R.e_of(R.rp_block)) {
-              R.replayed_below = R.rp_block;
-              --R.rp_block;
-              if (R.rp_block >= 0) R.rp_t = R.s_of(R.rp_block);
-            }
-          }
-          if (R.bk_block < 0) R.phase = 4;
-          break;
         }
-        case 2:
+        break;
+      case 1: {
+        const bool did_rp = R.rp_block >= 0 && R.bk_block <= R.rp_block + 1;
+        const bool did_bk = R.bk_block >= 0 && R.replayed_below <= R.bk_block;
+        if (did_bk) {
+          if (--R.bk_t < R.s_of(R.bk_block)) {
+            --R.bk_block;
+            if (R.bk_block >= 0) R.bk_t = R.e_of(R.bk_block) - 1;
+          }
+        }
+        if (did_rp) {
           if (++R.rp_t == R.e_of(R.rp_block)) {
-            if (++R.rp_block == R.n_states) {
-              R.phase = 3;
-              R.bk_t = R.cfg.nt_spec - 1;
-            } else {
-              R.rp_t = R.s_of(R.rp_block);
-            }
+            R.replayed_below = R.rp_block;
+            --R.rp_block;
+            if (R.rp_block >= 0) R.rp_t = R.s_of(R.rp_block);
           }
-          break;
-        case 3:
-          if (--R.bk_t < 0) R.phase = 4;
-          break;
-        default:
-          break;
+        }
+        if (R.bk_block < 0) R.phase = 4;
+        break;
       }
+      case 2:
+        if (++R.rp_t == R.e_of(R.rp_block)) {
+          if (++R.rp_block == R.n_states) {
+            R.phase = 3;
+            R.bk_t = R.cfg.nt_spec - 1;
+          } else {
+            R.rp_t = R.s_of(R.rp_block);
+          }
+        }
+        break;
+      case 3:
+        if (--R.bk_t < 0) R.phase = 4;
+        break;
+      default:
+        break;
     }
+  }
+  return true;
+}
+
+void migrate_batch(std::vector<ShotRun>& runs, cudaStream_t st) {
+  std::vector<ShotRun*> ptrs;
+  for (ShotRun& R : runs) ptrs.push_back(&R);
+  std::vector<DevProp> table;
+  DevBuf dtable;
+  upload_table(ptrs, table, dtable, st);
+  while (batch_tick(ptrs, dtable.as<DevProp>(), st)) {
   }
   for (ShotRun& R : runs) finish_run(R, st);
 }
+
+// --------------------------------------------------------------------------
+// Batch sessions (serving): shots join between ticks and leave when done, so
+// shots that arrive while others run share their ticks (continuous batching).
+// --------------------------------------------------------------------------
+struct Session {
+  cudaStream_t st = nullptr;
+  std::vector<std::unique_ptr<ShotRun>> runs;
+  std::vector<int64_t> tags;
+  std::vector<DevProp> table;
+  DevBuf dtable;
+  bool dirty = true;
+  int64_t ticks = 0;
+};
 
 // --------------------------------------------------------------------------
 // Allocation-free stacking (ertm_stack_noalloc)
@@ -1331,7 +1361,7 @@ void require_device_pointer(const void* p, const char* what) {
   cudaPointerAttributes a{};
   CK(cudaPointerGetAttributes(&a, p));
   REQUIRE(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged,
-          std::string(what) + " must be device memory (ertm_stack_noalloc copies nothing through the host)");
+          std::string(what) + " must be device memory");
 }
 
 }  // namespace
@@ -1708,6 +1738,90 @@ int32_t ertm_migrate_batch(int32_t n_shots, const ertm_batch_shot* shots) {
   });
 }
 
+int32_t ertm_session_create(void** out) {
+  return guarded([&] {
+    REQUIRE(out, "bad arguments");
+    auto S = std::make_unique<Session>();
+    // a blocking stream: work the caller queued on the legacy default stream
+    // (inputs, output buffers) is ordered before the session's ticks
+    CK(cudaStreamCreate(&S->st));
+    *out = S.release();
+  });
+}
+
+int32_t ertm_session_add(void* session, const ertm_batch_shot* shot, int64_t tag) {
+  return guarded([&] {
+    REQUIRE(session && shot, "bad arguments");
+    Session& S = *static_cast<Session*>(session);
+    const ertm_batch_shot& B = *shot;
+    REQUIRE(B.fwd && B.back && B.wavelet, "missing propagator or wavelet");
+    REQUIRE(B.fwd != B.back, "a shot needs two propagators");
+    REQUIRE(B.cfg.n_comp == 0 || B.record, "record missing");
+    for (auto& R : S.runs)
+      REQUIRE(R->F != B.fwd && R->B != B.back && R->F != B.back && R->B != B.fwd,
+              "the propagators are in use by another shot of the session");
+    for (int64_t t : S.tags) REQUIRE(t != tag, "tag already in use");
+    auto R = std::make_unique<ShotRun>();
+    prepare_run(*R, *static_cast<Prop*>(B.fwd), *static_cast<Prop*>(B.back), B.cfg, B.wavelet, B.record, B.num,
+                B.illum, B.rillum, S.st, 2);
+    S.runs.push_back(std::move(R));
+    S.tags.push_back(tag);
+    S.dirty = true;
+  });
+}
+
+int32_t ertm_session_advance(void* session, int32_t max_ticks, int64_t* done_tags, int32_t cap, int32_t* n_done) {
+  return guarded([&] {
+    REQUIRE(session && n_done && max_ticks >= 0 && cap >= 0 && (done_tags || cap == 0), "bad arguments");
+    Session& S = *static_cast<Session*>(session);
+    *n_done = 0;
+    std::vector<ShotRun*> ptrs;
+    for (auto& R : S.runs) ptrs.push_back(R.get());
+    if (S.dirty) {
+      upload_table(ptrs, S.table, S.dtable, S.st);
+      S.dirty = false;
+    }
+    auto any_done = [&] {
+      for (ShotRun* R : ptrs)
+        if (R->phase == 4) return true;
+      return false;
+    };
+    for (int k = 0; k < max_ticks && !any_done(); ++k) {
+      if (!batch_tick(ptrs, S.dtable.as<DevProp>(), S.st)) break;
+      ++S.ticks;
+    }
+    for (size_t i = 0; i < S.runs.size() && *n_done < cap;) {
+      if (S.runs[i]->phase != 4) {
+        ++i;
+        continue;
+      }
+      finish_run(*S.runs[i], S.st);
+      done_tags[(*n_done)++] = S.tags[i];
+      S.runs.erase(S.runs.begin() + (std::ptrdiff_t)i);
+      S.tags.erase(S.tags.begin() + (std::ptrdiff_t)i);
+      S.dirty = true;
+    }
+  });
+}
+
+int32_t ertm_session_active(void* session) {
+  return session ? (int32_t) static_cast<Session*>(session)->runs.size() : 0;
+}
+
+int64_t ertm_session_ticks(void* session) { return session ? static_cast<Session*>(session)->ticks : 0; }
+
+int32_t ertm_session_destroy(void* session) {
+  return guarded([&] {
+    if (!session) return;
+    std::unique_ptr<Session> S(static_cast<Session*>(session));
+    cudaStreamSynchronize(S->st);
+    S->runs.clear();
+    S->dtable = DevBuf();
+    CK(cudaStreamSynchronize(S->st));
+    CK(cudaStreamDestroy(S->st));
+  });
+}
+
 int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const double* num, const double* illum,
                          const double* rillum, int32_t by_illum, int32_t by_rillum, double eps, int32_t laplacian,
                          double lowpass, int32_t npml, int32_t top_mask, float* out, void* stream) {
@@ -1780,6 +1894,46 @@ int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int3
     k_stack_finish<<<g, 256, 0, st>>>(acc.as<double>(), n, n_images, o.as<float>());
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_stack_partial(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, double* sum,
+                           void* stream) {
+  return guarded([&] {
+    REQUIRE(n_images >= 0 && n >= 1 && (images || n_images == 0) && sum, "bad arguments");
+    require_device_pointer(sum, "sum");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DevBuf img, sc(4, st);
+    const unsigned g = (unsigned)((n + 255) / 256);
+    for (int k = 0; k < n_images; ++k) {
+      const float* src = images[k];
+      cudaPointerAttributes a{};
+      CK(cudaPointerGetAttributes(&a, src));
+      if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) {
+        if (!img.p) img = DevBuf(n * 4, st);
+        upload(img.p, src, n * 4, st);
+        src = img.as<float>();
+      }
+      CK(cudaMemsetAsync(sc.p, 0, 4, st));
+      if (normalize) k_absmax_f32<<<std::min<unsigned>(g, 1184), 256, 0, st>>>(src, n, sc.as<unsigned>());
+      k_stack_add<<<g, 256, 0, st>>>(src, n, sc.as<unsigned>(), normalize, sum);
+      g_launches += normalize ? 2 : 1;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_stack_finish(int64_t n, const double* sum, int64_t count, float* out, void* stream) {
+  return guarded([&] {
+    REQUIRE(n >= 1 && sum && out && count >= 1, "bad arguments");
+    require_device_pointer(sum, "sum");
+    require_device_pointer(out, "out");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_stack_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(sum, n, (int)count, out);
+    ++g_launches;
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
   });
 }

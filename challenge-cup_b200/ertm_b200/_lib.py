@@ -98,6 +98,14 @@ _SIGNATURES = {
                                 _I32, C.c_double, _I32, _I32, _P, _P]),
     "ertm_stack": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
     "ertm_stack_noalloc": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
+    "ertm_stack_partial": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
+    "ertm_session_create": (_I32, [C.POINTER(C.c_void_p)]),
+    "ertm_session_add": (_I32, [_P, C.POINTER(BatchShot), C.c_int64]),
+    "ertm_session_advance": (_I32, [_P, _I32, C.POINTER(C.c_int64), _I32, C.POINTER(C.c_int32)]),
+    "ertm_session_active": (_I32, [_P]),
+    "ertm_session_ticks": (C.c_int64, [_P]),
+    "ertm_session_destroy": (_I32, [_P]),
+    "ertm_stack_finish": (_I32, [C.c_int64, _P, C.c_int64, _P, _P]),
 }
 
 _lock = threading.Lock()

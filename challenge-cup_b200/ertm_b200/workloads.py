@@ -135,3 +135,60 @@ def visco_layered(seed: int = 0, n_shots: int = 64, nt: int | None = None, nx: i
 
 
 WORKLOADS = {"elastic4c": elastic_borehole_4c, "acoustic": acoustic_layered, "visco": visco_layered}
+
+
+def serving_jobs(seed: int = 0, n_jobs: int = 32, *, max_scale: tuple[float, float] = (16.0, 8.0),
+                 nt_range: tuple[int, int] = (1000, 8000), max_shots: int = 16):
+    """A stream of migration jobs of mixed engine, grid and length.
+
+    Engine uniform over acoustic / elastic / viscoacoustic; grid 256·u × 256·v
+    with u, v log-uniform in [1, max_scale] (the full range is 256×256 to
+    4096×2048); spacing 5–10 m; random layered vp 1500–4000 m/s with Gardner
+    density and layered Q 30–200; dt at the CFL limit (safety 0.5); length
+    uniform in nt_range; 1..max_shots surface shots with 10–30 Hz Ricker
+    wavelets; receivers every 4 cells at 2 cells depth.  Records are seeded
+    noise (the work of a shot does not depend on the record's values).
+    Returns ``ServeJob`` objects."""
+    from .config import ImagingConfig, QConfig, SolverConfig
+    from .imaging import RTMImager
+    from .serving import ServeJob
+    from .types import ShotRecord
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(n_jobs):
+        engine = ("acoustic", "elastic", "viscoacoustic")[int(rng.integers(0, 3))]
+        nx = int(round(256 * np.exp(rng.uniform(0.0, np.log(max_scale[0])))))
+        nz = int(round(256 * np.exp(rng.uniform(0.0, np.log(max_scale[1])))))
+        h = float(rng.integers(5, 11))
+        grid = GridSpec(nx=nx, nz=nz, dx=h, dz=h)
+        n_layers = int(rng.integers(3, 7))
+        tops = np.sort(rng.uniform(0.1, 0.95, n_layers - 1)) * nz * h
+        vps = np.sort(rng.uniform(1500.0, 4000.0, n_layers))
+        qs = np.round(np.exp(rng.uniform(np.log(30.0), np.log(200.0), n_layers)))
+        layer = np.searchsorted(tops, np.arange(nz) * h)
+        vp = vps[layer][:, None].repeat(nx, 1).astype(np.float32)
+        qp = qs[layer][:, None].repeat(nx, 1).astype(np.float32)
+        model = ElasticModel(grid=grid, vp=vp, vs=(vp / 1.8).astype(np.float32), rho=gardner(vp), qp=qp,
+                             qs=(qp * 0.5).astype(np.float32), name=f"serving-{j}")
+        dt = cfl_dt(float(vps.max()), h, h, 8, 0.5)
+        nt = int(rng.integers(nt_range[0], nt_range[1] + 1))
+        f0 = float(rng.uniform(10.0, 30.0))
+        boundary = "free" if engine == "elastic" else "cpml"
+        solver = SolverConfig(nt=nt, dt=dt, order=8, boundary=boundary, engine=engine)
+        q = QConfig(enabled=True, model="gsls", alpha_c=1.0, f_ref=f0, gain_budget_db=40.0, f_max=2.0 * f0,
+                    amplitude_cap=50.0, lowpass_interval=20, n_mechanisms=3) if engine == "viscoacoustic" else None
+        imaging = ImagingConfig(mode="pp", condition="normalized", separation="divcurl", checkpoint_mb=256.0)
+        imager = RTMImager(imaging, solver, q)
+        xr = np.arange(0, nx, 4) * h
+        receivers = ReceiverSpec(x=xr, z=np.full_like(xr, 2.0 * h), component="p")
+        comps = ("vz", "p") if engine == "elastic" else ("p",)
+        shots = []
+        for k in range(int(rng.integers(1, max_shots + 1))):
+            src = SourceSpec(x=float(rng.uniform(0.1, 0.9) * (nx - 1) * h), z=2.0 * h, f0=f0, delay=1.2 / f0)
+            data = {c: (rng.standard_normal((nt, len(xr))) * 1e-6).astype(np.float32) for c in comps}
+            shots.append(ShotRecord(data=data[comps[0]], dt=dt, t=np.arange(nt) * dt, receivers=receivers,
+                                    source=src, components=data))
+        modes = ("pp", "ps") if engine == "elastic" else ("pp",)
+        jobs.append(ServeJob(shots=shots, model=model, imager=imager, modes=modes,
+                             name=f"{engine} {nx}x{nz} nt={nt} shots={len(shots)}"))
+    return jobs

@@ -197,6 +197,23 @@ typedef struct ertm_batch_shot {
  * overlaps the backward pass over block b.  Shots may differ in grid, engine,
  * length and condition.  Results equal n_shots separate ertm_migrate calls. */
 int32_t ertm_migrate_batch(int32_t n_shots, const ertm_batch_shot* shots);
+
+/* Batch sessions: the tick loop of ertm_migrate_batch made resumable, for a
+ * serving loop (no single reference counterpart: it runs RTMImager.migrate,
+ * imaging.py:205-349, for shots that join and leave between ticks).
+ * ertm_session_add copies the shot's wavelet and record and prepares its
+ * checkpoints; the shot's num/illum/rillum outputs must stay valid until
+ * ertm_session_advance reports its tag done.  ertm_session_advance runs at
+ * most max_ticks ticks, stopping early after the tick in which a shot
+ * finishes, then writes the finished shots' accumulators and returns up to cap
+ * of their tags.  A shot's propagators belong to the session until then. */
+int32_t ertm_session_create(void** session);
+int32_t ertm_session_add(void* session, const ertm_batch_shot* shot, int64_t tag);
+int32_t ertm_session_advance(void* session, int32_t max_ticks, int64_t* done_tags, int32_t cap, int32_t* n_done);
+int32_t ertm_session_active(void* session);
+int64_t ertm_session_ticks(void* session);
+int32_t ertm_session_destroy(void* session);
+
 /* Normalisation and _postprocess (imaging.py:326-333, 476-502): image =
  * num/(illum+eps)/(rillum+eps) as selected, Laplacian, wavenumber low-pass
  * (lowpass < 1), PML mask of width npml (top too when top_mask). */
@@ -207,6 +224,18 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
 /* stack_images (pipeline.py:133-161): images is n_images pointers to (n,) float32. */
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream);
+
+/* pipeline.py:143-151 split in two so the sum can cross GPUs: the float64
+ * accumulation loop (per image: max|.| when normalize, divide, add in image
+ * order) and the final divide + cast.  ertm_stack_partial adds the images into
+ * sum (a caller-zeroed device array of n float64, kept across calls); images
+ * may be host or device pointers.  ertm_stack_finish writes
+ * out = float32(sum / count) (device arrays).  A one-image stack is the image
+ * itself in the reference, so callers pass normalize = 0 when the whole stack
+ * holds one image. */
+int32_t ertm_stack_partial(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, double* sum,
+                           void* stream);
+int32_t ertm_stack_finish(int64_t n, const double* sum, int64_t count, float* out, void* stream);
 
 /* No counterpart in the reference.  Same result as ertm_stack, but it
  * allocates nothing, for callers that cannot allocate device memory: a

@@ -156,3 +156,20 @@ def test_float64_wavefields_are_rejected():
                      qs=np.full(sh, 50.0, np.float32))
     with pytest.raises(SolverError):
         AcousticPropagator(m, PropagationSpec(dt=1e-3, nt=10, dtype="float64"))
+
+
+def test_serving_fails_loudly_without_a_device():
+    """No GPU: the serving loop fails every submitted job instead of running
+    anything on the host."""
+    import types as _t
+
+    from ertm_b200.serving import RTMServer, ServeJob, percentile
+    job = ServeJob(shots=[], model=_t.SimpleNamespace(), imager=_t.SimpleNamespace(
+        config=_t.SimpleNamespace(mode="pp")))
+    srv = RTMServer()
+    fut = srv.submit(job)
+    srv.start()
+    with pytest.raises(Exception):
+        fut.result(timeout=60)
+    srv.stop(timeout=60)
+    assert percentile([1.0, 2.0, 3.0, 4.0], 50) == 2.5 and percentile([], 99) is None
