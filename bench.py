@@ -185,20 +185,14 @@ def job_config(wl, args, world: int) -> dict:
 
 
 def imager_for(wl):
-    from ertm_b200 import ImagingConfig, QConfig, RTMImager, SolverConfig
-    solver = SolverConfig(nt=wl.nt, dt=wl.dt, order=8, boundary=wl.boundary, dtype="float32", engine=wl.engine,
-                          npml=wl.npml)
-    imaging = ImagingConfig(mode=wl.modes[0], condition=wl.condition, separation=wl.separation,
-                            checkpoint_mb=wl.checkpoint_mb)
-    q = QConfig(**wl.q) if wl.q else None
-    return RTMImager(imaging, solver, q), solver
+    from ertm_b200.workloads import imager_for as make
+    return make(wl)
 
 
 def synthesize(wl, solver, sources):
     """Shot records from the GPU forward model (untimed set-up)."""
-    from ertm_b200.solver import FiniteDifferenceSolver
-    fd = FiniteDifferenceSolver(solver)
-    return [fd.forward(wl.model, s, wl.receivers, components=wl.components) for s in sources]
+    from ertm_b200.workloads import synthesize as make
+    return make(wl, solver, sources)
 
 
 def step_bytes(prop) -> float:

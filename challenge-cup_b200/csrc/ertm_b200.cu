@@ -830,6 +830,7 @@ void launch_epilogue(const Prop& P, const Epilogue& E) {
 struct ShotRun {
   Prop* F = nullptr;
   Prop* B = nullptr;
+  cudaStream_t f_st0 = nullptr, b_st0 = nullptr;   // the propagators' streams before the run
   ertm_migrate_config cfg{};
   int fi = 0, bi = 0;          // indices of F and B in the launch's DevProp table
   int nt = 0, iv = 1, n_states = 0;
@@ -865,6 +866,8 @@ void prepare_run(ShotRun& R, Prop& F, Prop& B, const ertm_migrate_config& cfg, c
     REQUIRE((cfg.src_wave[k] == 0 || cfg.src_wave[k] == 1) && (cfg.rcv_wave[k] == 0 || cfg.rcv_wave[k] == 1) &&
                 (F.h.engine == ENGINE_ELASTIC || (cfg.src_wave[k] == 0 && cfg.rcv_wave[k] == 0)),
             "wave not available for this engine");
+  R.f_st0 = F.st;
+  R.b_st0 = B.st;
   for (Prop* P : {&F, &B})
     if (P->st != st) {
       CK(cudaStreamSynchronize(P->st));
@@ -1007,6 +1010,14 @@ void finish_run(ShotRun& R, cudaStream_t st) {
     if (R.out[2]) copy_out(R.out[2] + (size_t)k * npix, R.ril[k]);
   }
   CK(cudaStreamSynchronize(st));
+}
+
+// Hand the propagators back to the streams they had before the run (a
+// session's stream dies with the session; the propagators outlive it).
+void release_streams(ShotRun& R, cudaStream_t st) {
+  CK(cudaStreamSynchronize(st));
+  R.F->st = R.f_st0;
+  R.B->st = R.b_st0;
 }
 
 void inject_one(ShotRun& R, int t, cudaStream_t st) {
@@ -1796,6 +1807,7 @@ int32_t ertm_session_advance(void* session, int32_t max_ticks, int64_t* done_tag
         continue;
       }
       finish_run(*S.runs[i], S.st);
+      release_streams(*S.runs[i], S.st);
       done_tags[(*n_done)++] = S.tags[i];
       S.runs.erase(S.runs.begin() + (std::ptrdiff_t)i);
       S.tags.erase(S.tags.begin() + (std::ptrdiff_t)i);
@@ -1815,6 +1827,10 @@ int32_t ertm_session_destroy(void* session) {
     if (!session) return;
     std::unique_ptr<Session> S(static_cast<Session*>(session));
     cudaStreamSynchronize(S->st);
+    for (auto& R : S->runs) {
+      R->F->st = R->f_st0;
+      R->B->st = R->b_st0;
+    }
     S->runs.clear();
     S->dtable = DevBuf();
     CK(cudaStreamSynchronize(S->st));

@@ -1,0 +1,90 @@
+"""Profiling entry point: one benchmark workload's migration job, alone in
+the process, for ncu launch lists and kernel captures.
+
+    PYTHONPATH=challenge-cup_b200 python -m ertm_b200.profiling \\
+        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2]
+
+The job is what ``bench.py`` times: every shot of the workload migrated
+(batched lockstep ticks, or one shot at a time with ``--path plain``) and the
+images stacked.  Records come from the GPU forward model first.  Each repeat
+is preceded by a 256 MiB fill (the benchmark's L2 flush), which also marks the
+start of a repeat in a launch list.  Prints one JSON line: the launches of this
+library per repeat and the stencil profiler's per-tick time and bytes.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+
+import numpy as np
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(prog="python -m ertm_b200.profiling")
+    ap.add_argument("--config", default="elastic4c")
+    ap.add_argument("--nt", type=int, default=48)
+    ap.add_argument("--shots", type=int, default=None)
+    ap.add_argument("--path", choices=("batched", "plain"), default="batched")
+    ap.add_argument("--repeat", type=int, default=2)
+    args = ap.parse_args(argv)
+
+    import torch
+
+    from . import _lib, workloads
+    from .batch import migrate_device_batch
+    from .imaging import ShotMigrator
+    from .propagation import source_wavelet
+
+    L = _lib.lib(0)
+    wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt, **({"n_shots": args.shots} if args.shots else {}))
+    imager, solver = workloads.imager_for(wl)
+    shots = workloads.synthesize(wl, solver, wl.sources)
+    names = list(wl.components)
+    rec = [torch.from_numpy(np.stack([s.components[n] for n in names])).cuda() for s in shots]
+    wavelets = [source_wavelet(s, wl.dt, wl.nt) for s in wl.sources]
+    g = wl.model.grid
+    npix = g.nx * g.nz
+    n = len(wl.sources)
+    migs = [ShotMigrator(imager, wl.model) for _ in range(n if args.path == "batched" else 1)]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    partial = torch.zeros((len(wl.modes), g.nz, g.nx), dtype=torch.float64, device="cuda")
+    out = torch.empty((len(wl.modes), g.nz, g.nx), dtype=torch.float32, device="cuda")
+
+    def job():
+        if args.path == "batched":
+            imgs = migrate_device_batch(imager, migs, wl.sources, [wl.receivers] * n, rec, names, wavelets,
+                                        modes=wl.modes)
+        else:
+            imgs = [migs[0].migrate_device(s, wl.receivers, rec[i], names, wavelets[i], modes=wl.modes)
+                    for i, s in enumerate(wl.sources)]
+        partial.zero_()
+        for k in range(len(wl.modes)):
+            ptrs = (C.c_void_p * n)(*[im[k].data_ptr() for im in imgs])
+            _lib.check(L.ertm_stack_partial(n, npix, C.cast(ptrs, C.c_void_p), int(n > 1), partial[k].data_ptr(),
+                                            None), "stack partial")
+            _lib.check(L.ertm_stack_finish(npix, partial[k].data_ptr(), n, out[k].data_ptr(), None), "stack finish")
+
+    launches = []
+    _lib.check(L.ertm_profile_stencil(1, 1), "profile")
+    for _ in range(args.repeat):
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        before = L.ertm_launch_count()
+        job()
+        torch.cuda.synchronize()
+        launches.append(int(L.ertm_launch_count() - before))
+    tot, cnt, byt = C.c_double(), C.c_int64(), C.c_double()
+    _lib.check(L.ertm_profile_read(C.byref(tot), C.byref(cnt), C.byref(byt)), "profile read")
+    _lib.check(L.ertm_profile_stencil(0, 1), "profile off")
+    ticks = max(int(cnt.value), 1)
+    print(json.dumps({"workload": wl.name, "path": args.path, "nt": wl.nt, "shots": n, "launches_per_repeat": launches,
+                      "stencil_us_per_tick": tot.value / ticks * 1e3, "bytes_per_tick": byt.value / ticks,
+                      "timed_ticks": int(cnt.value),
+                      "achieved_gbs": byt.value / (tot.value * 1e-3) / 1e9 if tot.value > 0 else None,
+                      "checksum": float(out.double().abs().sum().item())}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

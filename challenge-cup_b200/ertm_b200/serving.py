@@ -89,12 +89,11 @@ def shot_footprint_bound(model: Any, imager: RTMImager, n_steps: int, n_modes: i
     L = int(imager.q_config.n_mechanisms) if engine == "viscoacoustic" else 0
     n_fields = {"acoustic": 3, "elastic": 5}.get(engine, 4 + L)
     n_psi = 8 if engine == "elastic" else 4
-    n_coef = {"acoustic": 3, "elastic": 5}.get(engine, 4 + 2 * L)
     nzp, nxp = g.nz + 10, g.nx + 10
     ld = (nxp + 31) // 32 * 32
     fe = nzp * ld
     state = (n_fields + n_psi) * fe * 4
-    prop = state + (n_coef + 1) * fe * 4
+    prop = state + 12 * fe * 4          # coefficient block, Q index and profiles: at most 12 arrays
     field_bytes = n_fields * nzp * nxp * 4
     iv = checkpoint_interval(n_steps, field_bytes, float(imager.config.checkpoint_mb))
     n_states = (n_steps + iv - 1) // iv

@@ -137,6 +137,73 @@ def visco_layered(seed: int = 0, n_shots: int = 64, nt: int | None = None, nx: i
 WORKLOADS = {"elastic4c": elastic_borehole_4c, "acoustic": acoustic_layered, "visco": visco_layered}
 
 
+UNEVEN_GRIDS = ((501, 301), (1001, 501), (1601, 801), (2401, 1201))
+
+
+def uneven_batch(seed: int = 0, n_shots: int = 256, *, h: float = 10.0) -> list[Workload]:
+    """Uneven batch: one single-shot workload per shot.
+
+    Engine uniform over acoustic / elastic; the model one of four seeded
+    random-layer models with an anomaly (501×301, 1001×501, 1601×801,
+    2401×1201 at 10 m); dt at the CFL limit (safety 0.5); nt uniform in
+    1500–6000; 10–30 Hz Ricker; normalized condition (the batch is run with
+    Kahan-compensated float32 accumulation)."""
+    rng = np.random.default_rng(seed)
+    models = []
+    for k, (nx, nz) in enumerate(UNEVEN_GRIDS):
+        grid = GridSpec(nx=nx, nz=nz, dx=h, dz=h)
+        n_layers = int(rng.integers(4, 9))
+        tops = np.sort(rng.uniform(0.05, 0.95, n_layers - 1)) * nz * h
+        vps = np.sort(rng.uniform(1800.0, 4200.0, n_layers))
+        layer = np.searchsorted(tops, np.arange(nz) * h)
+        vp = vps[layer][:, None].repeat(nx, 1)
+        # anomaly: an elliptic body 15 % faster or slower than its layer
+        cx, cz = rng.uniform(0.3, 0.7) * nx * h, rng.uniform(0.4, 0.8) * nz * h
+        ax, az = rng.uniform(0.05, 0.15) * nx * h, rng.uniform(0.03, 0.08) * nz * h
+        xx, zz = np.meshgrid(np.arange(nx) * h, np.arange(nz) * h)
+        body = ((xx - cx) / ax) ** 2 + ((zz - cz) / az) ** 2 <= 1.0
+        vp = np.where(body, vp * (1.15 if rng.uniform() < 0.5 else 0.85), vp).astype(np.float32)
+        models.append(ElasticModel(grid=grid, vp=vp, vs=(vp / 1.8).astype(np.float32), rho=gardner(vp),
+                                   qp=np.full(grid.shape, 100.0, np.float32), qs=np.full(grid.shape, 50.0, np.float32),
+                                   name=f"uneven-{nx}x{nz}"))
+    out = []
+    for i in range(n_shots):
+        engine = ("acoustic", "elastic")[int(rng.integers(0, 2))]
+        m = models[int(rng.integers(0, len(models)))]
+        g = m.grid
+        nt = int(rng.integers(1500, 6001))
+        f0 = float(rng.uniform(10.0, 30.0))
+        dt = cfl_dt(float(m.vp.max()), g.dx, g.dz, 8, 0.5)
+        src = SourceSpec(x=float(rng.uniform(0.05, 0.95) * (g.nx - 1) * h), z=2.0 * h, f0=f0, delay=1.2 / f0)
+        xr = np.arange(0, g.nx, 4) * h
+        rec = ReceiverSpec(x=xr, z=np.full_like(xr, 2.0 * h), component="p")
+        boundary = "free" if engine == "elastic" else "cpml"
+        comps = ("vz", "p") if engine == "elastic" else ("p",)
+        modes = ("pp", "ps") if engine == "elastic" else ("pp",)
+        out.append(Workload(f"uneven shot {i}: {engine} {g.nx}x{g.nz} nt={nt}", engine, m, [src], rec, dt, nt, boundary,
+                            20, "normalized", separation="divcurl", modes=modes, components=comps,
+                            checkpoint_mb=256.0))
+    return out
+
+def imager_for(wl: Workload):
+    """The RTMImager (and its SolverConfig) a workload is migrated with."""
+    from .config import ImagingConfig, QConfig, SolverConfig
+    from .imaging import RTMImager
+    solver = SolverConfig(nt=wl.nt, dt=wl.dt, order=8, boundary=wl.boundary, dtype="float32", engine=wl.engine,
+                          npml=wl.npml)
+    imaging = ImagingConfig(mode=wl.modes[0], condition=wl.condition, separation=wl.separation,
+                            checkpoint_mb=wl.checkpoint_mb)
+    q = QConfig(**wl.q) if wl.q else None
+    return RTMImager(imaging, solver, q), solver
+
+
+def synthesize(wl: Workload, solver, sources):
+    """Shot records of ``sources`` from the GPU forward model."""
+    from .solver import FiniteDifferenceSolver
+    fd = FiniteDifferenceSolver(solver)
+    return [fd.forward(wl.model, s, wl.receivers, components=wl.components) for s in sources]
+
+
 def serving_jobs(seed: int = 0, n_jobs: int = 32, *, max_scale: tuple[float, float] = (16.0, 8.0),
                  nt_range: tuple[int, int] = (1000, 8000), max_shots: int = 16):
     """A stream of migration jobs of mixed engine, grid and length.

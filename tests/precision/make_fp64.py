@@ -1,0 +1,126 @@
+"""FP64 oracle images for the precision study (imaging in float32 wavefields
+on the device against float64 wavefields on the host).
+
+Runs on the CPU, with the oracle.  For a few seeded shots of each benchmark
+configuration it
+
+* synthesises the shot record with the oracle's float32 forward model (the
+  device forward model reproduces it bit for bit for the acoustic and elastic
+  engines, and to float32 rounding for the viscoacoustic one);
+* migrates it with the oracle in float64 wavefields (the reference's float64
+  mode: CPML coefficients and ψ memories stay float32, propagation.py
+  ``dtype="float64"``), imaging and post-processing as the path does;
+* stores the images every ``step``-th pixel in both axes as float32.
+
+Output: tests/precision/<config>.npz.  The device side of the comparison is
+tests/test_gpu_precision.py.
+
+    python tests/precision/make_fp64.py [config ...]     # acoustic elastic4c visco uneven
+"""
+
+from __future__ import annotations
+
+import json
+import multiprocessing as mp
+import sys
+import time
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+
+# (config, shot indices, decimation step, stack the shots)
+CASES = {
+    "acoustic": ([0, 1, 2], 2, True),
+    "elastic4c": ([0, 5], 4, False),
+    "visco": ([10, 40], 8, False),
+    "uneven": ([1, 4], 4, False),
+}
+
+
+def _paths() -> None:
+    for p in (str(ROOT), str(ROOT / "challenge-cup_b200")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+
+
+def case_workloads(config: str):
+    """The single-shot workloads of one configuration's study (also used by
+    the device test, so both sides see the same seeded inputs)."""
+    _paths()
+    from ertm_b200 import workloads
+    shots, _, _ = CASES[config]
+    if config == "uneven":
+        batch = workloads.uneven_batch(0, 8)
+        return [batch[i] for i in shots]
+    wl = workloads.WORKLOADS[config](seed=0)
+    out = []
+    for i in shots:
+        one = workloads.Workload(**{**wl.__dict__, "sources": [wl.sources[i]]})
+        out.append(one)
+    return out
+
+
+def _oracle_q(qcfg, compensation: bool):
+    return SimpleNamespace(enabled=True, f_ref=float(qcfg.f_ref), n_mechanisms=int(qcfg.n_mechanisms),
+                           band_ratio=float(qcfg.band_ratio), compensation=bool(compensation),
+                           alpha_c=float(qcfg.alpha_c), amplitude_cap=float(qcfg.amplitude_cap),
+                           lowpass_interval=int(qcfg.lowpass_interval),
+                           f_max=None if qcfg.f_max is None else float(qcfg.f_max),
+                           gain_budget_db=float(qcfg.gain_budget_db))
+
+
+def run_shot(args) -> dict:
+    config, k = args
+    _paths()
+    import oracle as orc
+    from ertm_b200 import workloads
+    wl = case_workloads(config)[k]
+    imager, solver = workloads.imager_for(wl)
+    t0 = time.perf_counter()
+    spec = orc.Spec(dt=wl.dt, nt=wl.nt, order=8, npml=wl.npml, dtype="float32", boundary=wl.boundary)
+    q_fwd = _oracle_q(imager.q_config, False) if wl.engine == "viscoacoustic" else None
+    record = orc.run_forward(wl.model, wl.sources[0], wl.receivers, spec, engine=wl.engine,
+                             components=list(wl.components), q=q_fwd)
+    t1 = time.perf_counter()
+    sv = SimpleNamespace(dt=wl.dt, nt=wl.nt, order=8, boundary=wl.boundary, dtype="float64", engine=wl.engine,
+                         npml=wl.npml)
+    q = _oracle_q(imager.q_config, bool(imager.q_config.enabled)) if wl.engine == "viscoacoustic" else None
+    images = {}
+    for m in wl.modes:
+        im = SimpleNamespace(**{**imager.config.__dict__, "mode": m})
+        images[m] = np.asarray(orc.migrate(record, wl.dt, wl.sources[0], wl.receivers, wl.model, sv, im, q),
+                               dtype=np.float64)
+    return {"config": config, "k": k, "images": images, "forward_s": t1 - t0,
+            "migrate_s": time.perf_counter() - t1}
+
+
+def main(configs) -> None:
+    _paths()
+    import oracle as orc
+    tasks = [(c, k) for c in configs for k in range(len(CASES[c][0]))]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(len(tasks), mp.cpu_count())) as pool:
+        results = pool.map(run_shot, tasks, chunksize=1)
+    for c in configs:
+        shots, step, stack = CASES[c]
+        rs = sorted((r for r in results if r["config"] == c), key=lambda r: r["k"])
+        modes = list(rs[0]["images"])
+        out, meta = {}, {"shots": shots, "step": step, "stacked": stack, "modes": modes,
+                         "forward_s": [r["forward_s"] for r in rs], "migrate_s": [r["migrate_s"] for r in rs]}
+        for m in modes:
+            imgs = [r["images"][m] for r in rs]
+            if stack:
+                out[m] = orc.stack_images(imgs, normalize=True)[::step, ::step].astype(np.float32)
+            else:
+                for k, im in enumerate(imgs):
+                    out[f"{m}_{k}"] = im[::step, ::step].astype(np.float32)
+        np.savez_compressed(HERE / f"{c}.npz", meta=json.dumps(meta), **out)
+        print(c, json.dumps(meta), flush=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or list(CASES))
