@@ -1,0 +1,55 @@
+"""Form (a): the device images (float32 wavefields; float64 or
+Kahan-compensated float32 imaging sums) against images of the oracle run in
+float64 wavefields, on seeded shots of each benchmark configuration.
+
+The float64 images are committed under tests/precision/ (made on the CPU by
+tests/precision/make_fp64.py, every ``step``-th pixel); the device computes
+the same shots from the same seeded inputs here.  Bound: relative L2 ≤ 1e-4.
+"""
+
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+
+PREC = Path(__file__).resolve().parent / "precision"
+sys.path.insert(0, str(PREC))
+from make_fp64 import CASES, case_workloads  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+CONFIGS = [c for c in CASES if (PREC / f"{c}.npz").exists()]
+
+
+@pytest.mark.parametrize("accumulation", ["fp64", "kahan"])
+@pytest.mark.parametrize("config", CONFIGS)
+def test_image_error_against_fp64_oracle(config, accumulation):
+    from ertm_b200 import RTMImager, workloads
+    from ertm_b200.stacking import stack_images
+    with np.load(PREC / f"{config}.npz") as z:
+        fx = {k: z[k] for k in z.files}
+    meta = json.loads(str(fx["meta"]))
+    step = int(meta["step"])
+    per_mode: dict[str, list] = {}
+    for wl in case_workloads(config):
+        base, solver = workloads.imager_for(wl)
+        imager = RTMImager(base.config, solver, base.q_config, accumulation=accumulation)
+        record = workloads.synthesize(wl, solver, wl.sources)[0]
+        for res in imager.migrate_modes(record, wl.model, modes=wl.modes):
+            per_mode.setdefault(res.mode, []).append(res)
+    errors = {}
+    for m, results in per_mode.items():
+        if meta["stacked"]:
+            img = stack_images(results).image[::step, ::step]
+            errors[m] = rel_l2(img, fx[m])
+        else:
+            for k, r in enumerate(results):
+                errors[f"{m}_{k}"] = rel_l2(r.image[::step, ::step], fx[f"{m}_{k}"])
+    print(f"\nprecision {config} {accumulation}: " + json.dumps(errors))
+    assert max(errors.values()) <= TOL, errors
