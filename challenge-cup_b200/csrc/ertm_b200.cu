@@ -1752,10 +1752,12 @@ int32_t ertm_migrate_batch(int32_t n_shots, const ertm_batch_shot* shots) {
 int32_t ertm_session_create(void** out) {
   return guarded([&] {
     REQUIRE(out, "bad arguments");
+    // The session works on the legacy default stream: work the caller queued
+    // there (inputs, output buffers) is ordered before its ticks, and buffers
+    // the session creates inside a propagator (injection and sampling plans)
+    // are freed on a stream that outlives the session.
     auto S = std::make_unique<Session>();
-    // a blocking stream: work the caller queued on the legacy default stream
-    // (inputs, output buffers) is ordered before the session's ticks
-    CK(cudaStreamCreate(&S->st));
+    S->st = nullptr;
     *out = S.release();
   });
 }
@@ -1834,7 +1836,6 @@ int32_t ertm_session_destroy(void* session) {
     S->runs.clear();
     S->dtable = DevBuf();
     CK(cudaStreamSynchronize(S->st));
-    CK(cudaStreamDestroy(S->st));
   });
 }
 
