@@ -150,7 +150,7 @@ def measured_hbm_peak() -> tuple[float, str]:
 
 
 def committed_traffic(name: str) -> float | None:
-    """Per-launch DRAM bytes from the committed ncu summary, if one exists."""
+    """DRAM bytes per algorithmic byte of a tick, from the committed ncu summary."""
     p = ROOT / "profiles" / f"{name}.traffic"
     try:
         return float(p.read_text().split()[0])
@@ -489,7 +489,10 @@ def run_ours(args, dist: Dist) -> None:
         "batched_equals_plain": same,
         "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": committed_traffic(f"{wl.engine}_step"),
+                     "traffic": (None if committed_traffic(f"{wl.engine}_step") is None else
+                                 committed_traffic(f"{wl.engine}_step") * float(byt.value) / max(int(cnt.value), 1)),
+                     "traffic_note": "DRAM bytes per tick: the ncu-measured DRAM/algorithmic ratio of a captured "
+                                     "16-step tick (profiles/) times this run's algorithmic bytes per tick",
                      "kernel": f"{wl.engine} velocity + stress launches of a batched tick (imaging epilogue fused)",
                      "bytes_definition": "per propagator step: Npad*(8*n_state + 4*n_coef) + 8*CPML strip cells*terms;"
                                          " per fused imaging epilogue: 16 B per accumulator, 4 B per replayed field",
