@@ -178,6 +178,22 @@ __device__ __forceinline__ void run_epilogue(const Epilogue& E, size_t c, size_t
   }
 }
 
+// The epilogue of one tile: the stress phase leaves P and S of its cells in
+// shared memory (TZ rows × 32 columns); the block then walks the tile one cell
+// per thread, so a warp covers 32 consecutive physical cells of a row and its
+// accumulator, replay and excitation accesses coalesce whatever their
+// alignment.  One copy of the epilogue code serves every cell.
+template <int TZ, int NT, class GEO>
+__device__ __forceinline__ void epilogue_tile(const Epilogue& E, const GEO& G, int i0, int j0, const float* e_p,
+                                              const float* e_s, size_t npix) {
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll 1
+  for (int idx = tid; idx < TZ * 32; idx += NT) {
+    size_t pc;
+    if (G.physical(i0 + (idx >> 5), j0 + (idx & 31), pc)) run_epilogue(E, pc, npix, e_p[idx], e_s ? e_s[idx] : 0.f);
+  }
+}
+
 // Scalars and pointers of one propagator, loaded once into registers at the
 // top of a kernel (the kernels store through float pointers, so reading the
 // DevProp in global memory after a store would force a reload).
@@ -341,7 +357,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   __syncthreads();
   if (j >= G.nxp) return;
   if (G.interior(L.i0, L.j0, TZ)) {
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
       const float* row = sp + (rr + M) * T::W + 4 * threadIdx.x;
@@ -364,7 +380,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
     return;
   }
   const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
-#pragma unroll
+#pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const int rr = threadIdx.y + BZ * r;
     const int i = L.i0 + rr;
@@ -439,7 +455,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   __syncthreads();
   if (j >= G.nxp) return;
   if (G.interior(L.i0, L.j0, TZ)) {
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
       const int ro = (rr + M) * T::W + 4 * threadIdx.x;
@@ -468,7 +484,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
     return;
   }
   const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
-#pragma unroll
+#pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const int rr = threadIdx.y + BZ * r;
     const int i = L.i0 + rr;
@@ -583,6 +599,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   stage<M, TZ, XT * BZ>(svx, P.f[A_VX], G.nzp, G.ld, L.i0, L.j0);
   stage<M, TZ, XT * BZ>(svz, P.f[A_VZ], G.nzp, G.ld, L.i0, L.j0);
   __shared__ __align__(16) float c_a[TZ * 32], c_b[TZ * 32];   // acoustic: p, κ; viscoacoustic: ε, K_R
+  __shared__ __align__(16) float e_p[TZ * 32];                  // P for the epilogue
   stage_cells<TZ, XT * BZ>(c_a, VISCO ? eps : p, G.nzp, G.ld, L.i0, L.j0);
   stage_cells<TZ, XT * BZ>(c_b, cA, G.nzp, G.ld, L.i0, L.j0);
   cp_async_commit();
@@ -595,7 +612,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   const size_t npix = (size_t)G.nz * G.nx;
   float peak = 0.f;
   if (jok && G.interior(L.i0, L.j0, TZ)) {
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
       const int i = L.i0 + rr;
@@ -631,15 +648,11 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
       }
       st4(p + g, out);
       if constexpr (VISCO) st4(eps + g, epsv);
-      if (w.epi.kind != EPI_NONE) {
-        const size_t pc = (size_t)(i - G.pad) * G.nx + (j - G.pad);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) run_epilogue(w.epi, pc + c, npix, comp(out, c), 0.f);
-      }
+      if (w.epi.kind != EPI_NONE) st4(e_p + rr * 32 + 4 * threadIdx.x, out);
     }
   } else if (jok) {
     const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
       const int i = L.i0 + rr;
@@ -703,12 +716,15 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
           peak = fmaxf(peak, fabsf(pv));
         }
         set_comp(out, c, pv);
-        size_t pc;
-        if (w.epi.kind != EPI_NONE && G.physical(i, jc, pc)) run_epilogue(w.epi, pc, npix, pv, 0.f);
       }
       st4(p + g, out);
       if constexpr (VISCO) st4(eps + g, epsv);
+      if (w.epi.kind != EPI_NONE) st4(e_p + rr * 32 + 4 * threadIdx.x, out);
     }
+  }
+  if (w.epi.kind != EPI_NONE) {
+    __syncthreads();
+    epilogue_tile<TZ, XT * BZ>(w.epi, G, L.i0, L.j0, e_p, nullptr, npix);
   }
   if constexpr (VISCO) {
     if (w.flags & STEP_PEAK) block_max_to(peak, P.peak);
@@ -745,6 +761,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   stage<M, TZ, XT * BZ>(svz, P.f[E_VZ], G.nzp, G.ld, L.i0, L.j0);
   __shared__ __align__(16) float c_xx[TZ * 32], c_zz[TZ * 32], c_xz[TZ * 32], c_lam[TZ * 32], c_l2m[TZ * 32],
       c_mu[TZ * 32];
+  __shared__ __align__(16) float e_p[TZ * 32], e_s[TZ * 32];   // P and S for the epilogue
   stage_cells<TZ, XT * BZ>(c_xx, sxx, G.nzp, G.ld, L.i0, L.j0);
   stage_cells<TZ, XT * BZ>(c_zz, szz, G.nzp, G.ld, L.i0, L.j0);
   stage_cells<TZ, XT * BZ>(c_xz, sxz, G.nzp, G.ld, L.i0, L.j0);
@@ -757,12 +774,12 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   source_amps(w, P, amp, amp_eps);
   cp_async_wait_all();
   __syncthreads();
-  if (j >= G.nxp) return;
   const size_t npix = (size_t)G.nz * G.nx;
   const Epilogue& E = w.epi;
-  if (G.interior(L.i0, L.j0, TZ)) {
-    const bool want_curl = E.kind != EPI_NONE && E.sep == 1 && E.need_s;
-#pragma unroll
+  const bool epi = E.kind != EPI_NONE;
+  const bool want_curl = epi && E.sep == 1 && E.need_s;
+  if (j < G.nxp && G.interior(L.i0, L.j0, TZ)) {
+#pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
       const int i = L.i0 + rr;
@@ -801,114 +818,117 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
       st4(sxx + g, oxx);
       st4(szz + g, ozz);
       st4(sxz + g, oxz);
-      if (E.kind != EPI_NONE) {
-        const size_t pc = (size_t)(i - G.pad) * G.nx + (j - G.pad);
+      if (epi) {
+        float4 pv4, sv4;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          float pv, sv = 0.f;
           if (E.sep == 0) {
-            pv = fmul(0.5f, fadd(comp(oxx, c), comp(ozz, c)));
-            sv = comp(oxz, c);
+            set_comp(pv4, c, fmul(0.5f, fadd(comp(oxx, c), comp(ozz, c))));
+            set_comp(sv4, c, comp(oxz, c));
           } else {
-            pv = fadd(exx[c], ezz[c]);
-            if (want_curl) sv = fsub(ca[c], cb[c]);
+            set_comp(pv4, c, fadd(exx[c], ezz[c]));
+            set_comp(sv4, c, want_curl ? fsub(ca[c], cb[c]) : 0.f);
           }
-          run_epilogue(E, pc + c, npix, pv, sv);
         }
+        st4(e_p + rr * 32 + 4 * threadIdx.x, pv4);
+        st4(e_s + rr * 32 + 4 * threadIdx.x, sv4);
       }
     }
-    return;
-  }
-  const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
+  } else if (j < G.nxp) {
+    const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      const int rr = threadIdx.y + BZ * r;
+      const int i = L.i0 + rr;
+      if (i >= G.nzp) break;
+      const int ro = (rr + M) * T::W + 4 * threadIdx.x;
+      const size_t g = (size_t)i * G.ld + j;
+      const bool zin = (i >= M && i < G.nzp - M);
+      const int sz = G.sz(i);
+      const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+      float exx[4], ezz[4], f1[4], f2[4], curl_a[4], curl_b[4];
+      {
+        float v[12];
+        row12(svx + ro, v);        // vx along x: D⁻ (εxx)
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int rr = threadIdx.y + BZ * r;
-    const int i = L.i0 + rr;
-    if (i >= G.nzp) break;
-    const int ro = (rr + M) * T::W + 4 * threadIdx.x;
-    const size_t g = (size_t)i * G.ld + j;
-    const bool zin = (i >= M && i < G.nzp - M);
-    const int sz = G.sz(i);
-    const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
-    const bool want_curl = E.kind != EPI_NONE && E.sep == 1 && E.need_s;
-    float exx[4], ezz[4], f1[4], f2[4], curl_a[4], curl_b[4];
-    {
-      float v[12];
-      row12(svx + ro, v);        // vx along x: D⁻ (εxx)
+        for (int c = 0; c < 4; ++c) exx[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+        row12(svz + ro, v);        // vz along x: D⁺ (σxz) and D⁻ (curl)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) exx[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
-      row12(svz + ro, v);        // vz along x: D⁺ (σxz) and D⁻ (curl)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        f2[c] = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
-        curl_b[c] = want_curl ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
-      }
-      float z[4][2 * M + 1];
-      col9<M>(svx + ro + 4, z);  // vx along z: D⁺ (σxz) and D⁻ (curl)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        f1[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
-        curl_a[c] = want_curl ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
-      }
-      col9<M>(svz + ro + 4, z);  // vz along z: D⁻ (εzz)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) ezz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
-    }
-    float4 oxx = CELL(c_xx, rr), ozz = CELL(c_zz, rr), oxz = CELL(c_xz, rr);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (!C.ok[c]) continue;
-      const int jc = j + c;
-      const float exx_raw = exx[c], ezz_raw = ezz[c];
-      float ex = exx_raw, ez = ezz_raw, g1 = f1[c], g2 = f2[c];
-      if (C.sx[c] >= 0) {
-        float* p0 = psx2 + (size_t)i * G.wx + C.sx[c];
-        float psi = *p0; ex = cpml(ex, psi, C.ax[c], C.bx[c]); *p0 = psi;
-        float* p1 = psx3 + (size_t)i * G.wx + C.sx[c];
-        psi = *p1; g2 = cpml(g2, psi, C.ax[c], C.bx[c]); *p1 = psi;
-      }
-      if (sz >= 0) {
-        float* p0 = psz2 + (size_t)sz * G.ld + jc;
-        float psi = *p0; ez = cpml(ez, psi, azi, bzi); *p0 = psi;
-        float* p1 = psz3 + (size_t)sz * G.ld + jc;
-        psi = *p1; g1 = cpml(g1, psi, azi, bzi); *p1 = psi;
-      }
-      const float lam = comp(CELL(c_lam, rr), c), l2m = comp(CELL(c_l2m, rr), c);
-      float vxx = fadd(comp(CELL(c_xx, rr), c), fmul(G.dt, fadd(fmul(l2m, ex), fmul(lam, ez))));
-      float vzz = fadd(comp(CELL(c_zz, rr), c), fmul(G.dt, fadd(fmul(lam, ex), fmul(l2m, ez))));
-      float vxz = fadd(comp(CELL(c_xz, rr), c), fmul(fmul(G.dt, comp(CELL(c_mu, rr), c)), fadd(g1, g2)));
-      if (i == G.src_iz && jc == G.src_ix && amp != 0.f) {
-        if (mech == MECH_SHEAR) {
-          vxz = fadd(vxz, amp);
-        } else if (mech == MECH_EXPLOSIVE) {
-          vxx = fadd(vxx, amp);
-          vzz = fadd(vzz, amp);
+        for (int c = 0; c < 4; ++c) {
+          f2[c] = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+          curl_b[c] = want_curl ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
         }
-        // force_z adds to vz after this launch (other blocks still read vz here).
+        float z[4][2 * M + 1];
+        col9<M>(svx + ro + 4, z);  // vx along z: D⁺ (σxz) and D⁻ (curl)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          f1[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
+          curl_a[c] = want_curl ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
+        }
+        col9<M>(svz + ro + 4, z);  // vz along z: D⁻ (εzz)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ezz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
       }
-      if (G.free_surface && i == G.pad) {
-        vzz = 0.f;
-        vxz = 0.f;
-      }
-      set_comp(oxx, c, vxx);
-      set_comp(ozz, c, vzz);
-      set_comp(oxz, c, vxz);
-      size_t pc;
-      if (E.kind != EPI_NONE && G.physical(i, jc, pc)) {
-        float pv, sv = 0.f;
+      float4 oxx = CELL(c_xx, rr), ozz = CELL(c_zz, rr), oxz = CELL(c_xz, rr);
+      float4 pv4 = make_float4(0.f, 0.f, 0.f, 0.f), sv4 = pv4;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (!C.ok[c]) continue;
+        const int jc = j + c;
+        const float exx_raw = exx[c], ezz_raw = ezz[c];
+        float ex = exx_raw, ez = ezz_raw, g1 = f1[c], g2 = f2[c];
+        if (C.sx[c] >= 0) {
+          float* p0 = psx2 + (size_t)i * G.wx + C.sx[c];
+          float psi = *p0; ex = cpml(ex, psi, C.ax[c], C.bx[c]); *p0 = psi;
+          float* p1 = psx3 + (size_t)i * G.wx + C.sx[c];
+          psi = *p1; g2 = cpml(g2, psi, C.ax[c], C.bx[c]); *p1 = psi;
+        }
+        if (sz >= 0) {
+          float* p0 = psz2 + (size_t)sz * G.ld + jc;
+          float psi = *p0; ez = cpml(ez, psi, azi, bzi); *p0 = psi;
+          float* p1 = psz3 + (size_t)sz * G.ld + jc;
+          psi = *p1; g1 = cpml(g1, psi, azi, bzi); *p1 = psi;
+        }
+        const float lam = comp(CELL(c_lam, rr), c), l2m = comp(CELL(c_l2m, rr), c);
+        float vxx = fadd(comp(CELL(c_xx, rr), c), fmul(G.dt, fadd(fmul(l2m, ex), fmul(lam, ez))));
+        float vzz = fadd(comp(CELL(c_zz, rr), c), fmul(G.dt, fadd(fmul(lam, ex), fmul(l2m, ez))));
+        float vxz = fadd(comp(CELL(c_xz, rr), c), fmul(fmul(G.dt, comp(CELL(c_mu, rr), c)), fadd(g1, g2)));
+        if (i == G.src_iz && jc == G.src_ix && amp != 0.f) {
+          if (mech == MECH_SHEAR) {
+            vxz = fadd(vxz, amp);
+          } else if (mech == MECH_EXPLOSIVE) {
+            vxx = fadd(vxx, amp);
+            vzz = fadd(vzz, amp);
+          }
+          // force_z adds to vz after this launch (other blocks still read vz here).
+        }
+        if (G.free_surface && i == G.pad) {
+          vzz = 0.f;
+          vxz = 0.f;
+        }
+        set_comp(oxx, c, vxx);
+        set_comp(ozz, c, vzz);
+        set_comp(oxz, c, vxz);
         if (E.sep == 0) {
-          pv = fmul(0.5f, fadd(vxx, vzz));
-          sv = vxz;
+          set_comp(pv4, c, fmul(0.5f, fadd(vxx, vzz)));
+          set_comp(sv4, c, vxz);
         } else {
-          pv = fadd(exx_raw, ezz_raw);
-          if (E.need_s) sv = fsub(curl_a[c], curl_b[c]);
+          set_comp(pv4, c, fadd(exx_raw, ezz_raw));
+          set_comp(sv4, c, E.need_s ? fsub(curl_a[c], curl_b[c]) : 0.f);
         }
-        run_epilogue(E, pc, npix, pv, sv);
+      }
+      st4(sxx + g, oxx);
+      st4(szz + g, ozz);
+      st4(sxz + g, oxz);
+      if (epi) {
+        st4(e_p + rr * 32 + 4 * threadIdx.x, pv4);
+        st4(e_s + rr * 32 + 4 * threadIdx.x, sv4);
       }
     }
-    st4(sxx + g, oxx);
-    st4(szz + g, ozz);
-    st4(sxz + g, oxz);
+  }
+  if (epi) {
+    __syncthreads();
+    epilogue_tile<TZ, XT * BZ>(E, G, L.i0, L.j0, e_p, e_s, npix);
   }
 }
 

@@ -8,6 +8,7 @@ or a B200 is missing, every call raises ``SolverError``.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
@@ -15,7 +16,9 @@ import numpy as np
 
 from .exceptions import SolverError
 
-LIB_PATH = Path(__file__).resolve().parent / "libertm_b200.so"
+# ERTM_B200_LIBRARY selects another build of the library (e.g. one compiled
+# with different tile options); the default is the in-tree build.
+LIB_PATH = Path(os.environ.get("ERTM_B200_LIBRARY") or Path(__file__).resolve().parent / "libertm_b200.so")
 
 ENGINE = {"acoustic": 0, "elastic": 1, "viscoacoustic": 2}
 COMP = {"p": 0, "vx": 1, "vz": 2, "sxx": 3, "szz": 4, "sxz": 5}

@@ -2,14 +2,15 @@
 the process, for ncu launch lists and kernel captures.
 
     PYTHONPATH=challenge-cup_b200 python -m ertm_b200.profiling \\
-        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2]
+        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--save x.npy]
 
 The job is what ``bench.py`` times: every shot of the workload migrated
 (batched lockstep ticks, or one shot at a time with ``--path plain``) and the
 images stacked.  Records come from the GPU forward model first.  Each repeat
 is preceded by a 256 MiB fill (the benchmark's L2 flush), which also marks the
 start of a repeat in a launch list.  Prints one JSON line: the launches of this
-library per repeat and the stencil profiler's per-tick time and bytes.
+library and the job time per repeat, and the stencil profiler's per-tick time
+and bytes over the last repeat.
 """
 
 from __future__ import annotations
@@ -28,6 +29,8 @@ def main(argv=None) -> None:
     ap.add_argument("--shots", type=int, default=None)
     ap.add_argument("--path", choices=("batched", "plain"), default="batched")
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--tile-rows", type=int, default=0, help="stencil tile height 8/16/32 (0: automatic)")
+    ap.add_argument("--save", default=None, help="write the stacked images of the last repeat (.npy)")
     args = ap.parse_args(argv)
 
     import torch
@@ -38,6 +41,7 @@ def main(argv=None) -> None:
     from .propagation import source_wavelet
 
     L = _lib.lib(0)
+    _lib.check(L.ertm_set_tile_rows(args.tile_rows), "tile rows")
     wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt, **({"n_shots": args.shots} if args.shots else {}))
     imager, solver = workloads.imager_for(wl)
     shots = workloads.synthesize(wl, solver, wl.sources)
@@ -66,20 +70,28 @@ def main(argv=None) -> None:
                                             None), "stack partial")
             _lib.check(L.ertm_stack_finish(npix, partial[k].data_ptr(), n, out[k].data_ptr(), None), "stack finish")
 
-    launches = []
-    _lib.check(L.ertm_profile_stencil(1, 1), "profile")
-    for _ in range(args.repeat):
+    launches, job_ms = [], []
+    for r in range(args.repeat):
         torch.cuda.synchronize()
+        if r == args.repeat - 1:
+            _lib.check(L.ertm_profile_stencil(1, 1), "profile")     # the last repeat's ticks
         flush.fill_(1.0)
         before = L.ertm_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         job()
+        e1.record()
         torch.cuda.synchronize()
+        job_ms.append(e0.elapsed_time(e1))
         launches.append(int(L.ertm_launch_count() - before))
+    if args.save:
+        np.save(args.save, out.cpu().numpy())
     tot, cnt, byt = C.c_double(), C.c_int64(), C.c_double()
     _lib.check(L.ertm_profile_read(C.byref(tot), C.byref(cnt), C.byref(byt)), "profile read")
     _lib.check(L.ertm_profile_stencil(0, 1), "profile off")
     ticks = max(int(cnt.value), 1)
     print(json.dumps({"workload": wl.name, "path": args.path, "nt": wl.nt, "shots": n, "launches_per_repeat": launches,
+                      "job_ms": job_ms,
                       "stencil_us_per_tick": tot.value / ticks * 1e3, "bytes_per_tick": byt.value / ticks,
                       "timed_ticks": int(cnt.value),
                       "achieved_gbs": byt.value / (tot.value * 1e-3) / 1e9 if tot.value > 0 else None,
