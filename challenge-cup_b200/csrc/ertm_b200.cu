@@ -432,21 +432,73 @@ InjectPlanHost& inject_plan(Prop& P, const std::vector<int>& comps, int64_t nt) 
 // --------------------------------------------------------------------------
 // stepping
 // --------------------------------------------------------------------------
+// Host-side access to the works of a WorkSet1 / WorkSetN.
+inline StepWork& ws_work(WorkSet1& ws, int) { return ws.w; }
+inline StepWork ws_work(const WorkSet1& ws, int) { return ws.w; }
+template <int N>
+inline StepWork& ws_work(WorkSetN<N>& ws, int k) { return ws.w[k]; }
+inline void ws_count(WorkSet1&, int) {}
+template <int N>
+inline void ws_count(WorkSetN<N>& ws, int n) { ws.n = n; }
+
+template <int M, int BZ, int R, int KIND, class WS>
+void launch_phase(int engine, int phase, const DevProp* d, const WS& ws, int blocks, cudaStream_t st) {
+  if (blocks <= 0) return;
+  const dim3 blk(XT, BZ);
+  if (phase == 0) {
+    if (engine == ENGINE_ELASTIC) k_elastic_velocity<M, BZ, R, KIND, WS><<<blocks, blk, 0, st>>>(d, ws);
+    else k_pressure_velocity<M, BZ, R, KIND, WS><<<blocks, blk, 0, st>>>(d, ws);
+  } else {
+    if (engine == ENGINE_ACOUSTIC) k_pressure_stress<M, BZ, R, false, KIND, WS><<<blocks, blk, 0, st>>>(d, ws);
+    else if (engine == ENGINE_VISCO) k_pressure_stress<M, BZ, R, true, KIND, WS><<<blocks, blk, 0, st>>>(d, ws);
+    else k_elastic_stress<M, BZ, R, KIND, WS><<<blocks, blk, 0, st>>>(d, ws);
+  }
+  ++g_launches;
+}
+
 template <int M, int BZ, int R, class WS>
 void launch_step_shape(int engine, const DevProp* d, const WS& ws, int blocks, cudaStream_t st) {
-  const dim3 blk(XT, BZ);
-  switch (engine) {
-    case ENGINE_ACOUSTIC:
-      k_pressure_velocity<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
-      k_pressure_stress<M, BZ, R, false, WS><<<blocks, blk, 0, st>>>(d, ws);
-      break;
-    case ENGINE_VISCO:
-      k_pressure_velocity<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
-      k_pressure_stress<M, BZ, R, true, WS><<<blocks, blk, 0, st>>>(d, ws);
-      break;
-    default:
-      k_elastic_velocity<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
-      k_elastic_stress<M, BZ, R, WS><<<blocks, blk, 0, st>>>(d, ws);
+  launch_phase<M, BZ, R, TILES_ALL>(engine, 0, d, ws, blocks, st);
+  launch_phase<M, BZ, R, TILES_ALL>(engine, 1, d, ws, blocks, st);
+}
+
+// A second stream (per device) and fork/join events for the boundary-tile
+// launches, so that they run beside the interior launches.
+struct SplitStreams {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+SplitStreams& split_streams() {
+  static std::mutex mu;
+  static std::map<int, SplitStreams> per_device;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  SplitStreams& s = per_device[dev];
+  if (!s.side) {
+    CK(cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
+  }
+  return s;
+}
+
+// Interior tiles in their own launches: the straight-line kernels then carry
+// none of the boundary code's registers (more resident warps per SM).  The
+// boundary-frame launch of each phase runs on the side stream, concurrently
+// with the interior launch; the two join before the next phase.
+template <int M, int BZ, int R, class WS>
+void launch_step_split(int engine, const DevProp* d, const WS& inner, int n_in, const WS& frame, int n_fr,
+                       cudaStream_t st) {
+  SplitStreams& ss = split_streams();
+  for (int phase = 0; phase < 2; ++phase) {
+    CK(cudaEventRecord(ss.fork, st));
+    CK(cudaStreamWaitEvent(ss.side, ss.fork, 0));
+    launch_phase<M, BZ, R, TILES_FRAME>(engine, phase, d, frame, n_fr, ss.side);
+    launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st);
+    CK(cudaEventRecord(ss.join, ss.side));
+    CK(cudaStreamWaitEvent(st, ss.join, 0));
   }
 }
 
@@ -465,7 +517,78 @@ void launch_step(int M, int tz, int engine, const DevProp* d, const WS& ws, int 
   } else {
     launch_step_shape<1, 16, 1>(engine, d, ws, blocks, st);
   }
-  g_launches += 2;
+}
+
+// The interior rectangle of a work for tile height tz, as Geo::interior
+// decides it tile by tile: physical, clear of every CPML strip, below the
+// free-surface row, with the verified float64-product division; the source
+// node's tile becomes the hole.  Returns the number of interior tiles.
+int plan_interior(const DevProp& h, int tz, StepWork& w) {
+  w.ti0 = w.ti1 = w.tj0 = w.tj1 = 0;
+  w.hole_i = w.hole_j = -1;
+  if (!(h.fast_x == 1 && h.fast_z == 1)) return 0;
+  const int lo_i = std::max(std::max(h.pad, h.npz_t), h.free_surface ? h.pad + 1 : 0);
+  const int hi_i = std::min(h.pad + h.nz, h.nzp - h.npz_b);
+  const int lo_j = std::max(h.pad, h.npx_l);
+  const int hi_j = std::min(h.pad + h.nx, h.nxp - h.npx_r);
+  const int ti0 = (lo_i + tz - 1) / tz, ti1 = hi_i / tz;
+  const int tj0 = (lo_j + TILE_X - 1) / TILE_X, tj1 = hi_j / TILE_X;
+  if (ti1 <= ti0 || tj1 <= tj0) return 0;
+  w.ti0 = ti0;
+  w.ti1 = ti1;
+  w.tj0 = tj0;
+  w.tj1 = tj1;
+  int n = (ti1 - ti0) * (tj1 - tj0);
+  if (h.src_iz >= 0) {
+    const int si = h.src_iz / tz, sj = h.src_ix / TILE_X;
+    if (si >= ti0 && si < ti1 && sj >= tj0 && sj < tj1) {
+      w.hole_i = si;
+      w.hole_j = sj;
+      --n;
+    }
+  }
+  return n;
+}
+
+// Split launches pay off once the interior tiles alone fill the GPU.
+constexpr int64_t kSplitMinTiles = 148 * 4;
+std::atomic<int> g_tile_split{0};   // 0 automatic, 1 never, 2 whenever there are interior tiles
+
+// One step of the works ws.w[0..n) (tile heights tz; tile0/tiles/tiles_x set):
+// split into interior and boundary launches where that pays, else one launch
+// per phase over every tile.
+template <class WS>
+void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, const DevProp* const* hosts,
+                  cudaStream_t st) {
+  int total = 0;
+  for (int k = 0; k < n; ++k) total += ws_work(ws, k).tiles;
+  const int split_mode = g_tile_split.load();
+  if (split_mode != 1 && M == 4 && (tz == 16 || tz == 8)) {
+    WS inner = ws, frame = ws;
+    int n_in = 0, n_fr = 0, ki = 0, kf = 0;
+    for (int k = 0; k < n; ++k) {
+      StepWork w = ws_work(ws, k);
+      const int in = plan_interior(*hosts[k], tz, w);
+      if (in > 0) {
+        StepWork a = w;
+        a.tile0 = n_in;
+        ws_work(inner, ki++) = a;
+        n_in += in;
+      }
+      StepWork b = w;
+      b.tile0 = n_fr;
+      ws_work(frame, kf++) = b;
+      n_fr += w.tiles - in;
+    }
+    if (n_in > 0 && (n_in >= kSplitMinTiles || split_mode == 2)) {
+      ws_count(inner, ki);
+      ws_count(frame, kf);
+      if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st);
+      else launch_step_split<4, 8, 1>(engine, d, inner, n_in, frame, n_fr, st);
+      return;
+    }
+  }
+  launch_step(M, tz, engine, d, ws, total, st);
 }
 
 // Division mode for a grid spacing h (see divh): the cheapest form that the
@@ -657,7 +780,8 @@ void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, co
   WorkSet1 ws{make_work(P, amp64, wave, t, epi)};
   cudaEvent_t e0 = nullptr;
   const bool timed = g_prof.begin(P.st, e0);
-  launch_step(P.M, P.tz, P.h.engine, P.dp(), ws, P.tiles, P.st);
+  const DevProp* hosts[1] = {&P.h};
+  launch_works(P.M, P.tz, P.h.engine, P.dp(), ws, 1, hosts, P.st);
   if (timed) g_prof.end(P.st, e0, step_bytes(P) + (epi ? epilogue_bytes(*epi, (size_t)P.h.nz * P.h.nx) : 0.0));
   after_step(P, amp64, wave, t);
 }
@@ -1118,6 +1242,7 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
     WorkSetB ws{};
     ws.n = (int)(c1 - c0);
     int tile0 = 0;
+    const DevProp* hosts[MAX_BATCH_WORKS];
     for (size_t k = c0; k < c1; ++k) {
       const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
       StepWork w = items[k]->w;
@@ -1126,9 +1251,10 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
       w.tiles = tiles_for(P.h, tz);
       tile0 += w.tiles;
       ws.w[k - c0] = w;
+      hosts[k - c0] = &P.h;
       bytes += step_bytes(P) + epilogue_bytes(w.epi, (size_t)P.h.nz * P.h.nx);
     }
-    launch_step(M, tz, engine, table, ws, tile0, st);
+    launch_works(M, tz, engine, table, ws, ws.n, hosts, st);
   }
 }
 
@@ -1401,6 +1527,13 @@ int32_t ertm_set_tile_rows(int32_t rows) {
   return guarded([&] {
     REQUIRE(rows == 0 || rows == 8 || rows == 16 || rows == 32, "tile rows must be 0 (auto), 8, 16 or 32");
     g_tile_rows = rows;
+  });
+}
+
+int32_t ertm_set_tile_split(int32_t mode) {
+  return guarded([&] {
+    REQUIRE(mode >= 0 && mode <= 2, "tile split mode must be 0 (automatic), 1 (never) or 2 (always)");
+    g_tile_split.store(mode);
   });
 }
 

@@ -115,6 +115,11 @@ struct StepWork {
   float amp;            // source amplitude (when wavelet == nullptr)
   float amp_eps;        // viscoacoustic strain amplitude (when wavelet == nullptr)
   int32_t flags;        // STEP_* bits
+  // Straight-line interior tiles: rows [ti0, ti1) × columns [tj0, tj1) of
+  // tiles, less the source node's tile (hole_i, hole_j; −1 when none).  A
+  // launch of interior tiles walks the rectangle; a launch of boundary tiles
+  // walks the frame around it and then the hole.
+  int32_t ti0, ti1, tj0, tj1, hole_i, hole_j;
   Epilogue epi;
 };
 constexpr int STEP_PEAK = 1;        // visco: reduce max|p| into DevProp::peak

@@ -96,6 +96,39 @@ __device__ __forceinline__ TileLoc tile_of(const StepWork& w, int block, int tz)
   return {ti * tz, (t - ti * w.tiles_x) * TILE_X};
 }
 
+// Tile kinds of a launch: 0 every tile of the propagators (each block picks
+// the interior or the boundary form), 1 the interior rectangle only, 2 the
+// boundary frame (and the hole) only.
+constexpr int TILES_ALL = 0, TILES_INTERIOR = 1, TILES_FRAME = 2;
+
+template <int KIND>
+__device__ __forceinline__ TileLoc tile_loc(const StepWork& w, int block, int tz) {
+  if constexpr (KIND == TILES_ALL) {
+    return tile_of(w, block, tz);
+  } else if constexpr (KIND == TILES_INTERIOR) {
+    const int nx_r = w.tj1 - w.tj0;
+    int k = block - w.tile0;
+    if (w.hole_i >= 0 && k >= (w.hole_i - w.ti0) * nx_r + (w.hole_j - w.tj0)) ++k;
+    const int q = k / nx_r;
+    return {(w.ti0 + q) * tz, (w.tj0 + (k - q * nx_r)) * TILE_X};
+  } else {
+    int k = block - w.tile0;
+    const int tx = w.tiles_x, rows = w.tiles / w.tiles_x;
+    const int top = w.ti0 * tx;
+    if (k < top) return {(k / tx) * tz, (k % tx) * TILE_X};
+    k -= top;
+    const int bottom = (rows - w.ti1) * tx;
+    if (k < bottom) return {(w.ti1 + k / tx) * tz, (k % tx) * TILE_X};
+    k -= bottom;
+    const int side = w.tj0 + (tx - w.tj1);
+    if (k < (w.ti1 - w.ti0) * side) {
+      const int q = k / side, c = k - q * side;
+      return {(w.ti0 + q) * tz, (c < w.tj0 ? c : w.tj1 + (c - w.tj0)) * TILE_X};
+    }
+    return {w.hole_i * tz, w.hole_j * TILE_X};
+  }
+}
+
 // Source amplitudes of this step: float32(amp) for the field and, for the
 // viscoacoustic strain, float32(amp / K_R) computed in float64
 // (propagation.py:707-713).
@@ -325,7 +358,7 @@ __device__ __forceinline__ ColInfo col_info(const Geo& G, int j, const float* ax
 // velocity phase
 // ---------------------------------------------------------------------------
 // Acoustic and viscoacoustic: vx += (dt·irx)·(D⁺ₓp + ψ), vz += (dt·irz)·(D⁺_z p + ψ).
-template <int M, int BZ, int R, class WS>
+template <int M, int BZ, int R, int KIND, class WS>
 __global__ void __launch_bounds__(XT* BZ)
 k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
@@ -334,7 +367,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
-  const TileLoc L = tile_of(w, blockIdx.x, TZ);
+  const TileLoc L = tile_loc<KIND>(w, blockIdx.x, TZ);
   float* const vx = P.f[A_VX];
   float* const vz = P.f[A_VZ];
   const float* const irx = P.coef[CA_IRX];
@@ -356,7 +389,9 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   cp_async_wait_all();
   __syncthreads();
   if (j >= G.nxp) return;
-  if (G.interior(L.i0, L.j0, TZ)) {
+  if (KIND == TILES_INTERIOR && !G.interior(L.i0, L.j0, TZ)) return;   // the host plans only interior tiles here
+  if (KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ))) {
+    if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
@@ -377,8 +412,10 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
       st4(vx + g, ox);
       st4(vz + g, oz);
     }
+    }
     return;
   }
+  if constexpr (KIND != TILES_INTERIOR) {
   const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
@@ -419,10 +456,11 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
     }
     st4(vz + g, oz);
   }
+  }
 }
 
 // Elastic: vx += (dt·irx)·(D⁺ₓσxx + D⁻_zσxz), vz += (dt·irz)·(D⁻ₓσxz + D⁺_zσzz).
-template <int M, int BZ, int R, class WS>
+template <int M, int BZ, int R, int KIND, class WS>
 __global__ void __launch_bounds__(XT* BZ)
 k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
@@ -433,7 +471,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
-  const TileLoc L = tile_of(w, blockIdx.x, TZ);
+  const TileLoc L = tile_loc<KIND>(w, blockIdx.x, TZ);
   float* const vx = P.f[E_VX];
   float* const vz = P.f[E_VZ];
   const float* const irx = P.coef[CE_IRX];
@@ -454,7 +492,9 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   cp_async_wait_all();
   __syncthreads();
   if (j >= G.nxp) return;
-  if (G.interior(L.i0, L.j0, TZ)) {
+  if (KIND == TILES_INTERIOR && !G.interior(L.i0, L.j0, TZ)) return;   // the host plans only interior tiles here
+  if (KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ))) {
+    if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
@@ -481,8 +521,10 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
       }
       st4(vz + g, oz);
     }
+    }
     return;
   }
+  if constexpr (KIND != TILES_INTERIOR) {
   const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
@@ -550,6 +592,7 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
     }
     st4(vz + g, oz);
   }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -573,7 +616,7 @@ __device__ __forceinline__ void block_max_to(float v, float* dst) {
 
 // Acoustic (VISCO=false): p += (dt·κ)·div.  Viscoacoustic (VISCO=true):
 // ε += dt·div; r_l ← r_l·a_l + b_l·Δε; p = K_R·ε + Σ r_l.
-template <int M, int BZ, int R, bool VISCO, class WS>
+template <int M, int BZ, int R, bool VISCO, int KIND, class WS>
 __global__ void __launch_bounds__(XT* BZ)
 k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
@@ -583,7 +626,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
-  const TileLoc L = tile_of(w, blockIdx.x, TZ);
+  const TileLoc L = tile_loc<KIND>(w, blockIdx.x, TZ);
   float* const p = P.f[A_P];
   float* const eps = VISCO ? P.f[V_EPS] : nullptr;
   float* const r0 = VISCO ? P.f[V_R0] : nullptr;
@@ -611,7 +654,10 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   __syncthreads();
   const size_t npix = (size_t)G.nz * G.nx;
   float peak = 0.f;
-  if (jok && G.interior(L.i0, L.j0, TZ)) {
+  const bool valid = KIND != TILES_INTERIOR || G.interior(L.i0, L.j0, TZ);   // the host plans only interior tiles there
+  const bool inner = KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ));
+  if (jok && inner && valid) {
+    if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
@@ -650,7 +696,9 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
       if constexpr (VISCO) st4(eps + g, epsv);
       if (w.epi.kind != EPI_NONE) st4(e_p + rr * 32 + 4 * threadIdx.x, out);
     }
-  } else if (jok) {
+    }
+  } else if (jok && !inner) {
+    if constexpr (KIND != TILES_INTERIOR) {
     const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
@@ -721,8 +769,9 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
       if constexpr (VISCO) st4(eps + g, epsv);
       if (w.epi.kind != EPI_NONE) st4(e_p + rr * 32 + 4 * threadIdx.x, out);
     }
+    }
   }
-  if (w.epi.kind != EPI_NONE) {
+  if (valid && w.epi.kind != EPI_NONE) {
     __syncthreads();
     epilogue_tile<TZ, XT * BZ>(w.epi, G, L.i0, L.j0, e_p, nullptr, npix);
   }
@@ -736,7 +785,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
 //   σxz += (dt·μxz)·(D⁺_z vx + D⁺ₓ vz); source; free surface σzz = σxz = 0;
 // then the epilogue with P/S from the stresses (stress separation) or from
 // the raw velocity divergence/curl (divcurl, propagation.py:953-976).
-template <int M, int BZ, int R, class WS>
+template <int M, int BZ, int R, int KIND, class WS>
 __global__ void __launch_bounds__(XT* BZ)
 k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   constexpr int TZ = BZ * R;
@@ -746,7 +795,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
-  const TileLoc L = tile_of(w, blockIdx.x, TZ);
+  const TileLoc L = tile_loc<KIND>(w, blockIdx.x, TZ);
   float* const sxx = P.f[E_SXX];
   float* const szz = P.f[E_SZZ];
   float* const sxz = P.f[E_SXZ];
@@ -778,7 +827,10 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   const Epilogue& E = w.epi;
   const bool epi = E.kind != EPI_NONE;
   const bool want_curl = epi && E.sep == 1 && E.need_s;
-  if (j < G.nxp && G.interior(L.i0, L.j0, TZ)) {
+  const bool valid = KIND != TILES_INTERIOR || G.interior(L.i0, L.j0, TZ);   // the host plans only interior tiles there
+  const bool inner = KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ));
+  if (j < G.nxp && inner && valid) {
+    if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int rr = threadIdx.y + BZ * r;
@@ -834,7 +886,9 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
         st4(e_s + rr * 32 + 4 * threadIdx.x, sv4);
       }
     }
-  } else if (j < G.nxp) {
+    }
+  } else if (j < G.nxp && !inner) {
+    if constexpr (KIND != TILES_INTERIOR) {
     const ColInfo C = col_info<M>(G, j, P.ax, P.bx);
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
@@ -925,8 +979,9 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
         st4(e_s + rr * 32 + 4 * threadIdx.x, sv4);
       }
     }
+    }
   }
-  if (epi) {
+  if (epi && valid) {
     __syncthreads();
     epilogue_tile<TZ, XT * BZ>(E, G, L.i0, L.j0, e_p, e_s, npix);
   }

@@ -120,6 +120,11 @@ int64_t ertm_launch_count(void);
 /* Pin the stencil tile height (8, 16 or 32 rows; 0 = automatic) for
  * propagators created afterwards — the autotuner's knob (order 8 only). */
 int32_t ertm_set_tile_rows(int32_t rows);
+/* Interior tiles (clear of CPML strips, free surface and source) in launches
+ * of their own, apart from the boundary tiles: 0 = when the interior tiles
+ * alone fill the GPU (default), 1 = never, 2 = whenever there are any.  The
+ * results are the same either way; the knob is for tuning and tests. */
+int32_t ertm_set_tile_split(int32_t mode);
 /* Count, over all 2^32 float inputs a, where the fast division form `mode`
  * (3 one-FMA, 2 FMA correction, 1 float64 product) differs in value from
  * __fdiv_rn(a, h) (no reference counterpart; diagnostics). */

@@ -221,3 +221,81 @@ def test_kahan_accumulation_close_to_fp64(eb):
     a = RTMImager(imaging, solver).migrate(shot, model_from_types(fx))
     b = RTMImager(imaging, solver, accumulation="kahan").migrate(shot, model_from_types(fx))
     assert rel_l2(b.image, a.image) < 1e-5
+
+
+@pytest.fixture
+def split_always(eb):
+    """Interior tiles in launches of their own even on small grids."""
+    from ertm_b200 import _lib
+    _lib.check(_lib.lib().ertm_set_tile_split(2), "split")
+    yield
+    _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
+
+
+@pytest.mark.parametrize("engine,boundary,mechanism,tile_rows", [
+    ("acoustic", "cpml", "explosive", 16), ("acoustic", "free", "explosive", 8),
+    ("elastic", "free", "explosive", 16), ("elastic", "cpml", "force_z", 8), ("elastic", "free", "shear", 16),
+    ("viscoacoustic", "cpml", "explosive", 16)])
+def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, boundary, mechanism, tile_rows):
+    """Interior tiles and the boundary frame in separate launches (the source
+    node's tile, inside the interior rectangle, goes with the frame): GPU ==
+    oracle on a grid with an interior rectangle of several tiles."""
+    from ertm_b200 import _lib
+    from ertm_b200.propagation import PropagationSpec, QOptions, run_forward
+    _lib.check(_lib.lib().ertm_set_tile_rows(tile_rows), "tile rows")
+    try:
+        rng = np.random.default_rng(11)
+        nz, nx = 150, 200
+        vp = rng.uniform(2000.0, 3000.0, size=(nz, nx)).astype(np.float32)
+        model = model_from({"m_vp": vp, "m_vs": (vp / 1.9).astype(np.float32),
+                            "m_rho": rng.uniform(1800, 2400, (nz, nx)).astype(np.float32),
+                            "m_qp": np.where(np.arange(nz)[:, None] < 70, 40.0, 90.0).repeat(nx, 1).astype(np.float32),
+                            "m_qs": np.full((nz, nx), 30.0, np.float32),
+                            "m_grid": np.array([nx, nz, 5.0, 5.0, 0.0, 0.0])})
+        dt = 0.8 * orc.cfl_dt(float(vp.max()), 5.0, 5.0, 8, 0.5)
+        spec = PropagationSpec(dt=dt, nt=90, order=8, npml=12, boundary=boundary)
+        src = source_from({"src": np.array([502.0, 371.0, 40.0, 0.02, 1.0])}, mechanism)
+        rcv = receivers_from({"rx": rng.uniform(0, 995, 31), "rz": rng.uniform(0, 745, 31)})
+        comps = ("p", "vx", "vz") if engine != "elastic" else ("p", "vx", "vz", "sxz")
+        q = QOptions(enabled=True, f_ref=30.0) if engine == "viscoacoustic" else None
+        got = run_forward(model, src, rcv, spec, engine=engine, components=comps, q_options=q)
+        ospec = orc.Spec(dt=dt, nt=90, order=8, npml=12, boundary=boundary)
+        want = orc.run_forward(model, src, rcv, ospec, engine=engine, components=comps, q=q)
+    finally:
+        _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
+    for n in comps:
+        if engine == "viscoacoustic":
+            assert rel_l2(got[n], want[n]) < VISCO_TOL, n
+        else:
+            assert np.array_equal(got[n], want[n]), (n, rel_l2(got[n], want[n]))
+
+
+def test_batched_images_equal_with_and_without_split_launches(eb):
+    """The batched migration gives the same images whether interior tiles run
+    in launches of their own or with the boundary tiles."""
+    from ertm_b200 import ImagingConfig, RTMImager, SolverConfig, _lib
+    from ertm_b200.batch import BatchMigrator
+    from ertm_b200.propagation import PropagationSpec, forward_shot
+    from ertm_b200.types import ElasticModel, GridSpec, ReceiverSpec, SourceSpec
+    rng = np.random.default_rng(5)
+    g = GridSpec(nx=180, nz=140, dx=5.0, dz=5.0)
+    vp = (2200.0 + 900.0 * (np.arange(g.nz)[:, None] > 70) + rng.uniform(0, 60, g.shape)).astype(np.float32)
+    model = ElasticModel(grid=g, vp=vp, vs=(vp / 1.8).astype(np.float32), rho=np.full(g.shape, 2100.0, np.float32),
+                         qp=np.full(g.shape, 80.0, np.float32), qs=np.full(g.shape, 40.0, np.float32))
+    x = np.arange(0.0, 895.0, 20.0)
+    rec = ReceiverSpec(x=x, z=np.full_like(x, 10.0))
+    shots = [forward_shot(model, SourceSpec(x=300.0 + 150.0 * k, z=10.0, f0=30.0, delay=0.03), rec,
+                          PropagationSpec(dt=4e-4, nt=260, npml=20, boundary="free"), engine="elastic",
+                          components=("vz", "p")) for k in range(3)]
+    imager = RTMImager(ImagingConfig(condition="normalized", checkpoint_mb=2.0),
+                       SolverConfig(nt=260, dt=4e-4, boundary="free", engine="elastic"))
+    out = {}
+    for mode in (1, 2):
+        _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
+        try:
+            out[mode] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
+        finally:
+            _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
+    for a, b in zip(out[1], out[2]):
+        for x1, x2 in zip(a, b):
+            assert np.array_equal(x1.image, x2.image), x1.mode
