@@ -550,8 +550,10 @@ int plan_interior(const DevProp& h, int tz, StepWork& w) {
   return n;
 }
 
-// Split launches pay off once the interior tiles alone fill the GPU.
-constexpr int64_t kSplitMinTiles = 148 * 4;
+// Split launches (twice the launches, a fork and a join per phase) pay off
+// once the interior tiles alone fill the GPU several times over; below that
+// (a single 401×601 grid, say) the single launch per phase is faster.
+constexpr int64_t kSplitMinTiles = 148 * 16;
 std::atomic<int> g_tile_split{0};   // 0 automatic, 1 never, 2 whenever there are interior tiles
 
 // One step of the works ws.w[0..n) (tile heights tz; tile0/tiles/tiles_x set):
@@ -563,7 +565,7 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
   int total = 0;
   for (int k = 0; k < n; ++k) total += ws_work(ws, k).tiles;
   const int split_mode = g_tile_split.load();
-  if (split_mode != 1 && M == 4 && (tz == 16 || tz == 8)) {
+  if (split_mode != 1 && M == 4) {
     WS inner = ws, frame = ws;
     int n_in = 0, n_fr = 0, ki = 0, kf = 0;
     for (int k = 0; k < n; ++k) {
@@ -583,7 +585,8 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
     if (n_in > 0 && (n_in >= kSplitMinTiles || split_mode == 2)) {
       ws_count(inner, ki);
       ws_count(frame, kf);
-      if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st);
+      if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st);
+      else if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st);
       else launch_step_split<4, 8, 1>(engine, d, inner, n_in, frame, n_fr, st);
       return;
     }
