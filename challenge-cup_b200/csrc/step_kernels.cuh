@@ -216,9 +216,66 @@ __device__ __forceinline__ void run_epilogue(const Epilogue& E, size_t c, size_t
 // per thread, so a warp covers 32 consecutive physical cells of a row and its
 // accumulator, replay and excitation accesses coalesce whatever their
 // alignment.  One copy of the epilogue code serves every cell.
+//
+// The imaging condition with float64 sums (the common case) gathers: a thread
+// loads the replayed source values of all its cells, then, accumulator by
+// accumulator, loads all its cells' sums before it adds and stores them, so
+// several global loads are in flight per thread instead of one.
+template <int IT>
+struct ImageCells {
+  uint32_t pc[IT];
+  bool ok[IT];
+  float s0[IT], s1[IT];
+};
+
+template <int IT, class TERM>
+__device__ __forceinline__ void accumulate_cells(double* acc, const ImageCells<IT>& C, TERM term) {
+  double a[IT];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) a[it] = C.ok[it] ? acc[C.pc[it]] : 0.0;
+#pragma unroll
+  for (int it = 0; it < IT; ++it)
+    if (C.ok[it]) acc[C.pc[it]] = dadd(a[it], (double)term(it));
+}
+
+template <int TZ, int NT, class GEO>
+__device__ __forceinline__ void image_tile_f64(const Epilogue& E, const GEO& G, int i0, int j0, const float* e_p,
+                                               const float* e_s) {
+  constexpr int IT = TZ * 32 / NT;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+  ImageCells<IT> C;
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = tid + it * NT;
+    size_t pc = 0;
+    C.ok[it] = G.physical(i0 + (idx >> 5), j0 + (idx & 31), pc);
+    C.pc[it] = (uint32_t)pc;
+  }
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    C.s0[it] = (C.ok[it] && E.src[0]) ? E.src[0][C.pc[it]] : 0.f;
+    C.s1[it] = (C.ok[it] && E.src[1]) ? E.src[1][C.pc[it]] : 0.f;
+  }
+#pragma unroll 1
+  for (int k = 0; k < E.n_images; ++k) {
+    const bool s_is_1 = E.src_slot[k] != 0;
+    const bool r_is_s = E.rcv_wave[k] != 0;
+    auto src = [&](int it) { return s_is_1 ? C.s1[it] : C.s0[it]; };
+    auto rcv = [&](int it) { return r_is_s ? (e_s ? e_s[tid + it * NT] : 0.f) : e_p[tid + it * NT]; };
+    // imaging.py:313-324: illum += S², rillum += R² (all steps); num += S·R (t ≥ start)
+    if (E.illum && E.ill[k]) accumulate_cells(E.ill[k], C, [&](int it) { return fmul(src(it), src(it)); });
+    if (E.rillum && E.ril[k]) accumulate_cells(E.ril[k], C, [&](int it) { return fmul(rcv(it), rcv(it)); });
+    if (E.cross) accumulate_cells(E.num[k], C, [&](int it) { return fmul(src(it), rcv(it)); });
+  }
+}
+
 template <int TZ, int NT, class GEO>
 __device__ __forceinline__ void epilogue_tile(const Epilogue& E, const GEO& G, int i0, int j0, const float* e_p,
                                               const float* e_s, size_t npix) {
+  if (E.kind == EPI_IMAGE && !E.kahan && (TZ * 32) % NT == 0) {
+    image_tile_f64<TZ, NT>(E, G, i0, j0, e_p, e_s);
+    return;
+  }
   const int tid = threadIdx.y * XT + threadIdx.x;
 #pragma unroll 1
   for (int idx = tid; idx < TZ * 32; idx += NT) {
