@@ -86,6 +86,48 @@ __device__ __forceinline__ void stage_cells(float* s, const float* __restrict__ 
   }
 }
 
+// Several arrays of one propagator staged together: they share the row pitch,
+// so a thread computes each chunk's offset and bounds once and issues one copy
+// per array.
+template <int M, int TZ, int NT, int NF>
+__device__ __forceinline__ void stage_n(float* const (&s)[NF], const float* const (&g)[NF], int nzp, int ld, int i0,
+                                        int j0) {
+  using T = TileShape<M, TZ>;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (T::CHUNKS + NT - 1) / NT; ++it) {
+    const int idx = tid + it * NT;
+    if (T::CHUNKS % NT != 0 && idx >= T::CHUNKS) break;
+    const int r = idx / (T::W / 4);
+    const int ch = idx - r * (T::W / 4);
+    const int gi = i0 - M + r, gj = j0 - T::OFF + 4 * ch;
+    const bool ok = gi >= 0 && gi < nzp && gj >= 0 && gj < ld;
+    const size_t off = ok ? (size_t)gi * ld + gj : 0;
+    const int so = r * T::W + 4 * ch;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) cp_async16(s[f] + so, g[f] + off, ok);
+  }
+}
+
+template <int TZ, int NT, int NF>
+__device__ __forceinline__ void stage_cells_n(float* const (&s)[NF], const float* const (&g)[NF], int nzp, int ld,
+                                              int i0, int j0) {
+  constexpr int CH = TZ * 8;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (CH + NT - 1) / NT; ++it) {
+    const int idx = tid + it * NT;
+    if (CH % NT != 0 && idx >= CH) break;
+    const int r = idx >> 3, ch = idx & 7;
+    const int gi = i0 + r;
+    const bool ok = gi < nzp;
+    const size_t off = ok ? (size_t)gi * ld + j0 + 4 * ch : 0;
+    const int so = r * 32 + 4 * ch;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) cp_async16(s[f] + so, g[f] + off, ok);
+  }
+}
+
 struct TileLoc {
   int i0, j0;
 };
@@ -436,10 +478,11 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
     *P.peak = 0.f;  // the stress phase of this step reduces into it
   __shared__ __align__(16) float c_vx[TZ * 32], c_vz[TZ * 32], c_irx[TZ * 32], c_irz[TZ * 32];
   stage<M, TZ, XT * BZ>(sp, P.f[A_P], G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_vx, vx, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_vz, vz, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_irx, irx, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_irz, irz, G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const cs[4] = {c_vx, c_vz, c_irx, c_irz};
+    const float* const cg[4] = {vx, vz, irx, irz};
+    stage_cells_n<TZ, XT * BZ, 4>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
+  }
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
 #define CELL(arr, rr) ld4(arr + (rr) * 32 + 4 * threadIdx.x)
@@ -536,14 +579,17 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   float* const psx0 = P.psix[0]; float* const psx1 = P.psix[1];
   float* const psz0 = P.psiz[0]; float* const psz1 = P.psiz[1];
   const float* const azp = P.az; const float* const bzp = P.bz;
-  stage<M, TZ, XT * BZ>(sxx_s, P.f[E_SXX], G.nzp, G.ld, L.i0, L.j0);
-  stage<M, TZ, XT * BZ>(szz_s, P.f[E_SZZ], G.nzp, G.ld, L.i0, L.j0);
-  stage<M, TZ, XT * BZ>(sxz_s, P.f[E_SXZ], G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const hs[3] = {sxx_s, szz_s, sxz_s};
+    const float* const hg[3] = {P.f[E_SXX], P.f[E_SZZ], P.f[E_SXZ]};
+    stage_n<M, TZ, XT * BZ, 3>(hs, hg, G.nzp, G.ld, L.i0, L.j0);
+  }
   __shared__ __align__(16) float c_vx[TZ * 32], c_vz[TZ * 32], c_irx[TZ * 32], c_irz[TZ * 32];
-  stage_cells<TZ, XT * BZ>(c_vx, vx, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_vz, vz, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_irx, irx, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_irz, irz, G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const cs[4] = {c_vx, c_vz, c_irx, c_irz};
+    const float* const cg[4] = {vx, vz, irx, irz};
+    stage_cells_n<TZ, XT * BZ, 4>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
+  }
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
   cp_async_wait_all();
@@ -696,12 +742,18 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   float* const psx = P.psix[1];
   float* const psz = P.psiz[1];
   const float* const azp = P.az; const float* const bzp = P.bz;
-  stage<M, TZ, XT * BZ>(svx, P.f[A_VX], G.nzp, G.ld, L.i0, L.j0);
-  stage<M, TZ, XT * BZ>(svz, P.f[A_VZ], G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const hs[2] = {svx, svz};
+    const float* const hg[2] = {P.f[A_VX], P.f[A_VZ]};
+    stage_n<M, TZ, XT * BZ, 2>(hs, hg, G.nzp, G.ld, L.i0, L.j0);
+  }
   __shared__ __align__(16) float c_a[TZ * 32], c_b[TZ * 32];   // acoustic: p, κ; viscoacoustic: ε, K_R
   __shared__ __align__(16) float e_p[TZ * 32];                  // P for the epilogue
-  stage_cells<TZ, XT * BZ>(c_a, VISCO ? eps : p, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_b, cA, G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const cs[2] = {c_a, c_b};
+    const float* const cg[2] = {VISCO ? eps : p, cA};
+    stage_cells_n<TZ, XT * BZ, 2>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
+  }
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
   const bool jok = j < G.nxp;
@@ -863,17 +915,19 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   float* const psz2 = P.psiz[2]; float* const psz3 = P.psiz[3];
   const float* const azp = P.az; const float* const bzp = P.bz;
   const int mech = P.mech;
-  stage<M, TZ, XT * BZ>(svx, P.f[E_VX], G.nzp, G.ld, L.i0, L.j0);
-  stage<M, TZ, XT * BZ>(svz, P.f[E_VZ], G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const hs[2] = {svx, svz};
+    const float* const hg[2] = {P.f[E_VX], P.f[E_VZ]};
+    stage_n<M, TZ, XT * BZ, 2>(hs, hg, G.nzp, G.ld, L.i0, L.j0);
+  }
   __shared__ __align__(16) float c_xx[TZ * 32], c_zz[TZ * 32], c_xz[TZ * 32], c_lam[TZ * 32], c_l2m[TZ * 32],
       c_mu[TZ * 32];
   __shared__ __align__(16) float e_p[TZ * 32], e_s[TZ * 32];   // P and S for the epilogue
-  stage_cells<TZ, XT * BZ>(c_xx, sxx, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_zz, szz, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_xz, sxz, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_lam, clam, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_l2m, cl2m, G.nzp, G.ld, L.i0, L.j0);
-  stage_cells<TZ, XT * BZ>(c_mu, cmu, G.nzp, G.ld, L.i0, L.j0);
+  {
+    float* const cs[6] = {c_xx, c_zz, c_xz, c_lam, c_l2m, c_mu};
+    const float* const cg[6] = {sxx, szz, sxz, clam, cl2m, cmu};
+    stage_cells_n<TZ, XT * BZ, 6>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
+  }
   cp_async_commit();
   const int j = L.j0 + 4 * threadIdx.x;
   float amp, amp_eps;
