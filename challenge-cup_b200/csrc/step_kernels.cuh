@@ -344,6 +344,12 @@ struct Geo {
   // Straight-line interior form (only used when the float64-product form was verified).
   __device__ __forceinline__ float dxf(float a) const { return __double2float_rn(__dmul_rn((double)a, rx)); }
   __device__ __forceinline__ float dzf(float a) const { return __double2float_rn(__dmul_rn((double)a, rz)); }
+  // Boundary tiles of a split launch: the host splits only propagators whose
+  // spacings passed the float64-product check, so that form is the only one.
+  template <int KIND>
+  __device__ __forceinline__ float dxk(float a) const { return KIND == 2 ? dxf(a) : dx_(a); }
+  template <int KIND>
+  __device__ __forceinline__ float dzk(float a) const { return KIND == 2 ? dzf(a) : dz_(a); }
   // A tile whose cells are all physical, away from every CPML strip, the
   // free-surface row and the source node, with the FMA division verified:
   // its stencils run without per-cell branches.
@@ -533,7 +539,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
-      float d = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+      float d = C.xin[c] ? G.template dxk<KIND>(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
       if (C.sx[c] >= 0) {
         float* ps = psx + (size_t)i * G.wx + C.sx[c];
         float psi = *ps; d = cpml(d, psi, C.ax[c], C.bx[c]); *ps = psi;
@@ -547,7 +553,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (!C.ok[c]) continue;
-      float d = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
+      float d = zin ? G.template dzk<KIND>(sum_plus<M>(z[c], M, G.c)) : 0.f;
       if (sz >= 0) {
         float* ps = psz + (size_t)sz * G.ld + j + c;
         float psi = *ps; d = cpml(d, psi, azi, bzi); *ps = psi;
@@ -645,11 +651,11 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
       float v[12];
       row12(sxx_s + ro, v);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) a[c] = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+      for (int c = 0; c < 4; ++c) a[c] = C.xin[c] ? G.template dxk<KIND>(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
       float z[4][2 * M + 1];
       col9<M>(sxz_s + ro + 4, z);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
+      for (int c = 0; c < 4; ++c) b[c] = zin ? G.template dzk<KIND>(sum_minus<M>(z[c], M, G.c)) : 0.f;
     }
     float4 ox = CELL(c_vx, rr);
 #pragma unroll
@@ -672,11 +678,11 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
       float v[12];
       row12(sxz_s + ro, v);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) a[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+      for (int c = 0; c < 4; ++c) a[c] = C.xin[c] ? G.template dxk<KIND>(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
       float z[4][2 * M + 1];
       col9<M>(szz_s + ro + 4, z);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
+      for (int c = 0; c < 4; ++c) b[c] = zin ? G.template dzk<KIND>(sum_plus<M>(z[c], M, G.c)) : 0.f;
     }
     float4 oz = CELL(c_vz, rr);
 #pragma unroll
@@ -824,11 +830,11 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
         float v[12];
         row12(svx + ro, v);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) dx[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+        for (int c = 0; c < 4; ++c) dx[c] = C.xin[c] ? G.template dxk<KIND>(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
         float z[4][2 * M + 1];
         col9<M>(svz + ro + 4, z);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) dz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
+        for (int c = 0; c < 4; ++c) dz[c] = zin ? G.template dzk<KIND>(sum_minus<M>(z[c], M, G.c)) : 0.f;
       }
       float4 out = CELL(c_a, rr);
       float4 epsv = out;
@@ -1016,23 +1022,23 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
         float v[12];
         row12(svx + ro, v);        // vx along x: D⁻ (εxx)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) exx[c] = C.xin[c] ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+        for (int c = 0; c < 4; ++c) exx[c] = C.xin[c] ? G.template dxk<KIND>(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
         row12(svz + ro, v);        // vz along x: D⁺ (σxz) and D⁻ (curl)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          f2[c] = C.xin[c] ? G.dx_(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
-          curl_b[c] = want_curl ? G.dx_(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
+          f2[c] = C.xin[c] ? G.template dxk<KIND>(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
+          curl_b[c] = want_curl ? G.template dxk<KIND>(sum_minus<M>(v, 4 + c, G.c)) : 0.f;
         }
         float z[4][2 * M + 1];
         col9<M>(svx + ro + 4, z);  // vx along z: D⁺ (σxz) and D⁻ (curl)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          f1[c] = zin ? G.dz_(sum_plus<M>(z[c], M, G.c)) : 0.f;
-          curl_a[c] = want_curl ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
+          f1[c] = zin ? G.template dzk<KIND>(sum_plus<M>(z[c], M, G.c)) : 0.f;
+          curl_a[c] = want_curl ? G.template dzk<KIND>(sum_minus<M>(z[c], M, G.c)) : 0.f;
         }
         col9<M>(svz + ro + 4, z);  // vz along z: D⁻ (εzz)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) ezz[c] = zin ? G.dz_(sum_minus<M>(z[c], M, G.c)) : 0.f;
+        for (int c = 0; c < 4; ++c) ezz[c] = zin ? G.template dzk<KIND>(sum_minus<M>(z[c], M, G.c)) : 0.f;
       }
       float4 oxx = CELL(c_xx, rr), ozz = CELL(c_zz, rr), oxz = CELL(c_xz, rr);
       float4 pv4 = make_float4(0.f, 0.f, 0.f, 0.f), sv4 = pv4;
