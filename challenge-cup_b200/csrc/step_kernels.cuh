@@ -459,6 +459,50 @@ __device__ __forceinline__ ColInfo col_info(const Geo& G, int j, const float* ax
   return C;
 }
 
+// Viscoacoustic memory variables of one thread's 4 cells (propagation.py:
+// 700-705): r_l ← r_l·a_l(Q) + b_l·Δε for l = 0 … L−1, total = Σ_l r_l in
+// that order.  Each r_l and b_l row is one aligned 16-byte word, so a
+// mechanism costs two vector loads and one vector store.  Columns with
+// keep[c] set are left as they are.
+__device__ __forceinline__ void relax4(float* r0, const float* b0, size_t fstride, const uint8_t* qidx,
+                                       const float* relax_a, int nL, size_t g, const float (&inc)[4],
+                                       const bool (&keep)[4], float (&tot)[4]) {
+  const uchar4 q4 = *reinterpret_cast<const uchar4*>(qidx + g);
+  const int q[4] = {q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tot[c] = 0.f;
+  for (int l = 0; l < nL; ++l) {
+    float* rl = r0 + l * fstride;
+    const float4 r4 = ld4(rl + g);
+    const float4 b4 = ldg4(b0 + l * fstride + g);
+    float4 o4;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const float rv = fadd(fmul(comp(r4, c), __ldg(relax_a + q[c] * nL + l)), fmul(comp(b4, c), inc[c]));
+      set_comp(o4, c, keep[c] ? comp(r4, c) : rv);
+      tot[c] = (l == 0) ? rv : fadd(tot[c], rv);
+    }
+    st4(rl + g, o4);
+  }
+}
+
+// CPML memories of one thread's 4 cells in one x-strip and one z-strip
+// array, loaded together before any is updated (the cells' memories are
+// distinct, so the loads can all be in flight at once).  z-strip rows hold ld
+// columns, so their 4 cells are one aligned 16-byte word.
+struct PsiCells {
+  float x[4];
+  float4 z;
+};
+__device__ __forceinline__ PsiCells psi_cells(const ColInfo& C, const float* psx, int i, int wx, const float* psz,
+                                              int sz, int ld, int j) {
+  PsiCells q;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) q.x[c] = (C.ok[c] && C.sx[c] >= 0) ? psx[(size_t)i * wx + C.sx[c]] : 0.f;
+  q.z = sz >= 0 ? ld4(psz + (size_t)sz * ld + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+  return q;
+}
+
 // ---------------------------------------------------------------------------
 // velocity phase
 // ---------------------------------------------------------------------------
@@ -533,6 +577,7 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
     const bool zin = (i >= M && i < G.nzp - M);
     const int sz = G.sz(i);
     const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+    PsiCells q = psi_cells(C, psx, i, G.wx, psz, sz, G.ld, j);
     float v[12];
     row12(row, v);
     float4 ox = CELL(c_vx, rr);
@@ -541,8 +586,8 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
       if (!C.ok[c]) continue;
       float d = C.xin[c] ? G.template dxk<KIND>(sum_plus<M>(v, 4 + c, G.c)) : 0.f;
       if (C.sx[c] >= 0) {
-        float* ps = psx + (size_t)i * G.wx + C.sx[c];
-        float psi = *ps; d = cpml(d, psi, C.ax[c], C.bx[c]); *ps = psi;
+        d = cpml(d, q.x[c], C.ax[c], C.bx[c]);
+        psx[(size_t)i * G.wx + C.sx[c]] = q.x[c];
       }
       set_comp(ox, c, fadd(comp(CELL(c_vx, rr), c), fmul(fmul(G.dt, comp(CELL(c_irx, rr), c)), d)));
     }
@@ -555,12 +600,14 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
       if (!C.ok[c]) continue;
       float d = zin ? G.template dzk<KIND>(sum_plus<M>(z[c], M, G.c)) : 0.f;
       if (sz >= 0) {
-        float* ps = psz + (size_t)sz * G.ld + j + c;
-        float psi = *ps; d = cpml(d, psi, azi, bzi); *ps = psi;
+        float psi = comp(q.z, c);
+        d = cpml(d, psi, azi, bzi);
+        set_comp(q.z, c, psi);
       }
       set_comp(oz, c, fadd(comp(CELL(c_vz, rr), c), fmul(fmul(G.dt, comp(CELL(c_irz, rr), c)), d)));
     }
     st4(vz + g, oz);
+    if (sz >= 0) st4(psz + (size_t)sz * G.ld + j, q.z);
   }
   }
 }
@@ -645,6 +692,8 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
     const bool zin = (i >= M && i < G.nzp - M);
     const int sz = G.sz(i);
     const float azi = sz >= 0 ? azp[i] : 0.f, bzi = sz >= 0 ? bzp[i] : 1.f;
+    PsiCells q0 = psi_cells(C, psx0, i, G.wx, psz0, sz, G.ld, j);
+    PsiCells q1 = psi_cells(C, psx1, i, G.wx, psz1, sz, G.ld, j);
     // vx: vx_dsxx (x, D⁺ of σxx) + vx_dsxz (z, D⁻ of σxz)
     float a[4], b[4];
     {
@@ -663,16 +712,18 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
       if (!C.ok[c]) continue;
       float av = a[c], bv = b[c];
       if (C.sx[c] >= 0) {
-        float* ps = psx0 + (size_t)i * G.wx + C.sx[c];
-        float psi = *ps; av = cpml(av, psi, C.ax[c], C.bx[c]); *ps = psi;
+        av = cpml(av, q0.x[c], C.ax[c], C.bx[c]);
+        psx0[(size_t)i * G.wx + C.sx[c]] = q0.x[c];
       }
       if (sz >= 0) {
-        float* ps = psz0 + (size_t)sz * G.ld + j + c;
-        float psi = *ps; bv = cpml(bv, psi, azi, bzi); *ps = psi;
+        float psi = comp(q0.z, c);
+        bv = cpml(bv, psi, azi, bzi);
+        set_comp(q0.z, c, psi);
       }
       set_comp(ox, c, fadd(comp(CELL(c_vx, rr), c), fmul(fmul(G.dt, comp(CELL(c_irx, rr), c)), fadd(av, bv))));
     }
     st4(vx + g, ox);
+    if (sz >= 0) st4(psz0 + (size_t)sz * G.ld + j, q0.z);
     // vz: vz_dsxz (x, D⁻ of σxz) + vz_dszz (z, D⁺ of σzz)
     {
       float v[12];
@@ -690,16 +741,18 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
       if (!C.ok[c]) continue;
       float av = a[c], bv = b[c];
       if (C.sx[c] >= 0) {
-        float* ps = psx1 + (size_t)i * G.wx + C.sx[c];
-        float psi = *ps; av = cpml(av, psi, C.ax[c], C.bx[c]); *ps = psi;
+        av = cpml(av, q1.x[c], C.ax[c], C.bx[c]);
+        psx1[(size_t)i * G.wx + C.sx[c]] = q1.x[c];
       }
       if (sz >= 0) {
-        float* ps = psz1 + (size_t)sz * G.ld + j + c;
-        float psi = *ps; bv = cpml(bv, psi, azi, bzi); *ps = psi;
+        float psi = comp(q1.z, c);
+        bv = cpml(bv, psi, azi, bzi);
+        set_comp(q1.z, c, psi);
       }
       set_comp(oz, c, fadd(comp(CELL(c_vz, rr), c), fmul(fmul(G.dt, comp(CELL(c_irz, rr), c)), fadd(av, bv))));
     }
     st4(vz + g, oz);
+    if (sz >= 0) st4(psz1 + (size_t)sz * G.ld + j, q1.z);
   }
   }
 }
@@ -783,29 +836,28 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
       row12(svx + ro, v);
       col9<M>(svz + ro + 4, z);
       float4 out, epsv;
+      float inc[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const float div = fadd(G.dxf(sum_minus<M>(v, 4 + c, G.c)), G.dzf(sum_minus<M>(z[c], M, G.c)));
-        float pv;
         if constexpr (!VISCO) {
-          pv = fadd(comp(CELL(c_a, rr), c), fmul(fmul(G.dt, comp(CELL(c_b, rr), c)), div));
+          set_comp(out, c, fadd(comp(CELL(c_a, rr), c), fmul(fmul(G.dt, comp(CELL(c_b, rr), c)), div)));
         } else {
-          const float inc = fmul(G.dt, div);
-          const float e = fadd(comp(CELL(c_a, rr), c), inc);
-          float total = 0.f;
-          const int q = qidx[g + c];
-          for (int l = 0; l < nL; ++l) {
-            float* rl = r0 + l * fstride;
-            const float rv = fadd(fmul(rl[g + c], __ldg(relax_a + q * nL + l)),
-                                  fmul(__ldg(b0 + l * fstride + g + c), inc));
-            rl[g + c] = rv;
-            total = (l == 0) ? rv : fadd(total, rv);
-          }
-          pv = fadd(fmul(comp(CELL(c_b, rr), c), e), total);
+          inc[c] = fmul(G.dt, div);
+        }
+      }
+      if constexpr (VISCO) {
+        const bool keep[4] = {false, false, false, false};
+        float tot[4];
+        relax4(r0, b0, fstride, qidx, relax_a, nL, g, inc, keep, tot);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float e = fadd(comp(CELL(c_a, rr), c), inc[c]);
+          const float pv = fadd(fmul(comp(CELL(c_b, rr), c), e), tot[c]);
           set_comp(epsv, c, e);
+          set_comp(out, c, pv);
           peak = fmaxf(peak, fabsf(pv));
         }
-        set_comp(out, c, pv);
       }
       st4(p + g, out);
       if constexpr (VISCO) st4(eps + g, epsv);
@@ -838,47 +890,52 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
       }
       float4 out = CELL(c_a, rr);
       float4 epsv = out;
+      PsiCells q = psi_cells(C, psx, i, G.wx, psz, sz, G.ld, j);
+      float inc[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
+        inc[c] = 0.f;
         if (!C.ok[c]) continue;
         const int jc = j + c;
         float ddx = dx[c], ddz = dz[c];
         if (C.sx[c] >= 0) {
-          float* ps = psx + (size_t)i * G.wx + C.sx[c];
-          float psi = *ps; ddx = cpml(ddx, psi, C.ax[c], C.bx[c]); *ps = psi;
+          ddx = cpml(ddx, q.x[c], C.ax[c], C.bx[c]);
+          psx[(size_t)i * G.wx + C.sx[c]] = q.x[c];
         }
         if (sz >= 0) {
-          float* ps = psz + (size_t)sz * G.ld + jc;
-          float psi = *ps; ddz = cpml(ddz, psi, azi, bzi); *ps = psi;
+          float psi = comp(q.z, c);
+          ddz = cpml(ddz, psi, azi, bzi);
+          set_comp(q.z, c, psi);
         }
         const float div = fadd(ddx, ddz);
-        const bool src = (i == G.src_iz && jc == G.src_ix && amp != 0.f);
-        float pv;
         if constexpr (!VISCO) {
-          pv = fadd(comp(CELL(c_a, rr), c), fmul(fmul(G.dt, comp(CELL(c_b, rr), c)), div));
+          const bool src = (i == G.src_iz && jc == G.src_ix && amp != 0.f);
+          float pv = fadd(comp(CELL(c_a, rr), c), fmul(fmul(G.dt, comp(CELL(c_b, rr), c)), div));
           if (src) pv = fadd(pv, amp);
           if (G.free_surface && i == G.pad) pv = 0.f;
+          set_comp(out, c, pv);
         } else {
-          const float inc = fmul(G.dt, div);
-          float e = fadd(comp(CELL(c_a, rr), c), inc);
-          float total = 0.f;
-          const int q = qidx[g + c];
-          for (int l = 0; l < nL; ++l) {
-            float* rl = r0 + l * fstride;
-            const float rv = fadd(fmul(rl[g + c], __ldg(relax_a + q * nL + l)),
-                                  fmul(__ldg(b0 + l * fstride + g + c), inc));
-            rl[g + c] = rv;
-            total = (l == 0) ? rv : fadd(total, rv);
-          }
-          pv = fadd(fmul(comp(CELL(c_b, rr), c), e), total);
-          if (src) {
+          inc[c] = fmul(G.dt, div);
+        }
+      }
+      if (sz >= 0) st4(psz + (size_t)sz * G.ld + j, q.z);
+      if constexpr (VISCO) {
+        const bool keep[4] = {!C.ok[0], !C.ok[1], !C.ok[2], !C.ok[3]};
+        float tot[4];
+        relax4(r0, b0, fstride, qidx, relax_a, nL, g, inc, keep, tot);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (!C.ok[c]) continue;
+          float e = fadd(comp(CELL(c_a, rr), c), inc[c]);
+          float pv = fadd(fmul(comp(CELL(c_b, rr), c), e), tot[c]);
+          if (i == G.src_iz && j + c == G.src_ix && amp != 0.f) {
             e = fadd(e, amp_eps);
             pv = fadd(pv, amp);
           }
           set_comp(epsv, c, e);
+          set_comp(out, c, pv);
           peak = fmaxf(peak, fabsf(pv));
         }
-        set_comp(out, c, pv);
       }
       st4(p + g, out);
       if constexpr (VISCO) st4(eps + g, epsv);
@@ -1042,6 +1099,8 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
       }
       float4 oxx = CELL(c_xx, rr), ozz = CELL(c_zz, rr), oxz = CELL(c_xz, rr);
       float4 pv4 = make_float4(0.f, 0.f, 0.f, 0.f), sv4 = pv4;
+      PsiCells q2 = psi_cells(C, psx2, i, G.wx, psz2, sz, G.ld, j);
+      PsiCells q3 = psi_cells(C, psx3, i, G.wx, psz3, sz, G.ld, j);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (!C.ok[c]) continue;
@@ -1049,16 +1108,19 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
         const float exx_raw = exx[c], ezz_raw = ezz[c];
         float ex = exx_raw, ez = ezz_raw, g1 = f1[c], g2 = f2[c];
         if (C.sx[c] >= 0) {
-          float* p0 = psx2 + (size_t)i * G.wx + C.sx[c];
-          float psi = *p0; ex = cpml(ex, psi, C.ax[c], C.bx[c]); *p0 = psi;
-          float* p1 = psx3 + (size_t)i * G.wx + C.sx[c];
-          psi = *p1; g2 = cpml(g2, psi, C.ax[c], C.bx[c]); *p1 = psi;
+          const size_t xo = (size_t)i * G.wx + C.sx[c];
+          ex = cpml(ex, q2.x[c], C.ax[c], C.bx[c]);
+          psx2[xo] = q2.x[c];
+          g2 = cpml(g2, q3.x[c], C.ax[c], C.bx[c]);
+          psx3[xo] = q3.x[c];
         }
         if (sz >= 0) {
-          float* p0 = psz2 + (size_t)sz * G.ld + jc;
-          float psi = *p0; ez = cpml(ez, psi, azi, bzi); *p0 = psi;
-          float* p1 = psz3 + (size_t)sz * G.ld + jc;
-          psi = *p1; g1 = cpml(g1, psi, azi, bzi); *p1 = psi;
+          float psi = comp(q2.z, c);
+          ez = cpml(ez, psi, azi, bzi);
+          set_comp(q2.z, c, psi);
+          psi = comp(q3.z, c);
+          g1 = cpml(g1, psi, azi, bzi);
+          set_comp(q3.z, c, psi);
         }
         const float lam = comp(CELL(c_lam, rr), c), l2m = comp(CELL(c_l2m, rr), c);
         float vxx = fadd(comp(CELL(c_xx, rr), c), fmul(G.dt, fadd(fmul(l2m, ex), fmul(lam, ez))));
@@ -1091,6 +1153,10 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
       st4(sxx + g, oxx);
       st4(szz + g, ozz);
       st4(sxz + g, oxz);
+      if (sz >= 0) {
+        st4(psz2 + (size_t)sz * G.ld + j, q2.z);
+        st4(psz3 + (size_t)sz * G.ld + j, q3.z);
+      }
       if (epi) {
         st4(e_p + rr * 32 + 4 * threadIdx.x, pv4);
         st4(e_s + rr * 32 + 4 * threadIdx.x, sv4);
