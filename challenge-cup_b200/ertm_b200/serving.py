@@ -28,6 +28,7 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
+import queue
 import threading
 import time
 from concurrent.futures import Future
@@ -154,6 +155,8 @@ class RTMServer:
                                       "peak_active": 0, "ticks": 0}
         self.shot_latencies: list[float] = []
         self.job_latencies: list[float] = []
+        self._prefit_jobs: queue.Queue = queue.Queue()
+        self._prefit_thread: threading.Thread | None = None
 
     # ------------------------------------------------------------------ API
     def start(self) -> "RTMServer":
@@ -161,6 +164,8 @@ class RTMServer:
             self._stop = False
             self._thread = threading.Thread(target=self._run, name="ertm-serve", daemon=True)
             self._thread.start()
+            self._prefit_thread = threading.Thread(target=self._prefit_loop, name="ertm-prefit", daemon=True)
+            self._prefit_thread.start()
         return self
 
     def submit(self, job: ServeJob) -> Future:
@@ -172,6 +177,9 @@ class RTMServer:
             self._next_id += 1
             self._queue.append(js)
             self._cv.notify()
+        solver = getattr(job.imager, "solver_config", None)
+        if str(getattr(solver, "engine", "")) == "viscoacoustic":
+            self._prefit_jobs.put(job)
         return fut
 
     def stop(self, timeout: float | None = None) -> None:
@@ -182,6 +190,10 @@ class RTMServer:
         if self._thread is not None:
             self._thread.join(timeout)
             self._thread = None
+        if self._prefit_thread is not None:
+            self._prefit_jobs.put(None)
+            self._prefit_thread.join(timeout)
+            self._prefit_thread = None
 
     def __enter__(self) -> "RTMServer":
         return self.start()
@@ -198,6 +210,21 @@ class RTMServer:
         return s
 
     # ------------------------------------------------------------- the loop
+    def _prefit_loop(self) -> None:
+        """Host-only work ahead of admission: the GSLS fits of queued
+        viscoacoustic jobs (memoised), done while the device runs other
+        shots, so that building their propagators later finds them ready."""
+        from .viscoelastic import prefit
+        while True:
+            job = self._prefit_jobs.get()
+            if job is None:
+                return
+            try:
+                q = job.imager.q_config
+                prefit(job.model.qp, float(q.f_ref), int(q.n_mechanisms), float(q.band_ratio))
+            except Exception:       # the serving loop reports any error when it builds the shot
+                pass
+
     def _run(self) -> None:
         handle = C.c_void_p()
         try:

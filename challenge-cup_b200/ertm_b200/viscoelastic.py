@@ -9,6 +9,9 @@ tables the CUDA kernels index.  The per-cell coefficient expansion
 
 from __future__ import annotations
 
+import copy
+import threading
+
 from dataclasses import dataclass, field
 from typing import Iterable
 
@@ -65,9 +68,27 @@ def _single_mechanism(q: float, f_ref: float) -> tuple[float, float]:
     return float(u / (2.0 * np.pi * f_ref)), float(1.0 - u * u)
 
 
+_FIT_CACHE: dict[tuple, GSLSParameters] = {}
+_FIT_LOCK = threading.Lock()
+
+
 def fit_gsls(q: float, f_ref: float, *, n_mechanisms: int = 3, band_ratio: float = 1.5,
              min_q: float = 2.0) -> GSLSParameters:
-    """Least-squares constant-Q fit over [f_ref/band, f_ref·band] in log Q."""
+    """Least-squares constant-Q fit over [f_ref/band, f_ref·band] in log Q.
+
+    The fit is a pure function of its arguments and takes ~0.1 s, so results
+    are memoised per process (a copy is returned each time)."""
+    key = (float(q), float(f_ref), int(n_mechanisms), float(band_ratio), float(min_q))
+    with _FIT_LOCK:
+        hit = _FIT_CACHE.get(key)
+    if hit is None:
+        hit = _fit_gsls(*key)
+        with _FIT_LOCK:
+            _FIT_CACHE[key] = hit
+    return copy.deepcopy(hit)
+
+
+def _fit_gsls(q: float, f_ref: float, n_mechanisms: int, band_ratio: float, min_q: float) -> GSLSParameters:
     if q <= min_q:
         raise ERTMError(f"GSLS fit needs Q > {min_q}, got {q}")
     if f_ref <= 0:
@@ -118,6 +139,18 @@ class RelaxationTables:
     alpha_mechanisms: tuple[float, ...] = ()
     f_peak_mechanisms: tuple[float, ...] = ()
     extra: dict = field(default_factory=dict)
+
+
+def distinct_q(qp: np.ndarray) -> np.ndarray:
+    """The distinct clipped Q values a viscoacoustic model is fitted for."""
+    return np.unique(np.clip(np.asarray(qp, dtype=np.float64).ravel(), 2.5, 1.0e5))
+
+
+def prefit(qp: np.ndarray, f_ref: float, n_mechanisms: int, band_ratio: float) -> None:
+    """Fit (and memoise) every distinct Q of a model ahead of propagator set-up."""
+    for qv in distinct_q(qp)[:33]:
+        if qv <= 1.0e4:
+            fit_gsls(float(qv), f_ref, n_mechanisms=n_mechanisms, band_ratio=band_ratio)
 
 
 def relaxation_tables(qp_padded: np.ndarray, dt: float, nt: int, *, f_ref: float, n_mechanisms: int,
