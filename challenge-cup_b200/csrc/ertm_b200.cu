@@ -469,20 +469,37 @@ struct SplitStreams {
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 
-SplitStreams& split_streams() {
+// Per device: stream pairs for the lanes of a batched tick (lane 0 runs on
+// the caller's stream; lane k > 0 on its own stream) and, per lane, the side
+// stream of its boundary-frame launches.
+constexpr int kLanes = 2;
+struct LaneStreams {
+  SplitStreams split[kLanes];          // frame-launch side streams, per lane
+  cudaStream_t lane[kLanes] = {};      // lane streams (lane[0] unused: the caller's)
+  cudaEvent_t fork[kLanes] = {}, join[kLanes] = {};
+};
+
+LaneStreams& lane_streams() {
   static std::mutex mu;
-  static std::map<int, SplitStreams> per_device;
+  static std::map<int, LaneStreams> per_device;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  SplitStreams& s = per_device[dev];
-  if (!s.side) {
-    CK(cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
+  LaneStreams& s = per_device[dev];
+  if (!s.split[0].side) {
+    for (int k = 0; k < kLanes; ++k) {
+      CK(cudaStreamCreateWithFlags(&s.split[k].side, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&s.split[k].fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&s.split[k].join, cudaEventDisableTiming));
+      if (k > 0) CK(cudaStreamCreateWithFlags(&s.lane[k], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&s.fork[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&s.join[k], cudaEventDisableTiming));
+    }
   }
   return s;
 }
+
+SplitStreams& split_streams(int lane = 0) { return lane_streams().split[lane]; }
 
 // Interior tiles in their own launches: the straight-line kernels then carry
 // none of the boundary code's registers (more resident warps per SM).  The
@@ -490,8 +507,8 @@ SplitStreams& split_streams() {
 // with the interior launch; the two join before the next phase.
 template <int M, int BZ, int R, class WS>
 void launch_step_split(int engine, const DevProp* d, const WS& inner, int n_in, const WS& frame, int n_fr,
-                       cudaStream_t st) {
-  SplitStreams& ss = split_streams();
+                       cudaStream_t st, int lane) {
+  SplitStreams& ss = split_streams(lane);
   for (int phase = 0; phase < 2; ++phase) {
     CK(cudaEventRecord(ss.fork, st));
     CK(cudaStreamWaitEvent(ss.side, ss.fork, 0));
@@ -561,7 +578,7 @@ std::atomic<int> g_tile_split{0};   // 0 automatic, 1 never, 2 whenever there ar
 // per phase over every tile.
 template <class WS>
 void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, const DevProp* const* hosts,
-                  cudaStream_t st) {
+                  cudaStream_t st, int lane = 0) {
   int total = 0;
   for (int k = 0; k < n; ++k) total += ws_work(ws, k).tiles;
   const int split_mode = g_tile_split.load();
@@ -585,9 +602,9 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
     if (n_in > 0 && (n_in >= kSplitMinTiles || split_mode == 2)) {
       ws_count(inner, ki);
       ws_count(frame, kf);
-      if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st);
-      else if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st);
-      else launch_step_split<4, 8, 1>(engine, d, inner, n_in, frame, n_fr, st);
+      if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st, lane);
+      else if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st, lane);
+      else launch_step_split<4, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane);
       return;
     }
   }
@@ -1228,6 +1245,12 @@ struct TickItem {
   Epilogue epi;      // the epilogue (fused into w, or stand-alone)
 };
 
+std::atomic<int> g_tick_lanes{0};   // 0 automatic, 1 or 2 lanes
+
+// One (engine, order) group of a tick.  Large groups run as two lanes (the
+// works alternate between them, each lane on its own stream): the stress
+// phase of one lane, bound by the latency of its epilogue loads, then
+// overlaps the velocity phase of the other, bound by instruction issue.
 void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStream_t st, double& bytes) {
   if (items.empty()) return;
   const Prop& P0 = items[0]->fwd ? *items[0]->run->F : *items[0]->run->B;
@@ -1242,22 +1265,36 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
       t8 += tiles_for(P.h, 8);
     }
     const int tz = choose_tz(M, 0, t32, t16, t8);
-    WorkSetB ws{};
-    ws.n = (int)(c1 - c0);
-    int tile0 = 0;
-    const DevProp* hosts[MAX_BATCH_WORKS];
+    const int lanes_mode = g_tick_lanes.load();
+    const int64_t total = tz == 32 ? t32 : (tz == 16 ? t16 : t8);
+    const int lanes = (lanes_mode == 2 || (lanes_mode == 0 && c1 - c0 >= 4 && total >= 4 * kSplitMinTiles))
+                          ? 2 : 1;
+    WorkSetB ws[kLanes]{};
+    int tile0[kLanes] = {0, 0};
+    const DevProp* hosts[kLanes][MAX_BATCH_WORKS];
     for (size_t k = c0; k < c1; ++k) {
       const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
+      const int l = lanes == 2 ? (int)((k - c0) & 1) : 0;
       StepWork w = items[k]->w;
-      w.tile0 = tile0;
+      w.tile0 = tile0[l];
       w.tiles_x = (P.h.nxp + TILE_X - 1) / TILE_X;
       w.tiles = tiles_for(P.h, tz);
-      tile0 += w.tiles;
-      ws.w[k - c0] = w;
-      hosts[k - c0] = &P.h;
+      tile0[l] += w.tiles;
+      hosts[l][ws[l].n] = &P.h;
+      ws[l].w[ws[l].n++] = w;
       bytes += step_bytes(P) + epilogue_bytes(w.epi, (size_t)P.h.nz * P.h.nx);
     }
-    launch_works(M, tz, engine, table, ws, ws.n, hosts, st);
+    if (lanes == 1) {
+      launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st);
+      continue;
+    }
+    LaneStreams& ls = lane_streams();
+    CK(cudaEventRecord(ls.fork[1], st));
+    CK(cudaStreamWaitEvent(ls.lane[1], ls.fork[1], 0));
+    launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0);
+    launch_works(M, tz, engine, table, ws[1], ws[1].n, hosts[1], ls.lane[1], 1);
+    CK(cudaEventRecord(ls.join[1], ls.lane[1]));
+    CK(cudaStreamWaitEvent(st, ls.join[1], 0));
   }
 }
 
@@ -1537,6 +1574,13 @@ int32_t ertm_set_tile_split(int32_t mode) {
   return guarded([&] {
     REQUIRE(mode >= 0 && mode <= 2, "tile split mode must be 0 (automatic), 1 (never) or 2 (always)");
     g_tile_split.store(mode);
+  });
+}
+
+int32_t ertm_set_tick_lanes(int32_t lanes) {
+  return guarded([&] {
+    REQUIRE(lanes >= 0 && lanes <= 2, "tick lanes must be 0 (automatic), 1 or 2");
+    g_tick_lanes.store(lanes);
   });
 }
 

@@ -2,7 +2,7 @@
 the process, for ncu launch lists and kernel captures.
 
     PYTHONPATH=challenge-cup_b200 python -m ertm_b200.profiling \\
-        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--save x.npy]
+        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--save x.npy]
 
 The job is what ``bench.py`` times: every shot of the workload migrated
 (batched lockstep ticks, or one shot at a time with ``--path plain``) and the
@@ -32,6 +32,7 @@ def main(argv=None) -> None:
     ap.add_argument("--tile-rows", type=int, default=0, help="stencil tile height 8/16/32 (0: automatic)")
     ap.add_argument("--split", type=int, default=0,
                     help="interior tiles in launches of their own: 0 automatic, 1 never, 2 always")
+    ap.add_argument("--lanes", type=int, default=0, help="batched ticks in 1 or 2 stream lanes (0: automatic)")
     ap.add_argument("--save", default=None, help="write the stacked images of the last repeat (.npy)")
     args = ap.parse_args(argv)
 
@@ -45,6 +46,7 @@ def main(argv=None) -> None:
     L = _lib.lib(0)
     _lib.check(L.ertm_set_tile_rows(args.tile_rows), "tile rows")
     _lib.check(L.ertm_set_tile_split(args.split), "tile split")
+    _lib.check(L.ertm_set_tick_lanes(args.lanes), "tick lanes")
     wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt, **({"n_shots": args.shots} if args.shots else {}))
     imager, solver = workloads.imager_for(wl)
     shots = workloads.synthesize(wl, solver, wl.sources)

@@ -125,6 +125,10 @@ int32_t ertm_set_tile_rows(int32_t rows);
  * alone fill the GPU (default), 1 = never, 2 = whenever there are any.  The
  * results are the same either way; the knob is for tuning and tests. */
 int32_t ertm_set_tile_split(int32_t mode);
+/* Batched ticks: the works of a large (engine, order) group in one lane or
+ * alternated over two lanes on separate streams (0 = automatic: two when the
+ * group has at least 4 works and enough tiles).  Results are identical. */
+int32_t ertm_set_tick_lanes(int32_t lanes);
 /* Count, over all 2^32 float inputs a, where the fast division form `mode`
  * (3 one-FMA, 2 FMA correction, 1 float64 product) differs in value from
  * __fdiv_rn(a, h) (no reference counterpart; diagnostics). */

@@ -97,28 +97,36 @@ def run_shot(args) -> dict:
             "migrate_s": time.perf_counter() - t1}
 
 
+def save(config: str, results: list[dict]) -> None:
+    import oracle as orc
+    shots, step, stack, over = CASES[config]
+    rs = sorted(results, key=lambda r: r["k"])
+    modes = sorted({m for r in rs for m in r["images"]})
+    meta = {"shots": shots, "step": step, "stacked": stack, "modes": modes, "overrides": over,
+            "forward_s": [r["forward_s"] for r in rs], "migrate_s": [r["migrate_s"] for r in rs]}
+    out = {}
+    for m in modes:
+        if stack:
+            imgs = [r["images"][m] for r in rs]
+            out[m] = orc.stack_images(imgs, normalize=True)[::step, ::step].astype(np.float32)
+        else:
+            for r in rs:
+                if m in r["images"]:
+                    out[f"{m}_{r['k']}"] = r["images"][m][::step, ::step].astype(np.float32)
+    np.savez_compressed(HERE / f"{config}.npz", meta=json.dumps(meta), **out)
+    print(config, json.dumps(meta), flush=True)
+
+
 def main(configs) -> None:
     _paths()
-    import oracle as orc
     tasks = [(c, k) for c in configs for k in range(len(CASES[c][0]))]
     ctx = mp.get_context("spawn")
+    done: dict[str, list] = {c: [] for c in configs}
     with ctx.Pool(min(len(tasks), mp.cpu_count())) as pool:
-        results = pool.map(run_shot, tasks, chunksize=1)
-    for c in configs:
-        shots, step, stack, over = CASES[c]
-        rs = sorted((r for r in results if r["config"] == c), key=lambda r: r["k"])
-        modes = list(rs[0]["images"])
-        out, meta = {}, {"shots": shots, "step": step, "stacked": stack, "modes": modes, "overrides": over,
-                         "forward_s": [r["forward_s"] for r in rs], "migrate_s": [r["migrate_s"] for r in rs]}
-        for m in modes:
-            imgs = [r["images"][m] for r in rs]
-            if stack:
-                out[m] = orc.stack_images(imgs, normalize=True)[::step, ::step].astype(np.float32)
-            else:
-                for k, im in enumerate(imgs):
-                    out[f"{m}_{k}"] = im[::step, ::step].astype(np.float32)
-        np.savez_compressed(HERE / f"{c}.npz", meta=json.dumps(meta), **out)
-        print(c, json.dumps(meta), flush=True)
+        for r in pool.imap_unordered(run_shot, tasks):
+            done[r["config"]].append(r)
+            if len(done[r["config"]]) == len(CASES[r["config"]][0]):
+                save(r["config"], done[r["config"]])
 
 
 if __name__ == "__main__":

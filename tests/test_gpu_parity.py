@@ -272,7 +272,8 @@ def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, b
 
 def test_batched_images_equal_with_and_without_split_launches(eb):
     """The batched migration gives the same images whether interior tiles run
-    in launches of their own or with the boundary tiles."""
+    in launches of their own or with the boundary tiles, and whether a tick's
+    works run in one stream lane or two."""
     from ertm_b200 import ImagingConfig, RTMImager, SolverConfig, _lib
     from ertm_b200.batch import BatchMigrator
     from ertm_b200.propagation import PropagationSpec, forward_shot
@@ -290,12 +291,15 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
     imager = RTMImager(ImagingConfig(condition="normalized", checkpoint_mb=2.0),
                        SolverConfig(nt=260, dt=4e-4, boundary="free", engine="elastic"))
     out = {}
-    for mode in (1, 2):
+    for mode, lanes in ((1, 1), (2, 1), (2, 2), (1, 2)):
         _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
+        _lib.check(_lib.lib().ertm_set_tick_lanes(lanes), "lanes")
         try:
-            out[mode] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
+            out[mode, lanes] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
         finally:
             _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
-    for a, b in zip(out[1], out[2]):
-        for x1, x2 in zip(a, b):
-            assert np.array_equal(x1.image, x2.image), x1.mode
+            _lib.check(_lib.lib().ertm_set_tick_lanes(0), "lanes")
+    for key in ((2, 1), (2, 2), (1, 2)):
+        for a, b in zip(out[1, 1], out[key]):
+            for x1, x2 in zip(a, b):
+                assert np.array_equal(x1.image, x2.image), (key, x1.mode)
