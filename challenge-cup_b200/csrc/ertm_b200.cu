@@ -578,10 +578,10 @@ std::atomic<int> g_tile_split{0};   // 0 automatic, 1 never, 2 whenever there ar
 // per phase over every tile.
 template <class WS>
 void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, const DevProp* const* hosts,
-                  cudaStream_t st, int lane = 0) {
+                  cudaStream_t st, int lane = 0, int split_mode = -1) {
   int total = 0;
   for (int k = 0; k < n; ++k) total += ws_work(ws, k).tiles;
-  const int split_mode = g_tile_split.load();
+  if (split_mode < 0) split_mode = g_tile_split.load();
   if (split_mode != 1 && M == 4) {
     WS inner = ws, frame = ws;
     int n_in = 0, n_fr = 0, ki = 0, kf = 0;
@@ -1246,8 +1246,83 @@ struct TickItem {
 };
 
 std::atomic<int> g_tick_lanes{0};   // 0 automatic, 1 or 2 lanes
+std::atomic<int> g_autotune{1};     // tune batched tick launches online
 
-// One (engine, order) group of a tick.  Large groups run as two lanes (the
+// ---------------------------------------------------------------------------
+// Online autotuner for batched ticks.  A tick group (engine, order, number of
+// works, size class) runs its first ticks with each candidate launch shape in
+// turn — tile height 8/16/32, interior/frame split off/on, one or two lanes —
+// timed with CUDA events on the launching stream and read back as they
+// complete (no synchronisation); once every candidate has kTuneSamples
+// samples the fastest one is kept for the process.  Every candidate computes
+// the same results, so switching shapes between ticks is safe.
+// ---------------------------------------------------------------------------
+struct TuneCfg {
+  int tz, split, lanes;
+};
+constexpr int kTuneSamples = 3;
+
+struct TuneState {
+  std::vector<TuneCfg> cands;
+  std::vector<double> sum_ms;
+  std::vector<int> n;
+  int best = -1, next = 0, pending = 0;
+};
+
+struct TuneSample {
+  TuneState* ts;
+  int cand;
+  cudaEvent_t e0, e1;
+};
+
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int, int, int>, TuneState> g_tune;
+std::vector<TuneSample> g_tune_pending;
+std::vector<cudaEvent_t> g_tune_events;
+
+cudaEvent_t tune_event() {
+  if (!g_tune_events.empty()) {
+    cudaEvent_t e = g_tune_events.back();
+    g_tune_events.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+// Fold in the samples whose events have completed.
+void tune_collect() {
+  for (size_t k = 0; k < g_tune_pending.size();) {
+    TuneSample& t = g_tune_pending[k];
+    const cudaError_t q = cudaEventQuery(t.e1);
+    if (q == cudaErrorNotReady) {
+      ++k;
+      continue;
+    }
+    CK(q);
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, t.e0, t.e1));
+    TuneState& ts = *t.ts;
+    ts.sum_ms[t.cand] += ms;
+    ++ts.n[t.cand];
+    --ts.pending;
+    g_tune_events.push_back(t.e0);
+    g_tune_events.push_back(t.e1);
+    g_tune_pending[k] = g_tune_pending.back();
+    g_tune_pending.pop_back();
+    bool all = ts.best < 0;
+    for (size_t c = 0; all && c < ts.cands.size(); ++c) all = ts.n[c] >= kTuneSamples;
+    if (all) {
+      int b = 0;
+      for (size_t c = 1; c < ts.cands.size(); ++c)
+        if (ts.sum_ms[c] / ts.n[c] < ts.sum_ms[b] / ts.n[b]) b = (int)c;
+      ts.best = b;
+    }
+  }
+}
+
+// One (engine, order) group of a tick.  Large groups may run as two lanes (the
 // works alternate between them, each lane on its own stream): the stress
 // phase of one lane, bound by the latency of its epilogue loads, then
 // overlaps the velocity phase of the other, bound by instruction issue.
@@ -1257,18 +1332,51 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
   const int M = P0.M, engine = P0.h.engine;
   for (size_t c0 = 0; c0 < items.size(); c0 += MAX_BATCH_WORKS) {
     const size_t c1 = std::min(items.size(), c0 + MAX_BATCH_WORKS);
-    int64_t t32 = 0, t16 = 0, t8 = 0;
+    int64_t t32 = 0, t16 = 0, t8 = 0, cells = 0;
     for (size_t k = c0; k < c1; ++k) {
       const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
       t32 += tiles_for(P.h, 32);
       t16 += tiles_for(P.h, 16);
       t8 += tiles_for(P.h, 8);
+      cells += (int64_t)P.h.nzp * P.h.nxp;
     }
-    const int tz = choose_tz(M, 0, t32, t16, t8);
-    const int lanes_mode = g_tick_lanes.load();
-    const int64_t total = tz == 32 ? t32 : (tz == 16 ? t16 : t8);
-    const int lanes = (lanes_mode == 2 || (lanes_mode == 0 && c1 - c0 >= 4 && total >= 4 * kSplitMinTiles))
-                          ? 2 : 1;
+    // heuristic shape, or the autotuner's choice
+    TuneCfg cfg{choose_tz(M, 0, t32, t16, t8), g_tile_split.load(), 0};
+    {
+      const int lanes_mode = g_tick_lanes.load();
+      const int64_t total = cfg.tz == 32 ? t32 : (cfg.tz == 16 ? t16 : t8);
+      cfg.lanes = (lanes_mode == 2 || (lanes_mode == 0 && c1 - c0 >= 4 && total >= 3 * kSplitMinTiles)) ? 2 : 1;
+    }
+    TuneState* ts = nullptr;
+    int cand = -1;
+    const bool forced = g_tile_rows.load() != 0 || g_tile_split.load() != 0 || g_tick_lanes.load() != 0;
+    if (M == 4 && g_autotune.load() && !forced && t16 >= kSplitMinTiles / 4) {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      tune_collect();
+      int lg = 0;
+      while ((int64_t(1) << (lg + 1)) <= cells) ++lg;
+      ts = &g_tune[{engine, M, (int)(c1 - c0), lg, 0}];
+      if (ts->cands.empty()) {
+        for (int tz : {16, 32, 8})
+          for (int split : {1, 2})
+            for (int lanes : {1, 2}) {
+              if (lanes == 2 && c1 - c0 < 2) continue;
+              ts->cands.push_back({tz, split, lanes});
+            }
+        ts->sum_ms.assign(ts->cands.size(), 0.0);
+        ts->n.assign(ts->cands.size(), 0);
+      }
+      if (ts->best >= 0) {
+        cfg = ts->cands[ts->best];
+      } else if (ts->pending < 8) {
+        // the candidate with the fewest samples (counting those in flight)
+        cand = ts->next;
+        ts->next = (ts->next + 1) % (int)ts->cands.size();
+        cfg = ts->cands[cand];
+      }
+    }
+    const int tz = cfg.tz;
+    const int lanes = cfg.lanes;
     WorkSetB ws[kLanes]{};
     int tile0[kLanes] = {0, 0};
     const DevProp* hosts[kLanes][MAX_BATCH_WORKS];
@@ -1284,17 +1392,30 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
       ws[l].w[ws[l].n++] = w;
       bytes += step_bytes(P) + epilogue_bytes(w.epi, (size_t)P.h.nz * P.h.nx);
     }
-    if (lanes == 1) {
-      launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st);
-      continue;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cand >= 0) {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      e0 = tune_event();
+      e1 = tune_event();
+      CK(cudaEventRecord(e0, st));
     }
-    LaneStreams& ls = lane_streams();
-    CK(cudaEventRecord(ls.fork[1], st));
-    CK(cudaStreamWaitEvent(ls.lane[1], ls.fork[1], 0));
-    launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0);
-    launch_works(M, tz, engine, table, ws[1], ws[1].n, hosts[1], ls.lane[1], 1);
-    CK(cudaEventRecord(ls.join[1], ls.lane[1]));
-    CK(cudaStreamWaitEvent(st, ls.join[1], 0));
+    if (lanes == 1) {
+      launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0, cfg.split);
+    } else {
+      LaneStreams& ls = lane_streams();
+      CK(cudaEventRecord(ls.fork[1], st));
+      CK(cudaStreamWaitEvent(ls.lane[1], ls.fork[1], 0));
+      launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0, cfg.split);
+      launch_works(M, tz, engine, table, ws[1], ws[1].n, hosts[1], ls.lane[1], 1, cfg.split);
+      CK(cudaEventRecord(ls.join[1], ls.lane[1]));
+      CK(cudaStreamWaitEvent(st, ls.join[1], 0));
+    }
+    if (cand >= 0) {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      CK(cudaEventRecord(e1, st));
+      g_tune_pending.push_back({ts, cand, e0, e1});
+      ++ts->pending;
+    }
   }
 }
 
@@ -1582,6 +1703,43 @@ int32_t ertm_set_tick_lanes(int32_t lanes) {
     REQUIRE(lanes >= 0 && lanes <= 2, "tick lanes must be 0 (automatic), 1 or 2");
     g_tick_lanes.store(lanes);
   });
+}
+
+int32_t ertm_set_autotune(int32_t enable) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_autotune.store(enable > 0 ? 1 : 0);
+    if (enable < 0) {                 // forget earlier choices (and keep tuning off)
+      for (TuneSample& t : g_tune_pending) {
+        CK(cudaEventSynchronize(t.e1));
+        g_tune_events.push_back(t.e0);
+        g_tune_events.push_back(t.e1);
+      }
+      g_tune_pending.clear();
+      g_tune.clear();
+    }
+  });
+}
+
+const char* ertm_autotune_report(void) {
+  static std::string report;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  tune_collect();
+  report.clear();
+  for (auto& kv : g_tune) {
+    const TuneState& ts = kv.second;
+    char line[256];
+    std::snprintf(line, sizeof line, "engine %d order %d works %d cells 2^%d:", std::get<0>(kv.first),
+                  2 * std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first));
+    report += line;
+    for (size_t c = 0; c < ts.cands.size(); ++c) {
+      std::snprintf(line, sizeof line, " %s%d/%d/%d=%.1fus", (int)c == ts.best ? "*" : "", ts.cands[c].tz,
+                    ts.cands[c].split, ts.cands[c].lanes, ts.n[c] ? 1e3 * ts.sum_ms[c] / ts.n[c] : -1.0);
+      report += line;
+    }
+    report += "\n";
+  }
+  return report.c_str();
 }
 
 int32_t ertm_profile_stencil(int32_t enable, int32_t every) {

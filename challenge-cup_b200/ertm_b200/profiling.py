@@ -2,7 +2,7 @@
 the process, for ncu launch lists and kernel captures.
 
     PYTHONPATH=challenge-cup_b200 python -m ertm_b200.profiling \\
-        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--save x.npy]
+        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--autotune 1] [--save x.npy]
 
 The job is what ``bench.py`` times: every shot of the workload migrated
 (batched lockstep ticks, or one shot at a time with ``--path plain``) and the
@@ -33,6 +33,7 @@ def main(argv=None) -> None:
     ap.add_argument("--split", type=int, default=0,
                     help="interior tiles in launches of their own: 0 automatic, 1 never, 2 always")
     ap.add_argument("--lanes", type=int, default=0, help="batched ticks in 1 or 2 stream lanes (0: automatic)")
+    ap.add_argument("--autotune", type=int, default=1, help="online autotuning of batched ticks (1 on, 0 off)")
     ap.add_argument("--save", default=None, help="write the stacked images of the last repeat (.npy)")
     args = ap.parse_args(argv)
 
@@ -47,6 +48,7 @@ def main(argv=None) -> None:
     _lib.check(L.ertm_set_tile_rows(args.tile_rows), "tile rows")
     _lib.check(L.ertm_set_tile_split(args.split), "tile split")
     _lib.check(L.ertm_set_tick_lanes(args.lanes), "tick lanes")
+    _lib.check(L.ertm_set_autotune(args.autotune), "autotune")
     wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt, **({"n_shots": args.shots} if args.shots else {}))
     imager, solver = workloads.imager_for(wl)
     shots = workloads.synthesize(wl, solver, wl.sources)
@@ -100,7 +102,8 @@ def main(argv=None) -> None:
                       "stencil_us_per_tick": tot.value / ticks * 1e3, "bytes_per_tick": byt.value / ticks,
                       "timed_ticks": int(cnt.value),
                       "achieved_gbs": byt.value / (tot.value * 1e-3) / 1e9 if tot.value > 0 else None,
-                      "checksum": float(out.double().abs().sum().item())}), flush=True)
+                      "checksum": float(out.double().abs().sum().item()),
+                      "autotune": L.ertm_autotune_report().decode().strip().splitlines()}), flush=True)
 
 
 if __name__ == "__main__":

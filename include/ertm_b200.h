@@ -129,6 +129,15 @@ int32_t ertm_set_tile_split(int32_t mode);
  * alternated over two lanes on separate streams (0 = automatic: two when the
  * group has at least 4 works and enough tiles).  Results are identical. */
 int32_t ertm_set_tick_lanes(int32_t lanes);
+/* Online autotuning of batched ticks (default on): the first ticks of each
+ * group shape (engine, order, works, size class) try tile heights 8/16/32,
+ * split off/on and one or two lanes, timed with CUDA events; the fastest is
+ * kept for the process.  Any forced knob above disables it.  1 = on, 0 = off,
+ * −1 = off and forget the choices made so far.  Results do not depend on it. */
+int32_t ertm_set_autotune(int32_t enable);
+/* One line per tuned group: each candidate tile height / split / lanes with
+ * its mean tick time; the chosen one is starred.  Valid until the next call. */
+const char* ertm_autotune_report(void);
 /* Count, over all 2^32 float inputs a, where the fast division form `mode`
  * (3 one-FMA, 2 FMA correction, 1 float64 product) differs in value from
  * __fdiv_rn(a, h) (no reference counterpart; diagnostics). */

@@ -303,3 +303,36 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
         for a, b in zip(out[1, 1], out[key]):
             for x1, x2 in zip(a, b):
                 assert np.array_equal(x1.image, x2.image), (key, x1.mode)
+
+
+def test_autotuned_batch_equals_untuned(eb):
+    """The online autotuner switches launch shapes between the first ticks of
+    a batch; the images equal those of a run with tuning off."""
+    from ertm_b200 import ImagingConfig, RTMImager, SolverConfig, _lib
+    from ertm_b200.batch import BatchMigrator
+    from ertm_b200.propagation import PropagationSpec, forward_shot
+    from ertm_b200.types import ElasticModel, GridSpec, ReceiverSpec, SourceSpec
+    rng = np.random.default_rng(9)
+    g = GridSpec(nx=420, nz=300, dx=5.0, dz=5.0)
+    vp = (2400.0 + 700.0 * (np.arange(g.nz)[:, None] > 150) + rng.uniform(0, 50, g.shape)).astype(np.float32)
+    model = ElasticModel(grid=g, vp=vp, vs=(vp / 1.8).astype(np.float32), rho=np.full(g.shape, 2100.0, np.float32),
+                         qp=np.full(g.shape, 80.0, np.float32), qs=np.full(g.shape, 40.0, np.float32))
+    x = np.arange(0.0, 2095.0, 40.0)
+    rec = ReceiverSpec(x=x, z=np.full_like(x, 10.0))
+    shots = [forward_shot(model, SourceSpec(x=500.0 + 400.0 * k, z=10.0, f0=25.0, delay=0.04), rec,
+                          PropagationSpec(dt=4e-4, nt=240, npml=20, boundary="free"), engine="elastic",
+                          components=("vz", "p")) for k in range(3)]
+    imager = RTMImager(ImagingConfig(condition="normalized", checkpoint_mb=8.0),
+                       SolverConfig(nt=240, dt=4e-4, boundary="free", engine="elastic"))
+    L = _lib.lib()
+    out = {}
+    try:
+        for mode in (0, -1, 1):
+            _lib.check(L.ertm_set_autotune(mode), "autotune")
+            out[mode] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
+    finally:
+        _lib.check(L.ertm_set_autotune(1), "autotune")
+    for mode in (-1, 1):
+        for a, b in zip(out[0], out[mode]):
+            for x1, x2 in zip(a, b):
+                assert np.array_equal(x1.image, x2.image), (mode, x1.mode)
