@@ -69,6 +69,7 @@ struct DevProp {
   const float* relax_a;               // visco: [n_q][L] float32 a_l table
   int32_t src_iz, src_ix, mech;       // source node (padded indices), mechanism
   int32_t free_surface;               // 1: zero the free-surface row (acoustic/elastic)
+  const void* tmap;                   // 9 tensor maps (tile heights 8/16/32 × halo/cell/coef) or null
   float* peak;                        // visco compensation: max|p| of the last step (float bits)
 };
 
@@ -120,6 +121,7 @@ struct StepWork {
   // launch of interior tiles walks the rectangle; a launch of boundary tiles
   // walks the frame around it and then the hole.
   int32_t ti0, ti1, tj0, tj1, hole_i, hole_j;
+  int32_t slot;         // index of this work's tensor maps in a TMA launch
   Epilogue epi;
 };
 constexpr int STEP_PEAK = 1;        // visco: reduce max|p| into DevProp::peak

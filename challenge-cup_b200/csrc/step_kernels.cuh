@@ -21,6 +21,8 @@
 // reference bit for bit.
 #pragma once
 
+#include <cuda.h>
+
 #include "ertm_device.cuh"
 
 namespace ertm {
@@ -125,6 +127,123 @@ __device__ __forceinline__ void stage_cells_n(float* const (&s)[NF], const float
     const int so = r * 32 + 4 * ch;
 #pragma unroll
     for (int f = 0; f < NF; ++f) cp_async16(s[f] + so, g[f] + off, ok);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TMA staging (interior tiles): one thread issues a tiled bulk copy per array
+// (halo boxes of 40 × (TZ+2M) floats at x = j0 − 4, cell boxes of 32 × TZ at
+// x = j0: both x offsets are multiples of 4 floats, i.e. 16 bytes), all
+// completing on one mbarrier; rows and columns outside the tensor read as
+// zero, as the cp.async path zero-fills them.  Waits are bounded: a wait that
+// runs out counts in g_stage_timeouts (the host reports it as an error) and
+// the block skips its tile.
+// ---------------------------------------------------------------------------
+struct TmaNone {
+  static constexpr bool kOn = false;
+};
+// Per work: [0] the state block with a halo box, [1] the state block with a
+// cell box, [2] the coefficient block with a cell box.
+template <int N>
+struct TmaSet {
+  static constexpr bool kOn = true;
+  static constexpr bool kGlobal = false;
+  CUtensorMap m[N][3];
+  __device__ __forceinline__ const CUtensorMap* maps(int slot, const DevProp&, int) const { return m[slot]; }
+};
+// The propagator's own tensor maps in device memory (DevProp::tmap, written
+// by the host before any launch): no per-launch parameter block.
+struct TmaGlobal {
+  static constexpr bool kOn = true;
+  static constexpr bool kGlobal = true;
+  __device__ __forceinline__ const CUtensorMap* maps(int, const DevProp& P, int tz) const {
+    return static_cast<const CUtensorMap*>(P.tmap) + 3 * (tz == 8 ? 0 : (tz == 16 ? 1 : 2));
+  }
+};
+
+__device__ unsigned int g_stage_timeouts;
+constexpr int kTmaSpinLimit = 1 << 22;   // try_wait rounds (each suspends briefly): seconds, not forever
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done = 0;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < kTmaSpinLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Stage one tile: NH halo arrays (state-block field slots hf) and NC cell
+// arrays (cf ≥ 0: state-block field slot; cf < 0: coefficient ~cf).  Returns
+// false (for the whole block) only when a bounded TMA wait ran out.
+template <int M, int TZ, int NT, int NH, int NC, class TM>
+__device__ __forceinline__ bool stage_tile(const TM& tm, int slot, const DevProp& P, int i0, int j0,
+                                           float* const (&hd)[NH], const int (&hf)[NH], float* const (&cd)[NC],
+                                           const int (&cf)[NC], uint64_t* bar) {
+  using T = TileShape<M, TZ>;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+  if constexpr (TM::kOn) {
+    if (tid == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+      const CUtensorMap* m = tm.maps(slot, P, TZ);
+      if constexpr (TM::kGlobal) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m + q) : "memory");
+      }
+      mbar_expect_tx(bar, (uint32_t)((NH * T::N + NC * TZ * 32) * sizeof(float)));
+#pragma unroll
+      for (int k = 0; k < NH; ++k) tma_load_3d(hd[k], &m[0], j0 - T::OFF, i0 - M, hf[k], bar);
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        if (cf[k] >= 0) tma_load_3d(cd[k], &m[1], j0, i0, cf[k], bar);
+        else tma_load_3d(cd[k], &m[2], j0, i0, ~cf[k], bar);
+      }
+    }
+    bool ok = mbar_wait_bounded(bar, 0);
+    if (!ok) {
+      atomicAdd(&g_stage_timeouts, 1u);
+      ok = mbar_wait_bounded(bar, 0);   // the copies still write this block's shared memory
+    }
+    return __syncthreads_and(ok) != 0;
+  } else {
+    const float* hg[NH];
+    const float* cg[NC];
+#pragma unroll
+    for (int k = 0; k < NH; ++k) hg[k] = P.f[hf[k]];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cg[k] = cf[k] >= 0 ? P.f[cf[k]] : P.coef[~cf[k]];
+    stage_n<M, TZ, NT, NH>(hd, hg, P.nzp, P.ld, i0, j0);
+    stage_cells_n<TZ, NT, NC>(cd, cg, P.nzp, P.ld, i0, j0);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    return true;
   }
 }
 
@@ -507,12 +626,17 @@ __device__ __forceinline__ PsiCells psi_cells(const ColInfo& C, const float* psx
 // velocity phase
 // ---------------------------------------------------------------------------
 // Acoustic and viscoacoustic: vx += (dt·irx)·(D⁺ₓp + ψ), vz += (dt·irz)·(D⁺_z p + ψ).
-template <int M, int BZ, int R, int KIND, class WS>
+template <int M, int BZ, int R, int KIND, class WS, class TM>
 __global__ void __launch_bounds__(XT* BZ)
-k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
+k_pressure_velocity(const DevProp* __restrict__ props, const WS ws, const __grid_constant__ TM tm) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ __align__(16) float sp[T::N];
+  __shared__ __align__(128) float sp[T::N];
+  __shared__ __align__(128) float c_vx[TZ * 32];
+  __shared__ __align__(128) float c_vz[TZ * 32];
+  __shared__ __align__(128) float c_irx[TZ * 32];
+  __shared__ __align__(128) float c_irz[TZ * 32];
+  __shared__ uint64_t tma_bar;
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
@@ -526,18 +650,17 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
   const float* const azp = P.az; const float* const bzp = P.bz;
   if ((w.flags & STEP_PEAK) && blockIdx.x == w.tile0 && threadIdx.x == 0 && threadIdx.y == 0)
     *P.peak = 0.f;  // the stress phase of this step reduces into it
-  __shared__ __align__(16) float c_vx[TZ * 32], c_vz[TZ * 32], c_irx[TZ * 32], c_irz[TZ * 32];
-  stage<M, TZ, XT * BZ>(sp, P.f[A_P], G.nzp, G.ld, L.i0, L.j0);
   {
-    float* const cs[4] = {c_vx, c_vz, c_irx, c_irz};
-    const float* const cg[4] = {vx, vz, irx, irz};
-    stage_cells_n<TZ, XT * BZ, 4>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
+    float* const hd[1] = {sp};
+    const int hf[1] = {A_P};
+    float* const cd[4] = {c_vx, c_vz, c_irx, c_irz};
+    const int cf[4] = {A_VX, A_VZ, ~CA_IRX, ~CA_IRZ};
+    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
   }
-  cp_async_commit();
+  (void)irx;
+  (void)irz;
   const int j = L.j0 + 4 * threadIdx.x;
 #define CELL(arr, rr) ld4(arr + (rr) * 32 + 4 * threadIdx.x)
-  cp_async_wait_all();
-  __syncthreads();
   if (j >= G.nxp) return;
   if (KIND == TILES_INTERIOR && !G.interior(L.i0, L.j0, TZ)) return;   // the host plans only interior tiles here
   if (KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ))) {
@@ -613,14 +736,19 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws) {
 }
 
 // Elastic: vx += (dt·irx)·(D⁺ₓσxx + D⁻_zσxz), vz += (dt·irz)·(D⁻ₓσxz + D⁺_zσzz).
-template <int M, int BZ, int R, int KIND, class WS>
+template <int M, int BZ, int R, int KIND, class WS, class TM>
 __global__ void __launch_bounds__(XT* BZ)
-k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
+k_elastic_velocity(const DevProp* __restrict__ props, const WS ws, const __grid_constant__ TM tm) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ __align__(16) float sxx_s[T::N];
-  __shared__ __align__(16) float szz_s[T::N];
-  __shared__ __align__(16) float sxz_s[T::N];
+  __shared__ __align__(128) float sxx_s[T::N];
+  __shared__ __align__(128) float szz_s[T::N];
+  __shared__ __align__(128) float sxz_s[T::N];
+  __shared__ __align__(128) float c_vx[TZ * 32];
+  __shared__ __align__(128) float c_vz[TZ * 32];
+  __shared__ __align__(128) float c_irx[TZ * 32];
+  __shared__ __align__(128) float c_irz[TZ * 32];
+  __shared__ uint64_t tma_bar;
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
@@ -633,20 +761,15 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws) {
   float* const psz0 = P.psiz[0]; float* const psz1 = P.psiz[1];
   const float* const azp = P.az; const float* const bzp = P.bz;
   {
-    float* const hs[3] = {sxx_s, szz_s, sxz_s};
-    const float* const hg[3] = {P.f[E_SXX], P.f[E_SZZ], P.f[E_SXZ]};
-    stage_n<M, TZ, XT * BZ, 3>(hs, hg, G.nzp, G.ld, L.i0, L.j0);
+    float* const hd[3] = {sxx_s, szz_s, sxz_s};
+    const int hf[3] = {E_SXX, E_SZZ, E_SXZ};
+    float* const cd[4] = {c_vx, c_vz, c_irx, c_irz};
+    const int cf[4] = {E_VX, E_VZ, ~CE_IRX, ~CE_IRZ};
+    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
   }
-  __shared__ __align__(16) float c_vx[TZ * 32], c_vz[TZ * 32], c_irx[TZ * 32], c_irz[TZ * 32];
-  {
-    float* const cs[4] = {c_vx, c_vz, c_irx, c_irz};
-    const float* const cg[4] = {vx, vz, irx, irz};
-    stage_cells_n<TZ, XT * BZ, 4>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
-  }
-  cp_async_commit();
+  (void)irx;
+  (void)irz;
   const int j = L.j0 + 4 * threadIdx.x;
-  cp_async_wait_all();
-  __syncthreads();
   if (j >= G.nxp) return;
   if (KIND == TILES_INTERIOR && !G.interior(L.i0, L.j0, TZ)) return;   // the host plans only interior tiles here
   if (KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ))) {
@@ -778,13 +901,17 @@ __device__ __forceinline__ void block_max_to(float v, float* dst) {
 
 // Acoustic (VISCO=false): p += (dt·κ)·div.  Viscoacoustic (VISCO=true):
 // ε += dt·div; r_l ← r_l·a_l + b_l·Δε; p = K_R·ε + Σ r_l.
-template <int M, int BZ, int R, bool VISCO, int KIND, class WS>
+template <int M, int BZ, int R, bool VISCO, int KIND, class WS, class TM>
 __global__ void __launch_bounds__(XT* BZ)
-k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
+k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_constant__ TM tm) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ __align__(16) float svx[T::N];
-  __shared__ __align__(16) float svz[T::N];
+  __shared__ __align__(128) float svx[T::N];
+  __shared__ __align__(128) float svz[T::N];
+  __shared__ __align__(128) float c_a[TZ * 32];
+  __shared__ __align__(128) float c_b[TZ * 32];
+  __shared__ __align__(16) float e_p[TZ * 32];                   // P for the epilogue
+  __shared__ uint64_t tma_bar;
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
@@ -802,24 +929,17 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
   float* const psz = P.psiz[1];
   const float* const azp = P.az; const float* const bzp = P.bz;
   {
-    float* const hs[2] = {svx, svz};
-    const float* const hg[2] = {P.f[A_VX], P.f[A_VZ]};
-    stage_n<M, TZ, XT * BZ, 2>(hs, hg, G.nzp, G.ld, L.i0, L.j0);
+    float* const hd[2] = {svx, svz};
+    const int hf[2] = {A_VX, A_VZ};
+    float* const cd[2] = {c_a, c_b};
+    const int cf[2] = {VISCO ? V_EPS : A_P, VISCO ? ~CV_KR : ~CA_KAPPA};
+    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
   }
-  __shared__ __align__(16) float c_a[TZ * 32], c_b[TZ * 32];   // acoustic: p, κ; viscoacoustic: ε, K_R
-  __shared__ __align__(16) float e_p[TZ * 32];                  // P for the epilogue
-  {
-    float* const cs[2] = {c_a, c_b};
-    const float* const cg[2] = {VISCO ? eps : p, cA};
-    stage_cells_n<TZ, XT * BZ, 2>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
-  }
-  cp_async_commit();
+  (void)cA;
   const int j = L.j0 + 4 * threadIdx.x;
   const bool jok = j < G.nxp;
   float amp, amp_eps;
   source_amps(w, P, amp, amp_eps);
-  cp_async_wait_all();
-  __syncthreads();
   const size_t npix = (size_t)G.nz * G.nx;
   float peak = 0.f;
   const bool valid = KIND != TILES_INTERIOR || G.interior(L.i0, L.j0, TZ);   // the host plans only interior tiles there
@@ -957,13 +1077,21 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws) {
 //   σxz += (dt·μxz)·(D⁺_z vx + D⁺ₓ vz); source; free surface σzz = σxz = 0;
 // then the epilogue with P/S from the stresses (stress separation) or from
 // the raw velocity divergence/curl (divcurl, propagation.py:953-976).
-template <int M, int BZ, int R, int KIND, class WS>
+template <int M, int BZ, int R, int KIND, class WS, class TM>
 __global__ void __launch_bounds__(XT* BZ)
-k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
+k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_constant__ TM tm) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
-  __shared__ __align__(16) float svx[T::N];
-  __shared__ __align__(16) float svz[T::N];
+  __shared__ __align__(128) float svx[T::N];
+  __shared__ __align__(128) float svz[T::N];
+  __shared__ __align__(128) float c_xx[TZ * 32];
+  __shared__ __align__(128) float c_zz[TZ * 32];
+  __shared__ __align__(128) float c_xz[TZ * 32];
+  __shared__ __align__(128) float c_lam[TZ * 32];
+  __shared__ __align__(128) float c_l2m[TZ * 32];
+  __shared__ __align__(128) float c_mu[TZ * 32];
+  __shared__ __align__(16) float e_p[TZ * 32], e_s[TZ * 32];   // P and S for the epilogue
+  __shared__ uint64_t tma_bar;
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
@@ -979,24 +1107,18 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws) {
   const float* const azp = P.az; const float* const bzp = P.bz;
   const int mech = P.mech;
   {
-    float* const hs[2] = {svx, svz};
-    const float* const hg[2] = {P.f[E_VX], P.f[E_VZ]};
-    stage_n<M, TZ, XT * BZ, 2>(hs, hg, G.nzp, G.ld, L.i0, L.j0);
+    float* const hd[2] = {svx, svz};
+    const int hf[2] = {E_VX, E_VZ};
+    float* const cd[6] = {c_xx, c_zz, c_xz, c_lam, c_l2m, c_mu};
+    const int cf[6] = {E_SXX, E_SZZ, E_SXZ, ~CE_LAM, ~CE_L2M, ~CE_MUXZ};
+    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
   }
-  __shared__ __align__(16) float c_xx[TZ * 32], c_zz[TZ * 32], c_xz[TZ * 32], c_lam[TZ * 32], c_l2m[TZ * 32],
-      c_mu[TZ * 32];
-  __shared__ __align__(16) float e_p[TZ * 32], e_s[TZ * 32];   // P and S for the epilogue
-  {
-    float* const cs[6] = {c_xx, c_zz, c_xz, c_lam, c_l2m, c_mu};
-    const float* const cg[6] = {sxx, szz, sxz, clam, cl2m, cmu};
-    stage_cells_n<TZ, XT * BZ, 6>(cs, cg, G.nzp, G.ld, L.i0, L.j0);
-  }
-  cp_async_commit();
+  (void)clam;
+  (void)cl2m;
+  (void)cmu;
   const int j = L.j0 + 4 * threadIdx.x;
   float amp, amp_eps;
   source_amps(w, P, amp, amp_eps);
-  cp_async_wait_all();
-  __syncthreads();
   const size_t npix = (size_t)G.nz * G.nx;
   const Epilogue& E = w.epi;
   const bool epi = E.kind != EPI_NONE;

@@ -77,6 +77,8 @@ _SIGNATURES = {
     "ertm_set_tile_split": (_I32, [_I32]),
     "ertm_set_tick_lanes": (_I32, [_I32]),
     "ertm_set_autotune": (_I32, [_I32]),
+    "ertm_set_tma": (_I32, [_I32]),
+    "ertm_stage_timeouts": (C.c_int64, []),
     "ertm_autotune_report": (C.c_char_p, []),
     "ertm_division_check": (_I32, [C.c_float, _I32, C.POINTER(C.c_uint64)]),
     "ertm_profile_stencil": (_I32, [_I32, _I32]),

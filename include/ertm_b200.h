@@ -135,6 +135,15 @@ int32_t ertm_set_tick_lanes(int32_t lanes);
  * kept for the process.  Any forced knob above disables it.  1 = on, 0 = off,
  * −1 = off and forget the choices made so far.  Results do not depend on it. */
 int32_t ertm_set_autotune(int32_t enable);
+/* Interior tiles staged by TMA tiled bulk copies (1) or by cp.async (0, the
+ * default: faster on the measured workloads).  Applies to propagators created
+ * afterwards (their tensor maps are encoded at creation).  Results are
+ * identical. */
+int32_t ertm_set_tma(int32_t enable);
+/* Bounded TMA waits that ran out since the library was loaded (0 in a healthy
+ * run; −1 if the counter cannot be read).  A block whose wait runs out skips
+ * its tile, so any non-zero value means wrong results. */
+int64_t ertm_stage_timeouts(void);
 /* One line per tuned group: each candidate tile height / split / lanes with
  * its mean tick time; the chosen one is starred.  Valid until the next call. */
 const char* ertm_autotune_report(void);

@@ -232,17 +232,20 @@ def split_always(eb):
     _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
 
 
+@pytest.mark.parametrize("tma", [1, 0])
 @pytest.mark.parametrize("engine,boundary,mechanism,tile_rows", [
     ("acoustic", "cpml", "explosive", 16), ("acoustic", "free", "explosive", 8),
-    ("elastic", "free", "explosive", 16), ("elastic", "cpml", "force_z", 8), ("elastic", "free", "shear", 16),
+    ("elastic", "free", "explosive", 16), ("elastic", "cpml", "force_z", 8), ("elastic", "free", "shear", 32),
     ("viscoacoustic", "cpml", "explosive", 16)])
-def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, boundary, mechanism, tile_rows):
+def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, boundary, mechanism, tile_rows, tma):
     """Interior tiles and the boundary frame in separate launches (the source
-    node's tile, inside the interior rectangle, goes with the frame): GPU ==
-    oracle on a grid with an interior rectangle of several tiles."""
+    node's tile, inside the interior rectangle, goes with the frame), interior
+    tiles staged by TMA or by cp.async: GPU == oracle on a grid with an
+    interior rectangle of several tiles."""
     from ertm_b200 import _lib
     from ertm_b200.propagation import PropagationSpec, QOptions, run_forward
     _lib.check(_lib.lib().ertm_set_tile_rows(tile_rows), "tile rows")
+    _lib.check(_lib.lib().ertm_set_tma(tma), "tma")
     try:
         rng = np.random.default_rng(11)
         nz, nx = 150, 200
@@ -263,6 +266,8 @@ def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, b
         want = orc.run_forward(model, src, rcv, ospec, engine=engine, components=comps, q=q)
     finally:
         _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
+        _lib.check(_lib.lib().ertm_set_tma(0), "tma")
+    assert _lib.lib().ertm_stage_timeouts() == 0
     for n in comps:
         if engine == "viscoacoustic":
             assert rel_l2(got[n], want[n]) < VISCO_TOL, n
