@@ -500,6 +500,8 @@ def run_ours(args, dist: Dist) -> None:
                      "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "serving": serving,
+        "autotune": L.ertm_autotune_report().decode().strip().splitlines(),
+        "stage_timeouts": int(L.ertm_stage_timeouts()),
         "clocks": clk,
         "gpu_launches": launches,
     }
