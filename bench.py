@@ -461,6 +461,7 @@ def run_ours(args, dist: Dist) -> None:
     e2e_s = dist.max(statistics.mean(e2e_times)) if e2e_times else float("nan")
     e2e_value = n_total / e2e_s
 
+    tuned = L.ertm_autotune_report().decode().strip().splitlines()   # the batched job's shapes
     serving = None
     if dist.world == 1 and args.serve_jobs > 0:
         serving = serving_run(args.serve_jobs)
@@ -500,7 +501,7 @@ def run_ours(args, dist: Dist) -> None:
                      "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "serving": serving,
-        "autotune": L.ertm_autotune_report().decode().strip().splitlines(),
+        "autotune": tuned,
         "stage_timeouts": int(L.ertm_stage_timeouts()),
         "clocks": clk,
         "gpu_launches": launches,
