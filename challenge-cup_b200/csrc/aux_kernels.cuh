@@ -410,3 +410,65 @@ __global__ void k_stack_finish(const double* acc, int64_t n, int count, float* o
 }
 
 }  // namespace ertm
+
+namespace ertm {
+
+// ---------------------------------------------------------------------------
+// Record preprocessing (preprocess.py:36-224, numerics.py:337-392).  Records
+// are (nt, ntr) float32, time-major; arithmetic in float64 as the reference
+// does, one float32 rounding at the end.
+// ---------------------------------------------------------------------------
+// Sinc resampling: out[o, s] = Σ_t w[o, t] · in[clamp(off0[o] + t), s] with the
+// weights and first offsets computed on the host (numerics.py:371-384).
+__global__ void k_resample(const float* __restrict__ in, int64_t n_in, int64_t ntr, const double* __restrict__ w,
+                           const int64_t* __restrict__ off0, int taps, int64_t n_out, float* __restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_out * ntr) return;
+  const int64_t o = idx / ntr, s = idx - o * ntr;
+  double acc = 0.0;
+  for (int t = 0; t < taps; ++t) {
+    int64_t k = off0[o] + t;
+    k = k < 0 ? 0 : (k >= n_in ? n_in - 1 : k);
+    acc = dadd(acc, dmul(w[o * taps + t], (double)in[k * ntr + s]));
+  }
+  out[idx] = __double2float_rn(acc);
+}
+
+// Direct-wave mute (preprocess.py:121-173): weight 0.5 − 0.5·cos(π·ramp) with
+// ramp = clip((t − start_r)/(end_r − start_r), 0, 1) per receiver r.
+__global__ void k_mute(const float* __restrict__ in, int64_t nt, int64_t ntr, const double* __restrict__ t,
+                       const double* __restrict__ start, const double* __restrict__ end, float* __restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nt * ntr) return;
+  const int64_t i = idx / ntr, r = idx - i * ntr;
+  double ramp = __ddiv_rn(dsub(t[i], start[r]), dsub(end[r], start[r]));
+  ramp = ramp < 0.0 ? 0.0 : (ramp > 1.0 ? 1.0 : ramp);
+  const double wgt = dsub(0.5, dmul(0.5, cos(dmul(3.141592653589793, ramp))));
+  out[idx] = __double2float_rn(dmul((double)in[idx], wgt));
+}
+
+// End taper (preprocess.py:176-191): the first w samples times ramp[k], the
+// last w times ramp[w−1−k], in that order (both when they overlap).
+__global__ void k_taper(const float* __restrict__ in, int64_t nt, int64_t ntr, const double* __restrict__ ramp,
+                        int64_t w, float* __restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nt * ntr) return;
+  const int64_t i = idx / ntr;
+  double x = (double)in[idx];
+  if (i < w) x = dmul(x, ramp[i]);
+  if (i >= nt - w) x = dmul(x, ramp[nt - 1 - i]);
+  out[idx] = __double2float_rn(x);
+}
+
+// Two-component rotation (preprocess.py:36-67): vx' = c·vx + s·vz,
+// vz' = (−s)·vx + c·vz in float64.
+__global__ void k_rotate(const float* __restrict__ vx, const float* __restrict__ vz, int64_t n, double c, double s,
+                         float* __restrict__ ox, float* __restrict__ oz) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const double x = (double)vx[idx], z = (double)vz[idx];
+  ox[idx] = __double2float_rn(dadd(dmul(c, x), dmul(s, z)));
+  oz[idx] = __double2float_rn(dadd(dmul(-s, x), dmul(c, z)));
+}
+
+}  // namespace ertm

@@ -1743,6 +1743,55 @@ void require_device_pointer(const void* p, const char* what) {
           std::string(what) + " must be device memory");
 }
 
+// Host-or-device arrays for the record kernels: device pointers are used in
+// place; host inputs are uploaded and host outputs downloaded at the end.
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+struct InArray {
+  DevBuf buf;
+  const void* d = nullptr;
+  InArray(const void* p, size_t bytes, cudaStream_t st) {
+    if (is_device_ptr(p)) {
+      d = p;
+    } else {
+      buf = DevBuf(bytes, st);
+      upload(buf.p, p, bytes, st);
+      d = buf.p;
+    }
+  }
+  template <class T>
+  const T* as() const { return static_cast<const T*>(d); }
+};
+
+struct OutArray {
+  DevBuf buf;
+  void* host = nullptr;
+  void* d = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  OutArray(void* p, size_t b, cudaStream_t s) : bytes(b), st(s) {
+    if (is_device_ptr(p)) {
+      d = p;
+    } else {
+      buf = DevBuf(b, s);
+      d = buf.p;
+      host = p;
+    }
+  }
+  void finish() {
+    if (host) CK(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, st));
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(d); }
+};
+
 }  // namespace
 
 // ==========================================================================
@@ -2314,6 +2363,74 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
     k_mask_cast<<<g2, b2, 0, st>>>(cur, o.as<float>(), nz, nx, npml, top_mask);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_resample(const float* in, int64_t n_in, int64_t ntr, const double* w, const int64_t* off0, int32_t taps,
+                      int64_t n_out, float* out, void* stream) {
+  return guarded([&] {
+    REQUIRE(in && w && off0 && out && n_in >= 1 && ntr >= 1 && n_out >= 1 && taps >= 1, "bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    InArray a(in, (size_t)n_in * ntr * 4, st), W(w, (size_t)n_out * taps * 8, st), O(off0, (size_t)n_out * 8, st);
+    OutArray b(out, (size_t)n_out * ntr * 4, st);
+    const int64_t n = n_out * ntr;
+    k_resample<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), n_in, ntr, W.as<double>(),
+                                                            O.as<int64_t>(), taps, n_out, b.as<float>());
+    ++g_launches;
+    CK(cudaGetLastError());
+    b.finish();
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_mute(const float* in, int64_t nt, int64_t ntr, const double* t, const double* start, const double* end,
+                  float* out, void* stream) {
+  return guarded([&] {
+    REQUIRE(in && t && start && end && out && nt >= 1 && ntr >= 1, "bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    InArray a(in, (size_t)nt * ntr * 4, st), T(t, (size_t)nt * 8, st), S(start, (size_t)ntr * 8, st),
+        E(end, (size_t)ntr * 8, st);
+    OutArray b(out, (size_t)nt * ntr * 4, st);
+    const int64_t n = nt * ntr;
+    k_mute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), nt, ntr, T.as<double>(), S.as<double>(),
+                                                        E.as<double>(), b.as<float>());
+    ++g_launches;
+    CK(cudaGetLastError());
+    b.finish();
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_taper(const float* in, int64_t nt, int64_t ntr, const double* ramp, int64_t w, float* out,
+                   void* stream) {
+  return guarded([&] {
+    REQUIRE(in && ramp && out && nt >= 1 && ntr >= 1 && w >= 1 && w <= nt, "bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    InArray a(in, (size_t)nt * ntr * 4, st), R(ramp, (size_t)w * 8, st);
+    OutArray b(out, (size_t)nt * ntr * 4, st);
+    const int64_t n = nt * ntr;
+    k_taper<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), nt, ntr, R.as<double>(), w, b.as<float>());
+    ++g_launches;
+    CK(cudaGetLastError());
+    b.finish();
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_rotate(const float* vx, const float* vz, int64_t n, double c, double s, float* ox, float* oz,
+                    void* stream) {
+  return guarded([&] {
+    REQUIRE(vx && vz && ox && oz && n >= 1, "bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    InArray a(vx, (size_t)n * 4, st), b(vz, (size_t)n * 4, st);
+    OutArray x(ox, (size_t)n * 4, st), z(oz, (size_t)n * 4, st);
+    k_rotate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), b.as<float>(), n, c, s, x.as<float>(),
+                                                          z.as<float>());
+    ++g_launches;
+    CK(cudaGetLastError());
+    x.finish();
+    z.finish();
     CK(cudaStreamSynchronize(st));
   });
 }

@@ -210,7 +210,15 @@ class RTMImager:
         for name, arr in comps.items():
             data = np.asarray(arr, dtype=np.float64)
             if abs(float(shot.dt) - spec.dt) > 1e-12 and data.shape[0] > 1:
-                data = num.resample_sinc(data, float(shot.dt), spec.dt)
+                if preprocess is None:
+                    # device sinc resampling: the record is cast to float32 for
+                    # injection anyway, so one float32 rounding of the float64
+                    # sums gives the reference's values
+                    from .preprocess import resample_sinc as device_resample
+                    data = np.asarray(device_resample(data, float(shot.dt), spec.dt), dtype=np.float64)
+                else:
+                    # the hook receives the float64 resampled record, as in the reference
+                    data = num.resample_sinc(data, float(shot.dt), spec.dt)
             if preprocess is not None:
                 data = np.asarray(preprocess(data, spec.dt), dtype=np.float64)
             out[name] = self._fit_length(data, int(spec.nt))

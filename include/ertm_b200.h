@@ -248,6 +248,25 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
                          const double* rillum, int32_t by_illum, int32_t by_rillum, double eps,
                          int32_t laplacian, double lowpass, int32_t npml, int32_t top_mask, float* out,
                          void* stream);
+/* Record preprocessing on the device (preprocess.py:36-224), for (nt, ntr)
+ * float32 records, time-major; host or device pointers; float64 arithmetic
+ * and one float32 rounding, as the reference.
+ *   ertm_resample: Kaiser-windowed sinc resampling (numerics.py:337-392) with
+ *     the host-computed weights w (n_out × taps) and first tap offsets off0
+ *     (n_out; clamped to the record): out[o,s] = Σ_t w[o,t]·in[off0[o]+t, s].
+ *   ertm_mute: direct-wave mute (preprocess.py:121-173), per-receiver ramp
+ *     bounds start/end (seconds) at sample times t.
+ *   ertm_taper: cosine end taper (preprocess.py:176-191) with the w-sample ramp.
+ *   ertm_rotate: COG→CSG rotation of (vx, vz) by cos/sin (preprocess.py:36-67). */
+int32_t ertm_resample(const float* in, int64_t n_in, int64_t ntr, const double* w, const int64_t* off0, int32_t taps,
+                      int64_t n_out, float* out, void* stream);
+int32_t ertm_mute(const float* in, int64_t nt, int64_t ntr, const double* t, const double* start, const double* end,
+                  float* out, void* stream);
+int32_t ertm_taper(const float* in, int64_t nt, int64_t ntr, const double* ramp, int64_t w, float* out,
+                   void* stream);
+int32_t ertm_rotate(const float* vx, const float* vz, int64_t n, double c, double s, float* ox, float* oz,
+                    void* stream);
+
 /* stack_images (pipeline.py:133-161): images is n_images pointers to (n,) float32. */
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream);

@@ -23,6 +23,9 @@ from typing import Any, Callable
 import numpy as np
 
 __all__ = [
+    "rotate_components",
+    "mute_weights",
+    "taper_ends",
     "STAGGER",
     "ghost_width",
     "coefficient_l1",
@@ -1103,3 +1106,46 @@ def stack_images(images: list[np.ndarray], normalize: bool = True) -> np.ndarray
         acc += d
     acc /= len(images)
     return acc.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Record preprocessing — preprocess.py:36-224 (arrays in, arrays out)
+# ---------------------------------------------------------------------------
+def rotate_components(components: dict, angle_deg: float) -> dict:
+    """preprocess.py:36-67."""
+    ang = np.deg2rad(float(angle_deg))
+    c, s = float(np.cos(ang)), float(np.sin(ang))
+    out = {n: np.array(a, copy=True) for n, a in components.items()}
+    if "vx" in out and "vz" in out:
+        vx = np.asarray(components["vx"], dtype=np.float64)
+        vz = np.asarray(components["vz"], dtype=np.float64)
+        out["vx"] = (c * vx + s * vz).astype(np.float32)
+        out["vz"] = (-s * vx + c * vz).astype(np.float32)
+    return out
+
+
+def mute_weights(t: np.ndarray, rx: np.ndarray, src_x: float, f0: float, delay: float, v_ref: float,
+                 margin_periods: float = 1.2, offset_factor: float = 1.05, taper_periods: float = 0.5) -> np.ndarray:
+    """preprocess.py:145-163 — (nt, nrec) float64 cosine mute weights."""
+    t = np.asarray(t, dtype=np.float64)
+    offset = np.abs(np.asarray(rx, dtype=np.float64) - src_x)
+    period = 1.0 / max(float(f0), 1e-6)
+    t_mute = float(delay) + margin_periods * period + offset_factor * offset / v_ref
+    taper = max(float(taper_periods) * period, 1e-9)
+    w = np.empty((t.size, offset.size))
+    for k in range(offset.size):
+        start, end = t_mute[k] - taper, t_mute[k] + taper
+        ramp = np.clip((t - start) / (end - start), 0.0, 1.0)
+        w[:, k] = 0.5 - 0.5 * np.cos(np.pi * ramp)
+    return w
+
+
+def taper_ends(a: np.ndarray, fraction: float = 0.05) -> np.ndarray:
+    """preprocess.py:176-188 — float64 result."""
+    out = np.array(a, dtype=np.float64, copy=True)
+    n = out.shape[0]
+    w = max(int(fraction * n), 1)
+    ramp = 0.5 - 0.5 * np.cos(np.pi * (np.arange(w) + 0.5) / w)
+    out[:w] *= ramp[:, None]
+    out[-w:] *= ramp[::-1][:, None]
+    return out

@@ -247,8 +247,46 @@ def stack_case() -> dict[str, np.ndarray]:
     return {"images": np.stack(imgs), "stacked": stacked.astype(np.float32)}
 
 
+def preprocess_case() -> dict[str, np.ndarray]:
+    """preprocess.py:36-224: rotation, sinc resampling (up and down), direct-wave
+    mute, end taper and the combined prepare_shot, on a seeded 3-component shot."""
+    from ertm import preprocess as pre
+    from ertm.types import ShotRecord
+    rng = np.random.default_rng(31)
+    nt, nrec, dt = 240, 19, 4e-4
+    rec = receivers_line(0.0, 540.0, nrec, 8.0)
+    src = SourceSpec(x=260.0, z=12.0, f0=30.0, delay=0.03)
+    t = np.arange(nt) * dt
+    comps = {n: (rng.normal(size=(nt, nrec)) * s).astype(np.float32) for n, s in (("p", 1.0), ("vx", 0.3),
+                                                                                  ("vz", 0.5))}
+    shot = ShotRecord(data=comps["p"], dt=dt, t=t, receivers=rec, source=src, components=dict(comps))
+    model = layered_model(60, 40, 10.0, 5)
+    out = {"nt": np.array(nt), "dt": np.array(dt), "rx": rec.x, "rz": rec.z,
+           "src": np.array([src.x, src.z, src.f0, src.delay, src.amplitude])}
+    out.update({f"in_{n}": v for n, v in comps.items()})
+    out.update(model_arrays("m_", model))
+    rot = pre.rotate_components(comps, 30.0)
+    out.update({f"rot_{n}": np.asarray(v) for n, v in rot.items()})
+    for tag, dt_out in (("up", 3e-4), ("down", 5.5e-4)):
+        r = pre.resample_shot(shot, dt_out)
+        out.update({f"res_{tag}_{n}": np.asarray(v) for n, v in r.components.items()})
+        out[f"res_{tag}_data"] = np.asarray(r.data)
+    m = pre.mute_direct_wave(shot, 2100.0)
+    out.update({f"mute_{n}": np.asarray(v) for n, v in m.components.items()})
+    out["mute_data"] = np.asarray(m.data)
+    tp = pre.taper_record_ends(shot, 0.05)
+    out.update({f"taper_{n}": np.asarray(v) for n, v in tp.components.items()})
+    out["taper_data"] = np.asarray(tp.data)
+    ps = pre.prepare_shot(shot, model=model, record_dt=3.5e-4, rotation_deg=25.0, mute=True, taper_fraction=0.05)
+    out.update({f"prep_{n}": np.asarray(v) for n, v in ps.components.items()})
+    out["prep_data"] = np.asarray(ps.data)
+    out["prep_dt"] = np.array(ps.dt)
+    return out
+
+
 def main() -> None:
     cases = {
+        "preprocess": preprocess_case,
         "numerics": numerics_case,
         "gsls": gsls_case,
         "acoustic_cpml": lambda: propagate_case("acoustic", "cpml", nt=90, inject_every=7),
