@@ -142,20 +142,12 @@ __device__ __forceinline__ void stage_cells_n(float* const (&s)[NF], const float
 struct TmaNone {
   static constexpr bool kOn = false;
 };
-// Per work: [0] the state block with a halo box, [1] the state block with a
-// cell box, [2] the coefficient block with a cell box.
-template <int N>
-struct TmaSet {
-  static constexpr bool kOn = true;
-  static constexpr bool kGlobal = false;
-  CUtensorMap m[N][3];
-  __device__ __forceinline__ const CUtensorMap* maps(int slot, const DevProp&, int) const { return m[slot]; }
-};
 // The propagator's own tensor maps in device memory (DevProp::tmap, written
-// by the host before any launch): no per-launch parameter block.
+// by the host at creation): per tile height, [0] the state block with a halo
+// box, [1] the state block with a cell box, [2] the coefficient block with a
+// cell box.
 struct TmaGlobal {
   static constexpr bool kOn = true;
-  static constexpr bool kGlobal = true;
   __device__ __forceinline__ const CUtensorMap* maps(int, const DevProp& P, int tz) const {
     return static_cast<const CUtensorMap*>(P.tmap) + 3 * (tz == 8 ? 0 : (tz == 16 ? 1 : 2));
   }
@@ -211,11 +203,9 @@ __device__ __forceinline__ bool stage_tile(const TM& tm, int slot, const DevProp
     __syncthreads();
     if (tid == 0) {
       const CUtensorMap* m = tm.maps(slot, P, TZ);
-      if constexpr (TM::kGlobal) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q)
-          asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m + q) : "memory");
-      }
+      for (int q = 0; q < 3; ++q)
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m + q) : "memory");
       mbar_expect_tx(bar, (uint32_t)((NH * T::N + NC * TZ * 32) * sizeof(float)));
 #pragma unroll
       for (int k = 0; k < NH; ++k) tma_load_3d(hd[k], &m[0], j0 - T::OFF, i0 - M, hf[k], bar);
