@@ -472,3 +472,54 @@ __global__ void k_rotate(const float* __restrict__ vx, const float* __restrict__
 }
 
 }  // namespace ertm
+
+namespace ertm {
+
+// ---------------------------------------------------------------------------
+// Short-time Fourier filtering with overlap-add (qcomp.py:98-147): frames of
+// L samples every hop samples, Hann-windowed, one complex response per frame
+// and frequency, windowed overlap-add normalised by Σ window².  Records are
+// (n, ntr) float64, time-major; frame s covers [s·hop, s·hop + L) ∩ [0, n).
+// ---------------------------------------------------------------------------
+__global__ void k_stft_frames(const double* __restrict__ x, int64_t n, int64_t ntr, int L, int hop, int S,
+                              const double* __restrict__ win, double* __restrict__ frames) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)S * ntr * L) return;
+  const int k = (int)(idx % L);
+  const int64_t sr = idx / L;
+  const int64_t s = sr / ntr, r = sr - s * ntr;
+  const int64_t t = s * hop + k;
+  frames[idx] = t < n ? dmul(x[t * ntr + r], win[k]) : 0.0;
+}
+
+// Frame spectra times the frame's response (complex, (a+ib)(c+id)).
+__global__ void k_stft_response(double2* __restrict__ spec, int64_t ntr, int F, int S,
+                                const double2* __restrict__ resp) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)S * ntr * F) return;
+  const int f = (int)(idx % F);
+  const int64_t s = idx / F / ntr;
+  const double2 a = spec[idx], b = resp[s * F + f];
+  spec[idx] = make_double2(dsub(dmul(a.x, b.x), dmul(a.y, b.y)), dadd(dmul(a.x, b.y), dmul(a.y, b.x)));
+}
+
+// Overlap-add in frame order: out(t) = Σ_s (filt_s(t − s·hop)/L)·win(t − s·hop),
+// divided by Σ_s win(t − s·hop)² (1 where that sum is ≤ 1e-12).
+__global__ void k_stft_overlap_add(const double* __restrict__ filt, int64_t n, int64_t ntr, int L, int hop, int S,
+                                   const double* __restrict__ win, double* __restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * ntr) return;
+  const int64_t t = idx / ntr, r = idx - t * ntr;
+  const int64_t s0 = t >= L ? (t - L) / hop + 1 : 0;
+  double acc = 0.0, wsum = 0.0;
+  for (int64_t s = s0; s < S && s * hop <= t; ++s) {
+    const int64_t k = t - s * hop;
+    if (k >= L) continue;
+    const double y = __ddiv_rn(filt[(s * ntr + r) * L + k], (double)L);
+    acc = dadd(acc, dmul(y, win[k]));
+    wsum = dadd(wsum, dmul(win[k], win[k]));
+  }
+  out[idx] = __ddiv_rn(acc, wsum > 1e-12 ? wsum : 1.0);
+}
+
+}  // namespace ertm

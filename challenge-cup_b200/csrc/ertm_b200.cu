@@ -2435,6 +2435,46 @@ int32_t ertm_rotate(const float* vx, const float* vz, int64_t n, double c, doubl
   });
 }
 
+int32_t ertm_stft_filter(const double* in, int64_t n, int64_t ntr, int32_t L, int32_t hop, int32_t S,
+                         const double* window, const double* response, double* out, void* stream) {
+  return guarded([&] {
+    REQUIRE(in && window && response && out && n >= 1 && ntr >= 1 && L >= 8 && hop >= 1 && S >= 1,
+            "bad arguments");
+    REQUIRE((int64_t)(S - 1) * hop < n, "more frames than the record holds");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int F = L / 2 + 1;
+    InArray a(in, (size_t)n * ntr * 8, st), W(window, (size_t)L * 8, st), R(response, (size_t)S * F * 16, st);
+    OutArray o(out, (size_t)n * ntr * 8, st);
+    const int64_t batch = (int64_t)S * ntr;
+    DevBuf frames((size_t)batch * L * 8, st), spec((size_t)batch * F * 16, st);
+    const int64_t nf = batch * L;
+    k_stft_frames<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(a.as<double>(), n, ntr, L, hop, S, W.as<double>(),
+                                                               frames.as<double>());
+    cufftHandle fwd = 0, inv = 0;
+    int dims[1] = {L};
+    CKFFT(cufftPlanMany(&fwd, 1, dims, nullptr, 1, L, nullptr, 1, F, CUFFT_D2Z, (int)batch));
+    struct Plan {
+      cufftHandle h;
+      ~Plan() { cufftDestroy(h); }
+    } pf{fwd};
+    CKFFT(cufftPlanMany(&inv, 1, dims, nullptr, 1, F, nullptr, 1, L, CUFFT_Z2D, (int)batch));
+    Plan pi{inv};
+    CKFFT(cufftSetStream(fwd, st));
+    CKFFT(cufftSetStream(inv, st));
+    CKFFT(cufftExecD2Z(fwd, frames.as<cufftDoubleReal>(), spec.as<cufftDoubleComplex>()));
+    const int64_t ns = batch * F;
+    k_stft_response<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(spec.as<double2>(), ntr, F, S, R.as<double2>());
+    CKFFT(cufftExecZ2D(inv, spec.as<cufftDoubleComplex>(), frames.as<cufftDoubleReal>()));
+    const int64_t no = n * ntr;
+    k_stft_overlap_add<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(frames.as<double>(), n, ntr, L, hop, S,
+                                                                    W.as<double>(), o.as<double>());
+    g_launches += 3;
+    CK(cudaGetLastError());
+    o.finish();
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream) {
   return guarded([&] {

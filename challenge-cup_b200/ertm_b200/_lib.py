@@ -112,6 +112,7 @@ _SIGNATURES = {
     "ertm_mute": (_I32, [_P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
     "ertm_taper": (_I32, [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P]),
     "ertm_rotate": (_I32, [_P, _P, C.c_int64, C.c_double, C.c_double, _P, _P, _P]),
+    "ertm_stft_filter": (_I32, [_P, C.c_int64, C.c_int64, _I32, _I32, _I32, _P, _P, _P, _P]),
     "ertm_session_create": (_I32, [C.POINTER(C.c_void_p)]),
     "ertm_session_add": (_I32, [_P, C.POINTER(BatchShot), C.c_int64]),
     "ertm_session_advance": (_I32, [_P, _I32, C.POINTER(C.c_int64), _I32, C.POINTER(C.c_int32)]),

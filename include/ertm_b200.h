@@ -267,6 +267,15 @@ int32_t ertm_taper(const float* in, int64_t nt, int64_t ntr, const double* ramp,
 int32_t ertm_rotate(const float* vx, const float* vz, int64_t n, double c, double s, float* ox, float* oz,
                     void* stream);
 
+/* Time-varying filter (qcomp.py:98-147): S Hann-windowed frames of L samples
+ * every hop samples of the (n, ntr) float64 record, each frame's spectrum
+ * (L/2+1 frequencies) times its complex response (S × (L/2+1) interleaved
+ * re/im float64), inverse, windowed overlap-add in frame order, divided by
+ * the summed squared window.  Host or device pointers; out is (n, ntr)
+ * float64. */
+int32_t ertm_stft_filter(const double* in, int64_t n, int64_t ntr, int32_t L, int32_t hop, int32_t S,
+                         const double* window, const double* response, double* out, void* stream);
+
 /* stack_images (pipeline.py:133-161): images is n_images pointers to (n,) float32. */
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream);

@@ -23,6 +23,8 @@ from typing import Any, Callable
 import numpy as np
 
 __all__ = [
+    "stft_filter",
+    "q_attenuation_response",
     "rotate_components",
     "mute_weights",
     "taper_ends",
@@ -1149,3 +1151,42 @@ def taper_ends(a: np.ndarray, fraction: float = 0.05) -> np.ndarray:
     out[:w] *= ramp[:, None]
     out[-w:] *= ramp[::-1][:, None]
     return out
+
+
+# ---------------------------------------------------------------------------
+# Data-domain Q filter — qcomp.py:44-147
+# ---------------------------------------------------------------------------
+def stft_filter(data: np.ndarray, dt: float, response_fn, nperseg: int = 128, overlap: float = 0.5) -> np.ndarray:
+    """qcomp.py:98-147 — Hann frames, per-frame response, windowed overlap-add."""
+    a = np.asarray(data, dtype=np.float64)
+    squeeze = a.ndim == 1
+    if squeeze:
+        a = a[:, None]
+    n = a.shape[0]
+    L = int(min(max(nperseg, 8), max(n, 8)))
+    hop = max(int(L * (1.0 - overlap)), 1)
+    win = np.hanning(L)
+    freqs = np.fft.rfftfreq(L, d=dt)
+    out = np.zeros_like(a)
+    weight = np.zeros(n)
+    for start in range(0, n, hop):
+        stop = min(start + L, n)
+        if stop - start < 4:
+            break
+        seg = np.zeros((L, a.shape[1]))
+        seg[: stop - start] = a[start:stop]
+        spec = np.fft.rfft(seg * win[:, None], axis=0)
+        resp = np.asarray(response_fn((start + 0.5 * L) * dt, freqs), dtype=np.complex128)
+        filt = np.fft.irfft(spec * resp[:, None], n=L, axis=0)
+        out[start:stop] += filt[: stop - start] * win[: stop - start, None]
+        weight[start:stop] += win[: stop - start] ** 2
+    out /= np.where(weight > 1e-12, weight, 1.0)[:, None]
+    return out[:, 0] if squeeze else out
+
+
+def q_attenuation_response(freqs, travel_time, q, f_ref, strength=1.0):
+    """qcomp.py:44-62 (amplitude and dispersion on)."""
+    f = np.abs(np.asarray(freqs, dtype=np.float64))
+    fs = np.where(f > 1e-9, f, 1e-9)
+    ts = float(travel_time) * float(strength)
+    return np.exp(-np.pi * f * ts / float(q)) * np.exp(1j * (-2.0 * f * ts / float(q) * np.log(fs / float(f_ref))))

@@ -284,8 +284,22 @@ def preprocess_case() -> dict[str, np.ndarray]:
     return out
 
 
+def qcomp_case() -> dict[str, np.ndarray]:
+    """qcomp.py:98-213: receiver-side compensation (the migrate preprocess hook)
+    and constant-Q attenuation through the short-time overlap-add filter."""
+    from ertm.qcomp import QCompensator, attenuate_record
+    rng = np.random.default_rng(41)
+    data = rng.normal(size=(300, 7)).astype(np.float32)
+    comp = QCompensator(config=QConfig(enabled=True, model="filter", alpha_c=0.8, gain_cap=30.0, f_ref=30.0),
+                        q_value=60.0)
+    return {"data": data, "dt": np.array(1e-3), "compensated": comp(data.astype(np.float64), 1e-3),
+            "attenuated": attenuate_record(data, 1e-3, 50.0, f_ref=30.0, nperseg=64),
+            "trace": attenuate_record(data[:, 0], 1e-3, 80.0, nperseg=96)}
+
+
 def main() -> None:
     cases = {
+        "qcomp": qcomp_case,
         "preprocess": preprocess_case,
         "numerics": numerics_case,
         "gsls": gsls_case,

@@ -26,3 +26,14 @@ def test_oracle_rotation_resampling_mute_taper_match_golden():
     for n in comps:
         assert np.array_equal((comps[n].astype(np.float64) * w).astype(np.float32), fx[f"mute_{n}"]), n
         assert np.array_equal(orc.taper_ends(comps[n], 0.05).astype(np.float32), fx[f"taper_{n}"]), n
+
+
+def test_oracle_q_filter_matches_golden():
+    fx = load("qcomp")
+    dt = float(fx["dt"])
+    got = orc.stft_filter(fx["data"], dt, lambda tc, f: orc.q_attenuation_response(f, max(tc, 1e-6), 50.0, 30.0),
+                          nperseg=64)
+    np.testing.assert_allclose(got, fx["attenuated"], rtol=0, atol=1e-12 * np.abs(fx["attenuated"]).max())
+    got = orc.stft_filter(fx["data"][:, 0], dt, lambda tc, f: orc.q_attenuation_response(f, max(tc, 1e-6), 80.0,
+                                                                                             30.0), nperseg=96)
+    np.testing.assert_allclose(got, fx["trace"], rtol=0, atol=1e-12 * np.abs(fx["trace"]).max())
