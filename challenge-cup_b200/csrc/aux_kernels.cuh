@@ -523,3 +523,122 @@ __global__ void k_stft_overlap_add(const double* __restrict__ filt, int64_t n, i
 }
 
 }  // namespace ertm
+
+namespace ertm {
+
+// ---------------------------------------------------------------------------
+// SEG-Y rev 1 trace samples ↔ float32 records (segy.py:103-155 reads with
+// segyio, segy.py:373-530 writes).  A trace block is 240 header bytes then ns
+// big-endian 4-byte samples, data sample format 5 (IEEE single) or 1 (IBM
+// System/360 hexadecimal single: sign, excess-64 base-16 exponent, 24-bit
+// fraction 0.F).  Records are (ns, width) float32, sample-major, so the
+// codec is a 32×32 shared-memory transpose: file reads run along samples,
+// record writes along traces.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t bswap32(uint32_t v) { return __byte_perm(v, 0, 0x0123); }
+
+// IBM → float32: |x| = F·2^(4(e−64)−24) is exact in double (leading bit at
+// most 2^227, least 2^−280); one round-to-nearest-even to float32 follows.
+__device__ __forceinline__ float ibm_to_float(uint32_t w) {
+  const uint32_t frac = w & 0x00ffffffu;
+  if (frac == 0) return __uint_as_float(w & 0x80000000u);
+  const int e16 = (int)((w >> 24) & 0x7fu);
+  const int p = 31 - __clz(frac);                         // leading bit of F, 0..23
+  const int e2 = p + 4 * (e16 - 64) - 24;                  // binary exponent of that bit
+  uint64_t bits = ((uint64_t)(e2 + 1023) << 52) | (((uint64_t)frac << (52 - p)) & 0x000fffffffffffffull);
+  bits |= (uint64_t)(w & 0x80000000u) << 32;
+  return __double2float_rn(__longlong_as_double((long long)bits));
+}
+
+// float32 → IBM, fraction rounded to nearest (ties to even); ±inf and NaN map
+// to the largest IBM magnitude; every finite float32 (denormals included) lies
+// inside the IBM exponent range.
+__device__ __forceinline__ uint32_t float_to_ibm(float x) {
+  const uint32_t u = __float_as_uint(x);
+  const uint32_t sign = u & 0x80000000u;
+  const uint32_t be = (u >> 23) & 0xffu;
+  uint32_t m = u & 0x7fffffu;
+  if (be == 0xffu) return sign | 0x7fffffffu;
+  int e2;
+  if (be == 0) {
+    if (m == 0) return sign;
+    e2 = -149;
+  } else {
+    m |= 0x800000u;
+    e2 = (int)be - 150;
+  }
+  const int lead = 31 - __clz(m) + e2;                     // |x| in [2^lead, 2^(lead+1))
+  int q = (lead >= 0 ? lead / 4 : -((-lead + 3) / 4)) + 1; // |x| in [16^(q−1), 16^q)
+  const int sh = e2 + 24 - 4 * q;                          // F = m·2^sh, F in [2^20, 2^24)
+  uint32_t F;
+  if (sh >= 0) {
+    F = m << sh;
+  } else {
+    const int r = -sh;                                     // 1..3 for normal inputs
+    const uint32_t rem = m & ((1u << r) - 1u), half = 1u << (r - 1);
+    F = m >> r;
+    if (rem > half || (rem == half && (F & 1u))) ++F;
+    if (F == (1u << 24)) {
+      F = 1u << 20;
+      ++q;
+    }
+  }
+  return sign | ((uint32_t)(q + 64) << 24) | F;
+}
+
+// Decode: output column c takes input trace order[c]; its samples go to
+// out[dest[c] + s·width[c]] (a column of that shot's (ns, width) record).
+// Grid: x over 32-column tiles, y over 32-sample tiles; block 32×8.
+__global__ void k_segy_decode(const uint8_t* __restrict__ traces, int64_t ns, int64_t tb, int64_t ncols,
+                              const int32_t* __restrict__ order, const int64_t* __restrict__ dest,
+                              const int32_t* __restrict__ width, int fmt, float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int64_t c0 = (int64_t)blockIdx.x * 32, s0 = (int64_t)blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += 8) {
+    const int64_t c = c0 + j, s = s0 + threadIdx.x;
+    float v = 0.f;
+    if (c < ncols && s < ns) {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(traces + (int64_t)order[c] * tb + 240);
+      const uint32_t word = bswap32(__ldg(w + s));
+      v = fmt == 1 ? ibm_to_float(word) : __uint_as_float(word);
+    }
+    tile[j][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int64_t s = s0 + i, c = c0 + threadIdx.x;
+    if (c < ncols && s < ns) out[dest[c] + s * (int64_t)width[c]] = tile[threadIdx.x][i];
+  }
+}
+
+// Encode a (ns, ntr) record: trace k's samples from column k, big-endian.
+__global__ void k_segy_encode(const float* __restrict__ rec, int64_t ns, int64_t ntr, int64_t tb, int fmt,
+                              uint8_t* __restrict__ traces) {
+  __shared__ uint32_t tile[32][33];
+  const int64_t c0 = (int64_t)blockIdx.x * 32, s0 = (int64_t)blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int64_t s = s0 + i, c = c0 + threadIdx.x;
+    uint32_t word = 0;
+    if (c < ntr && s < ns) {
+      const float v = rec[s * ntr + c];
+      word = bswap32(fmt == 1 ? float_to_ibm(v) : __float_as_uint(v));
+    }
+    tile[i][threadIdx.x] = word;
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += 8) {
+    const int64_t c = c0 + j, s = s0 + threadIdx.x;
+    if (c < ntr && s < ns) reinterpret_cast<uint32_t*>(traces + c * tb + 240)[s] = tile[threadIdx.x][j];
+  }
+}
+
+// The 240-byte trace headers, already big-endian, into their trace blocks.
+__global__ void k_segy_headers(const uint32_t* __restrict__ hdr, int64_t ntr, int64_t tb,
+                               uint8_t* __restrict__ traces) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ntr * 60) return;
+  const int64_t k = idx / 60, w = idx - k * 60;
+  reinterpret_cast<uint32_t*>(traces + k * tb)[w] = hdr[idx];
+}
+
+}  // namespace ertm

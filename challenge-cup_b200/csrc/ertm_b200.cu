@@ -2475,6 +2475,61 @@ int32_t ertm_stft_filter(const double* in, int64_t n, int64_t ntr, int32_t L, in
   });
 }
 
+int32_t ertm_segy_decode(const uint8_t* traces, int64_t n_traces, int64_t ns, int32_t fmt, int64_t ncols,
+                         const int32_t* order, const int64_t* dest, const int32_t* width, float* out,
+                         int64_t out_len, void* stream) {
+  return guarded([&] {
+    REQUIRE(traces && order && dest && width && out && n_traces >= 1 && ns >= 1 && ncols >= 1 && out_len >= 1,
+            "bad arguments");
+    REQUIRE(fmt == 1 || fmt == 5, "data sample format must be 1 (IBM float) or 5 (IEEE float)");
+    REQUIRE(!is_device_ptr(order) && !is_device_ptr(dest) && !is_device_ptr(width),
+            "column maps are host arrays");
+    for (int64_t c = 0; c < ncols; ++c) {
+      REQUIRE(order[c] >= 0 && order[c] < n_traces, "column reads a trace outside the file");
+      REQUIRE(width[c] >= 1 && dest[c] >= 0 && dest[c] + (ns - 1) * (int64_t)width[c] < out_len,
+              "column writes outside the output");
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t tb = 240 + 4 * ns;
+    InArray t(traces, (size_t)(n_traces * tb), st);
+    REQUIRE(reinterpret_cast<uintptr_t>(t.d) % 4 == 0, "trace section must be 4-byte aligned");
+    InArray o_(order, (size_t)ncols * 4, st), d_(dest, (size_t)ncols * 8, st), w_(width, (size_t)ncols * 4, st);
+    OutArray o(out, (size_t)out_len * 4, st);
+    if (o.host) CK(cudaMemsetAsync(o.d, 0, o.bytes, st));
+    const dim3 grid((unsigned)((ncols + 31) / 32), (unsigned)((ns + 31) / 32));
+    REQUIRE(grid.y <= 65535u, "too many samples per trace");
+    k_segy_decode<<<grid, dim3(32, 8), 0, st>>>(t.as<uint8_t>(), ns, tb, ncols, o_.as<int32_t>(),
+                                               d_.as<int64_t>(), w_.as<int32_t>(), fmt, o.as<float>());
+    ++g_launches;
+    CK(cudaGetLastError());
+    o.finish();
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_segy_encode(const float* rec, int64_t ns, int64_t ntr, int32_t fmt, const uint8_t* headers,
+                         uint8_t* traces, void* stream) {
+  return guarded([&] {
+    REQUIRE(rec && headers && traces && ns >= 1 && ntr >= 1, "bad arguments");
+    REQUIRE(fmt == 1 || fmt == 5, "data sample format must be 1 (IBM float) or 5 (IEEE float)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t tb = 240 + 4 * ns;
+    InArray r(rec, (size_t)(ns * ntr) * 4, st), h(headers, (size_t)ntr * 240, st);
+    REQUIRE(reinterpret_cast<uintptr_t>(h.d) % 4 == 0, "headers must be 4-byte aligned");
+    OutArray o(traces, (size_t)(ntr * tb), st);
+    REQUIRE(reinterpret_cast<uintptr_t>(o.d) % 4 == 0, "trace section must be 4-byte aligned");
+    const dim3 grid((unsigned)((ntr + 31) / 32), (unsigned)((ns + 31) / 32));
+    REQUIRE(grid.y <= 65535u, "too many samples per trace");
+    const int64_t nh = ntr * 60;
+    k_segy_headers<<<(unsigned)((nh + 255) / 256), 256, 0, st>>>(h.as<uint32_t>(), ntr, tb, o.as<uint8_t>());
+    k_segy_encode<<<grid, dim3(32, 8), 0, st>>>(r.as<float>(), ns, ntr, tb, fmt, o.as<uint8_t>());
+    g_launches += 2;
+    CK(cudaGetLastError());
+    o.finish();
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream) {
   return guarded([&] {

@@ -113,6 +113,8 @@ _SIGNATURES = {
     "ertm_taper": (_I32, [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P]),
     "ertm_rotate": (_I32, [_P, _P, C.c_int64, C.c_double, C.c_double, _P, _P, _P]),
     "ertm_stft_filter": (_I32, [_P, C.c_int64, C.c_int64, _I32, _I32, _I32, _P, _P, _P, _P]),
+    "ertm_segy_decode": (_I32, [_P, C.c_int64, C.c_int64, _I32, C.c_int64, _P, _P, _P, _P, C.c_int64, _P]),
+    "ertm_segy_encode": (_I32, [_P, C.c_int64, C.c_int64, _I32, _P, _P, _P]),
     "ertm_session_create": (_I32, [C.POINTER(C.c_void_p)]),
     "ertm_session_add": (_I32, [_P, C.POINTER(BatchShot), C.c_int64]),
     "ertm_session_advance": (_I32, [_P, _I32, C.POINTER(C.c_int64), _I32, C.POINTER(C.c_int32)]),

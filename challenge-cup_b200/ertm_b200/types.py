@@ -52,6 +52,12 @@ class GridSpec:
     def z_max(self) -> float:
         return float(self.z0 + (self.nz - 1) * self.dz)
 
+    def x_at(self, ix: int) -> float:
+        return float(self.x0 + ix * self.dx)
+
+    def z_at(self, iz: int) -> float:
+        return float(self.z0 + iz * self.dz)
+
     def index_of(self, x: float, z: float, *, clip: bool = True) -> tuple[int, int]:
         """Nearest node ``(ix, iz)``; Python's round (half to even) as in types.py:73-82."""
         ix = int(round((float(x) - self.x0) / self.dx))

@@ -276,6 +276,26 @@ int32_t ertm_rotate(const float* vx, const float* vz, int64_t n, double c, doubl
 int32_t ertm_stft_filter(const double* in, int64_t n, int64_t ntr, int32_t L, int32_t hop, int32_t S,
                          const double* window, const double* response, double* out, void* stream);
 
+/* SEG-Y rev 1 trace samples, replacing segyio's trace reads and writes in
+ * segy.py:103-155 (read_segy_shots, read_segy_image) and segy.py:373-530
+ * (write_segy_shot/shots/image).  A trace block is 240 header bytes followed
+ * by ns big-endian samples, format 1 (IBM hex float) or 5 (IEEE float).
+ *
+ * decode: traces is the trace section (n_traces blocks of 240 + 4·ns bytes,
+ * 4-byte aligned; host or device).  Output column c reads trace order[c] and
+ * writes its samples to out[dest[c] + s·width[c]], s < ns, so one call fills
+ * every shot's (ns, nrec) record of a file in its grouped, sorted order.
+ * order/dest/width are host arrays (ncols each), checked against n_traces and
+ * out_len (float32 elements) before the launch; out is host or device.
+ *
+ * encode: rec is (ns, ntr) float32; headers is ntr·240 bytes, big-endian,
+ * copied unchanged; traces receives the ntr trace blocks. */
+int32_t ertm_segy_decode(const uint8_t* traces, int64_t n_traces, int64_t ns, int32_t fmt, int64_t ncols,
+                         const int32_t* order, const int64_t* dest, const int32_t* width, float* out,
+                         int64_t out_len, void* stream);
+int32_t ertm_segy_encode(const float* rec, int64_t ns, int64_t ntr, int32_t fmt, const uint8_t* headers,
+                         uint8_t* traces, void* stream);
+
 /* stack_images (pipeline.py:133-161): images is n_images pointers to (n,) float32. */
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream);

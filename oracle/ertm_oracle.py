@@ -23,6 +23,10 @@ from typing import Any, Callable
 import numpy as np
 
 __all__ = [
+    "ibm_to_float32",
+    "float32_to_ibm",
+    "segy_bytes",
+    "segy_parse",
     "stft_filter",
     "q_attenuation_response",
     "rotate_components",
@@ -1190,3 +1194,90 @@ def q_attenuation_response(freqs, travel_time, q, f_ref, strength=1.0):
     fs = np.where(f > 1e-9, f, 1e-9)
     ts = float(travel_time) * float(strength)
     return np.exp(-np.pi * f * ts / float(q)) * np.exp(1j * (-2.0 * f * ts / float(q) * np.log(fs / float(f_ref))))
+
+
+# ---------------------------------------------------------------------------
+# SEG-Y rev 1 trace codec — segy.py:103-155 (reads) and :373-554 (writes),
+# which go through segyio 1.9.15 (a pinned dependency, absent here).  This
+# restates the standard's layout with struct, one field at a time, and the
+# IBM System/360 hexadecimal float from its definition
+#   x = (−1)^s · 0.F · 16^(e − 64),  F a 24-bit fraction, e 7 bits.
+# ---------------------------------------------------------------------------
+SEGY_BIN_POS = {"Interval": (3217, ">H"), "Samples": (3221, ">H"), "Format": (3225, ">h"),
+                "Sorting": (3229, ">h"), "SEGYRevision": (3501, ">H"), "TraceFlag": (3503, ">h"),
+                "ExtendedHeaders": (3505, ">h")}          # 1-based file byte positions
+SEGY_TRACE_POS = {"FieldRecord": (9, ">i"), "TraceNumber": (13, ">i"), "CDP": (21, ">i"), "offset": (37, ">i"),
+                  "SourceGroupScalar": (71, ">h"), "SourceX": (73, ">i"), "SourceY": (77, ">i"),
+                  "GroupX": (81, ">i"), "GroupY": (85, ">i"), "TRACE_SAMPLE_COUNT": (115, ">H"),
+                  "TRACE_SAMPLE_INTERVAL": (117, ">H")}   # 1-based positions inside a trace header
+
+
+def ibm_to_float32(words) -> np.ndarray:
+    """IBM words (as unsigned integers) → float32: exact in float64, one rounding."""
+    w = np.asarray(words, dtype=np.uint64)
+    frac = (w & 0xFFFFFF).astype(np.float64)
+    e = ((w >> 24) & 0x7F).astype(np.int64)
+    sign = np.where((w >> 31) & 1, -1.0, 1.0)
+    with np.errstate(over="ignore"):                     # beyond float32 range → ±inf
+        return (sign * np.ldexp(frac, 4 * (e - 64) - 24)).astype(np.float32)
+
+
+def float32_to_ibm(values) -> np.ndarray:
+    """float32 → IBM words, fraction rounded to nearest, ties to even; ±inf/NaN → largest magnitude."""
+    x = np.asarray(values, dtype=np.float32).astype(np.float64).reshape(-1)
+    out = np.zeros(x.size, dtype=np.uint64)
+    for i, v in enumerate(x):
+        sign = 0x80000000 if np.signbit(v) else 0
+        if not np.isfinite(v):
+            out[i] = sign | 0x7FFFFFFF
+            continue
+        a = abs(v)
+        if a == 0.0:
+            out[i] = sign
+            continue
+        _, ex = np.frexp(a)                     # a in [2^(ex−1), 2^ex)
+        q = (int(ex) - 1) // 4 + 1              # a in [16^(q−1), 16^q)
+        F = int(np.rint(np.ldexp(a, 24 - 4 * q)))   # exact scaling, then half-to-even
+        if F == 1 << 24:
+            F, q = 1 << 20, q + 1
+        out[i] = sign | ((q + 64) << 24) | F
+    return out.reshape(np.shape(values)).astype(np.uint32)
+
+
+def segy_bytes(rec: np.ndarray, headers: list[dict], interval: int, fmt: int, text: str) -> bytes:
+    """A whole SEG-Y file: rec is (ns, ntr) float32, headers one dict per trace."""
+    import struct
+    rec = np.asarray(rec, dtype=np.float32)
+    ns, ntr = rec.shape
+    head = bytearray(text[:3200].ljust(3200).encode("cp037")) + bytearray(400)
+    for name, val in (("Interval", interval), ("Samples", ns), ("Format", fmt), ("Sorting", 1),
+                      ("SEGYRevision", 0x0100), ("TraceFlag", 1), ("ExtendedHeaders", 0)):
+        pos, f = SEGY_BIN_POS[name]
+        struct.pack_into(f, head, pos - 1, val)
+    body = bytearray()
+    for k in range(ntr):
+        th = bytearray(240)
+        for name, val in headers[k].items():
+            pos, f = SEGY_TRACE_POS[name]
+            struct.pack_into(f, th, pos - 1, int(val))
+        col = rec[:, k]
+        words = float32_to_ibm(col) if fmt == 1 else col.view(np.uint32)
+        body += th + np.asarray(words, dtype=">u4").tobytes()
+    return bytes(head + body)
+
+
+def segy_parse(blob: bytes) -> tuple[dict, list[dict], np.ndarray]:
+    """(binary header fields, trace header dicts, samples (ns, ntr) float32) of a SEG-Y file."""
+    import struct
+    binh = {n: struct.unpack_from(f, blob, p - 1)[0] for n, (p, f) in SEGY_BIN_POS.items()}
+    ns, fmt = binh["Samples"], binh["Format"]
+    first = 3600 + 3200 * max(binh["ExtendedHeaders"], 0)
+    tb = 240 + 4 * ns
+    ntr = (len(blob) - first) // tb
+    heads, cols = [], []
+    for k in range(ntr):
+        base = first + k * tb
+        heads.append({n: struct.unpack_from(f, blob, base + p - 1)[0] for n, (p, f) in SEGY_TRACE_POS.items()})
+        words = np.frombuffer(blob, dtype=">u4", count=ns, offset=base + 240).astype(np.uint32)
+        cols.append(ibm_to_float32(words) if fmt == 1 else words.view(np.float32))
+    return binh, heads, np.stack(cols, axis=1) if cols else np.zeros((ns, 0), np.float32)

@@ -297,8 +297,42 @@ def qcomp_case() -> dict[str, np.ndarray]:
             "trace": attenuate_record(data[:, 0], 1e-3, 80.0, nperseg=96)}
 
 
+def store_case() -> dict[str, np.ndarray]:
+    """data.py:73-297: the reference's NumpyDataStore writes one model, one
+    three-component shot and one image; the three .npz files are committed
+    under tests/golden/store/ as written, and this case holds what went in."""
+    import shutil
+    import tempfile
+
+    from ertm.data import NumpyDataStore
+    from ertm.types import ImageResult, ShotRecord
+    model = layered_model(19, 13, 10.0, seed=5)
+    model.name, model.meta = "store-model", {"builder": "layered", "layers": 3}
+    rng = np.random.default_rng(9)
+    nt, nrec = 40, 6
+    comps = {n: rng.normal(size=(nt, nrec)).astype(np.float32) for n in ("p", "vx", "vz")}
+    shot = ShotRecord(data=comps["p"], dt=5e-4, t=np.arange(nt) * 5e-4,
+                      receivers=ReceiverSpec(x=np.linspace(10.0, 160.0, nrec), z=np.full(nrec, 20.0), component="p"),
+                      source=SourceSpec(x=90.0, z=20.0, f0=25.0, amplitude=2.0, delay=0.01, mechanism="shear"),
+                      meta={"synthetic": True, "engine": "elastic"}, components=comps)
+    image = ImageResult(image=rng.normal(size=model.grid.shape).astype(np.float32), grid=model.grid, mode="ps",
+                        meta={"condition": "normalized", "n_shots": 3})
+    out = HERE / "store"
+    out.mkdir(exist_ok=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        store = NumpyDataStore(tmp)
+        for written in (store.save_model(model, "model"), store.save_shot(shot, "shot"),
+                        store.save_image(image, "image")):
+            shutil.copyfile(written, out / written.name)
+    return {"vp": model.vp, "vs": model.vs, "rho": model.rho, "qp": model.qp, "qs": model.qs,
+            "grid": np.array([19, 13, 10.0, 10.0, 0.0, 0.0]), "data": shot.data, "t": shot.t,
+            "rx": shot.receivers.x, "rz": shot.receivers.z, "comp_p": comps["p"], "comp_vx": comps["vx"],
+            "comp_vz": comps["vz"], "image": image.image}
+
+
 def main() -> None:
     cases = {
+        "store": store_case,
         "qcomp": qcomp_case,
         "preprocess": preprocess_case,
         "numerics": numerics_case,
