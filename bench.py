@@ -48,6 +48,8 @@ def parse_args() -> argparse.Namespace:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=48)
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs in the serving run (0: no serving run)")
+    ap.add_argument("--no-adjacent", action="store_true",
+                    help="skip timing the steps either side of the path (preprocessing, Q filter, SEG-Y, stack)")
     return ap.parse_args()
 
 
@@ -328,6 +330,157 @@ def serving_run(n_jobs: int) -> dict:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def adjacent_rows_run(wl, peak: float, cpu: bool) -> dict:
+    """The steps either side of the path, on one job's data (all shots of the
+    workload), device-resident, each call timed with CUDA events after an L2
+    flush: record preprocessing (sinc resampling from a 1 ms field record,
+    direct-wave mute, end taper), the data-domain Q filter, SEG-Y decoding of
+    the job's records, per-shot image post-processing and the stack.  Bytes
+    are algorithmic (inputs read once, outputs written once); ``cpu_s`` is the
+    oracle on the same call (single thread), where ``cpu`` is set."""
+    import ctypes as C
+
+    import torch
+
+    from ertm_b200 import _lib, segy
+    from ertm_b200.preprocess import resample_weights
+    from oracle import ertm_oracle as orc
+
+    L = _lib.lib()
+    g = wl.model.grid
+    n_shots, ncomp, nt, nrec = len(wl.sources), len(wl.components), wl.nt, wl.receivers.nrec
+    ntr = n_shots * ncomp * nrec                      # every trace of the job side by side
+    npix = g.nx * g.nz
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    rec = torch.randn((nt, ntr), generator=gen, device="cuda", dtype=torch.float32)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed(call, reps=5):
+        for _ in range(2):
+            call()
+        ms = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            call()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    def cpu_time(fn):
+        if not cpu:
+            return None
+        t0 = time.perf_counter()
+        fn()
+        return time.perf_counter() - t0
+
+    rows = {}
+
+    def add(name, ms, nbytes, what, cpu_s=None):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        rows[name] = {"ms": ms, "bytes": int(nbytes), "gbs": gbs, "frac": gbs / peak, "what": what, "cpu_s": cpu_s}
+
+    # sinc resampling: a 1 ms record of the same duration to the propagation dt
+    n_in = int(np.floor((nt - 1) * wl.dt / 1e-3)) + 1
+    w, off0 = resample_weights(n_in, 1e-3, wl.dt)
+    n_out = w.shape[0]
+    rin = torch.randn((n_in, ntr), generator=gen, device="cuda", dtype=torch.float32)
+    rout = torch.empty((n_out, ntr), device="cuda", dtype=torch.float32)
+    wd, od = torch.from_numpy(w).cuda(), torch.from_numpy(off0).cuda()
+    ms = timed(lambda: _lib.check(L.ertm_resample(rin.data_ptr(), n_in, ntr, wd.data_ptr(), od.data_ptr(),
+                                                  w.shape[1], n_out, rout.data_ptr(), None), "resample"))
+    host_in = rin[:, :nrec].cpu().numpy()
+    add("resample", ms, 4 * (n_in + n_out) * ntr + w.nbytes + off0.nbytes,
+        f"sinc resampling 1 ms -> {wl.dt * 1e3:.4f} ms, {n_in}->{n_out} samples x {ntr} traces",
+        None if not cpu else cpu_time(lambda: orc.resample_sinc(host_in, 1e-3, wl.dt)) * (ntr / nrec))
+
+    # direct-wave mute and end taper over every trace of the job
+    t = torch.arange(nt, device="cuda", dtype=torch.float64) * wl.dt
+    start = torch.linspace(0.05, 0.4, ntr, device="cuda", dtype=torch.float64)
+    end = start + 0.02
+    out = torch.empty_like(rec)
+    ms = timed(lambda: _lib.check(L.ertm_mute(rec.data_ptr(), nt, ntr, t.data_ptr(), start.data_ptr(),
+                                              end.data_ptr(), out.data_ptr(), None), "mute"))
+    add("mute", ms, 8 * nt * ntr + 8 * nt + 16 * ntr, f"cosine direct-wave mute, {nt} x {ntr}")
+    wt = max(int(0.05 * nt), 1)
+    ramp = torch.from_numpy(0.5 - 0.5 * np.cos(np.pi * (np.arange(wt) + 0.5) / wt)).cuda()
+    ms = timed(lambda: _lib.check(L.ertm_taper(rec.data_ptr(), nt, ntr, ramp.data_ptr(), wt, out.data_ptr(), None),
+                                  "taper"))
+    host = rec[:, :nrec].cpu().numpy()
+    add("taper", ms, 8 * nt * ntr + 8 * wt, f"end taper 5%, {nt} x {ntr}",
+        None if not cpu else cpu_time(lambda: orc.taper_ends(host, 0.05)) * (ntr / nrec))
+
+    # data-domain Q filter on the job's pressure records (float64, nperseg 128, 50 % overlap)
+    nq = n_shots * nrec
+    q_in = rec[:, :nq].double().contiguous()
+    q_out = torch.empty_like(q_in)
+    Lf, hop = 128, 64
+    S = len(range(0, nt, hop)) - sum(1 for s in range(0, nt, hop) if min(s + Lf, nt) - s < 4)
+    freqs = np.fft.rfftfreq(Lf, d=wl.dt)
+    resp = np.stack([orc.q_attenuation_response(freqs, (s * hop + 0.5 * Lf) * wl.dt, 60.0, 30.0)
+                     for s in range(S)])
+    resp_d = torch.from_numpy(np.ascontiguousarray(resp).view(np.float64)).cuda()
+    win = torch.from_numpy(np.hanning(Lf)).cuda()
+    ms = timed(lambda: _lib.check(L.ertm_stft_filter(q_in.data_ptr(), nt, nq, Lf, hop, S, win.data_ptr(),
+                                                     resp_d.data_ptr(), q_out.data_ptr(), None), "stft"))
+    qh = q_in[:, :nrec].cpu().numpy()
+    add("q_filter", ms, 16 * nt * nq + resp.nbytes, f"STFT Q filter, {nt} x {nq} float64, {S} frames of {Lf}",
+        None if not cpu else cpu_time(lambda: orc.stft_filter(
+            qh, wl.dt, lambda tc, f: orc.q_attenuation_response(f, max(tc, 1e-6), 60.0, 30.0))) * (nq / nrec))
+
+    # SEG-Y: the job's records as one IEEE file section, decoded into per-record (nt, nrec) blocks
+    tb = 240 + 4 * nt
+    section = torch.zeros(ntr * tb, dtype=torch.uint8, device="cuda")
+    hdr = np.zeros(ntr, dtype=segy.TRACE_DTYPE)
+    hdr["TraceNumber"] = np.arange(1, ntr + 1)
+    hdr["TRACE_SAMPLE_COUNT"] = nt
+    hb = hdr.view(np.uint8)
+    _lib.check(L.ertm_segy_encode(rec.data_ptr(), nt, ntr, 5, hb.ctypes.data, section.data_ptr(), None), "encode")
+    perm = np.arange(ntr).reshape(-1, nrec)
+    order = np.ascontiguousarray(perm.reshape(-1), dtype=np.int32)
+    dest = np.ascontiguousarray((np.arange(ntr) // nrec) * nt * nrec + np.arange(ntr) % nrec, dtype=np.int64)
+    width = np.full(ntr, nrec, dtype=np.int32)
+    dec = torch.empty(nt * ntr, dtype=torch.float32, device="cuda")
+    ms = timed(lambda: _lib.check(L.ertm_segy_decode(section.data_ptr(), ntr, nt, 5, ntr, order.ctypes.data,
+                                                     dest.ctypes.data, width.ctypes.data, dec.data_ptr(),
+                                                     dec.numel(), None), "decode"))
+    blob = None
+    if cpu:
+        blob = orc.segy_bytes(host, [{"TRACE_SAMPLE_COUNT": nt}] * nrec, 1000, 5, "")
+    add("segy_decode", ms, ntr * tb + 4 * nt * ntr + 16 * ntr,
+        f"SEG-Y IEEE decode + transpose, {ntr} traces of {nt} samples into {ntr // nrec} records",
+        None if not cpu else cpu_time(lambda: orc.segy_parse(blob)) * (ntr / nrec))
+
+    # per-shot post-processing (normalisation by illumination, Laplacian, mask) and the stack
+    num = torch.randn((npix,), generator=gen, device="cuda", dtype=torch.float64)
+    ill = torch.rand((npix,), generator=gen, device="cuda", dtype=torch.float64) + 0.1
+    img = torch.empty((npix,), device="cuda", dtype=torch.float32)
+    ms = timed(lambda: _lib.check(L.ertm_postprocess(g.nz, g.nx, float(g.dx), float(g.dz), num.data_ptr(),
+                                                     ill.data_ptr(), None, 1, 0, 1e-6, 1, 1.0, 20, 1,
+                                                     img.data_ptr(), None), "postprocess"))
+    nh, ih = num.view(g.nz, g.nx).cpu().numpy(), ill.view(g.nz, g.nx).cpu().numpy()
+    add("postprocess", ms, 16 * npix + 4 * npix, f"illumination normalisation + Laplacian + PML mask, {g.nz} x {g.nx}",
+        None if not cpu else cpu_time(lambda: orc.postprocess(nh / (ih + 1e-6), g.dx, g.dz, laplacian_on=True,
+                                                              lowpass_fraction=1.0, npml=20, boundary="cpml")))
+    imgs = torch.randn((n_shots, npix), generator=gen, device="cuda", dtype=torch.float32)
+    acc = torch.zeros((npix,), device="cuda", dtype=torch.float64)
+    fin = torch.empty((npix,), device="cuda", dtype=torch.float32)
+    ptrs = (C.c_void_p * n_shots)(*[imgs[i].data_ptr() for i in range(n_shots)])
+
+    def stack():
+        acc.zero_()
+        _lib.check(L.ertm_stack_partial(n_shots, npix, C.cast(ptrs, C.c_void_p), 1, acc.data_ptr(), None), "stack")
+        _lib.check(L.ertm_stack_finish(npix, acc.data_ptr(), n_shots, fin.data_ptr(), None), "finish")
+    ms = timed(stack)
+    ih = [im.view(g.nz, g.nx).cpu().numpy() for im in imgs]
+    add("stack", ms, n_shots * 4 * npix + 8 * npix + 4 * npix,
+        f"per-shot max-normalised float64 stack of {n_shots} images {g.nz} x {g.nx}",
+        None if not cpu else cpu_time(lambda: orc.stack_images(ih, normalize=True)))
+    return rows
+
+
 def run_ours(args, dist: Dist) -> None:
     import ctypes as C
 
@@ -467,6 +620,9 @@ def run_ours(args, dist: Dist) -> None:
         serving = serving_run(args.serve_jobs)
 
     peak, peak_kind = measured_hbm_peak()
+    adjacent = None
+    if dist.world == 1 and not args.no_adjacent:
+        adjacent = adjacent_rows_run(wl, peak, cpu=not args.no_cpu_baseline)
     step_ms = float(tot.value) / max(int(cnt.value), 1)
     achieved = float(byt.value) / (float(tot.value) * 1e-3) / 1e9 if tot.value > 0 else 0.0
     cpu = None
@@ -501,6 +657,7 @@ def run_ours(args, dist: Dist) -> None:
                      "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "serving": serving,
+        "adjacent_rows": adjacent,
         "autotune": tuned,
         "stage_timeouts": int(L.ertm_stage_timeouts()),
         "clocks": clk,

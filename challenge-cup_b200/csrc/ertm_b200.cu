@@ -143,6 +143,25 @@ FftPair image_fft(int nz, int nx, cudaStream_t st) {
   return p;
 }
 
+// Batched 1-D plans of the short-time Q filter (L-point frames, `batch` of
+// them), cached by frame length, batch and stream.
+std::map<std::tuple<int, int64_t, cudaStream_t>, FftPair> g_stft_plans;
+
+FftPair stft_fft(int L, int64_t batch, cudaStream_t st) {
+  std::lock_guard<std::mutex> lock(g_fft_mutex);
+  auto key = std::make_tuple(L, batch, st);
+  auto it = g_stft_plans.find(key);
+  if (it != g_stft_plans.end()) return it->second;
+  const int F = L / 2 + 1;
+  int dims[1] = {L};
+  FftPair p;
+  CKFFT(cufftPlanMany(&p.fwd, 1, dims, nullptr, 1, L, nullptr, 1, F, CUFFT_D2Z, (int)batch));
+  CKFFT(cufftPlanMany(&p.inv, 1, dims, nullptr, 1, F, nullptr, 1, L, CUFFT_Z2D, (int)batch));
+  CKFFT(cufftSetStream(p.fwd, st));
+  CKFFT(cufftSetStream(p.inv, st));
+  g_stft_plans[key] = p;
+  return p;
+}
 
 size_t round64(size_t n) { return (n + 63) / 64 * 64; }
 
@@ -2450,21 +2469,12 @@ int32_t ertm_stft_filter(const double* in, int64_t n, int64_t ntr, int32_t L, in
     const int64_t nf = batch * L;
     k_stft_frames<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(a.as<double>(), n, ntr, L, hop, S, W.as<double>(),
                                                                frames.as<double>());
-    cufftHandle fwd = 0, inv = 0;
-    int dims[1] = {L};
-    CKFFT(cufftPlanMany(&fwd, 1, dims, nullptr, 1, L, nullptr, 1, F, CUFFT_D2Z, (int)batch));
-    struct Plan {
-      cufftHandle h;
-      ~Plan() { cufftDestroy(h); }
-    } pf{fwd};
-    CKFFT(cufftPlanMany(&inv, 1, dims, nullptr, 1, F, nullptr, 1, L, CUFFT_Z2D, (int)batch));
-    Plan pi{inv};
-    CKFFT(cufftSetStream(fwd, st));
-    CKFFT(cufftSetStream(inv, st));
-    CKFFT(cufftExecD2Z(fwd, frames.as<cufftDoubleReal>(), spec.as<cufftDoubleComplex>()));
+    REQUIRE(batch <= INT32_MAX, "too many frames for one batched transform");
+    const FftPair plan = stft_fft(L, batch, st);
+    CKFFT(cufftExecD2Z(plan.fwd, frames.as<cufftDoubleReal>(), spec.as<cufftDoubleComplex>()));
     const int64_t ns = batch * F;
     k_stft_response<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(spec.as<double2>(), ntr, F, S, R.as<double2>());
-    CKFFT(cufftExecZ2D(inv, spec.as<cufftDoubleComplex>(), frames.as<cufftDoubleReal>()));
+    CKFFT(cufftExecZ2D(plan.inv, spec.as<cufftDoubleComplex>(), frames.as<cufftDoubleReal>()));
     const int64_t no = n * ntr;
     k_stft_overlap_add<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(frames.as<double>(), n, ntr, L, hop, S,
                                                                     W.as<double>(), o.as<double>());

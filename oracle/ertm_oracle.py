@@ -1224,7 +1224,8 @@ def ibm_to_float32(words) -> np.ndarray:
 
 def float32_to_ibm(values) -> np.ndarray:
     """float32 → IBM words, fraction rounded to nearest, ties to even; ±inf/NaN → largest magnitude."""
-    x = np.asarray(values, dtype=np.float32).astype(np.float64).reshape(-1)
+    with np.errstate(invalid="ignore"):                  # signalling NaN payloads widen quietly
+        x = np.asarray(values, dtype=np.float32).astype(np.float64).reshape(-1)
     out = np.zeros(x.size, dtype=np.uint64)
     for i, v in enumerate(x):
         sign = 0x80000000 if np.signbit(v) else 0
