@@ -1344,6 +1344,10 @@ struct TickItem {
 };
 
 std::atomic<int> g_tick_lanes{0};   // 0 automatic, 1 or 2 lanes
+// Which works share a lane: 0 alternate works (a shot's replay step on one
+// lane, its backward step on the other), 1 alternate shots (both steps of a
+// shot on one lane, so the lanes carry equal mixes).
+std::atomic<int> g_lane_assign{0};
 std::atomic<int> g_autotune{1};     // tune batched tick launches online
 
 // ---------------------------------------------------------------------------
@@ -1478,9 +1482,12 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
     WorkSetB ws[kLanes]{};
     int tile0[kLanes] = {0, 0};
     const Prop* hosts[kLanes][MAX_BATCH_WORKS];
+    const bool by_shot = g_lane_assign.load() == 1;
+    int shot_no = 0;
     for (size_t k = c0; k < c1; ++k) {
       const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
-      const int l = lanes == 2 ? (int)((k - c0) & 1) : 0;
+      if (k > c0 && items[k]->run != items[k - 1]->run) ++shot_no;
+      const int l = lanes == 2 ? (by_shot ? (shot_no & 1) : (int)((k - c0) & 1)) : 0;
       StepWork w = items[k]->w;
       w.tile0 = tile0[l];
       w.tiles_x = (P.h.nxp + TILE_X - 1) / TILE_X;
@@ -1849,6 +1856,13 @@ int32_t ertm_set_tick_lanes(int32_t lanes) {
   return guarded([&] {
     REQUIRE(lanes >= 0 && lanes <= 2, "tick lanes must be 0 (automatic), 1 or 2");
     g_tick_lanes.store(lanes);
+  });
+}
+
+int32_t ertm_set_lane_assign(int32_t mode) {
+  return guarded([&] {
+    REQUIRE(mode == 0 || mode == 1, "lane assignment must be 0 (alternate works) or 1 (alternate shots)");
+    g_lane_assign.store(mode);
   });
 }
 

@@ -129,6 +129,10 @@ int32_t ertm_set_tile_split(int32_t mode);
  * alternated over two lanes on separate streams (0 = automatic: two when the
  * group has at least 4 works and enough tiles).  Results are identical. */
 int32_t ertm_set_tick_lanes(int32_t lanes);
+/* With two lanes: 0 alternates works between them (a shot's replay step on
+ * one, its backward step on the other), 1 alternates shots (both steps of a
+ * shot on one lane).  Results do not depend on it. */
+int32_t ertm_set_lane_assign(int32_t mode);
 /* Online autotuning of batched ticks (default on): the first ticks of each
  * group shape (engine, order, works, size class) try tile heights 8/16/32,
  * split off/on and one or two lanes, timed with CUDA events; the fastest is

@@ -296,16 +296,18 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
     imager = RTMImager(ImagingConfig(condition="normalized", checkpoint_mb=2.0),
                        SolverConfig(nt=260, dt=4e-4, boundary="free", engine="elastic"))
     out = {}
-    for mode, lanes in ((1, 1), (2, 1), (2, 2), (1, 2)):
+    for mode, lanes, assign in ((1, 1, 0), (2, 1, 0), (2, 2, 0), (1, 2, 0), (2, 2, 1), (1, 2, 1)):
         _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
         _lib.check(_lib.lib().ertm_set_tick_lanes(lanes), "lanes")
+        _lib.check(_lib.lib().ertm_set_lane_assign(assign), "lane assignment")
         try:
-            out[mode, lanes] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
+            out[mode, lanes, assign] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
         finally:
             _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
             _lib.check(_lib.lib().ertm_set_tick_lanes(0), "lanes")
-    for key in ((2, 1), (2, 2), (1, 2)):
-        for a, b in zip(out[1, 1], out[key]):
+            _lib.check(_lib.lib().ertm_set_lane_assign(0), "lane assignment")
+    for key in ((2, 1, 0), (2, 2, 0), (1, 2, 0), (2, 2, 1), (1, 2, 1)):
+        for a, b in zip(out[1, 1, 0], out[key]):
             for x1, x2 in zip(a, b):
                 assert np.array_equal(x1.image, x2.image), (key, x1.mode)
 
