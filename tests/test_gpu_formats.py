@@ -147,3 +147,49 @@ def test_image_roundtrip(tmp_path):
     assert back.shape == grid.shape and dz == pytest.approx(grid.dz, abs=1e-6)
     assert np.allclose(x, np.arange(grid.nx) * grid.dx, atol=1e-6)
     assert np.array_equal(back, image.image)
+
+
+def test_extended_headers_single_trace_and_limits(tmp_path):
+    """A file with one extended textual header and a single trace; a shot limit."""
+    from ertm_b200 import segy
+    rec = np.arange(37, dtype=np.float32)[:, None] * 0.5 - 3.0
+    blob = bytearray(orc.segy_bytes(rec, [{"SourceX": 7, "GroupX": 9, "TRACE_SAMPLE_COUNT": 37}], 250, 1, "x"))
+    blob[3504:3506] = (1).to_bytes(2, "big")            # one extended textual header follows the binary header
+    blob[3600:3600] = b"\x40" * 3200
+    p = tmp_path / "ext.sgy"
+    p.write_bytes(bytes(blob))
+    (s,) = segy.read_segy_shots(p)
+    assert s.data.shape == (37, 1) and s.dt == pytest.approx(2.5e-4)
+    assert np.array_equal(s.data, orc.ibm_to_float32(orc.float32_to_ibm(rec)))
+    assert s.source.x == 7.0 and s.receivers.x.tolist() == [9.0]
+    shots = [_make_shot(100.0 + 50 * k, nrec=3, nt=20) for k in range(4)]
+    segy.write_segy_shots(shots, tmp_path / "four.sgy")
+    two = segy.read_segy_shots(tmp_path / "four.sgy", segy.SegYReadOptions(shot_limit=2))
+    assert [r.source.x for r in two] == [100.0, 150.0]
+    for r, s0 in zip(two, shots):
+        assert np.array_equal(r.data, s0.data)
+
+
+def test_decode_rejects_columns_outside_the_file_or_output():
+    import ctypes as C
+    from ertm_b200 import _lib
+    L = _lib.lib()
+    ns, ntr = 8, 3
+    section = np.zeros(ntr * (240 + 4 * ns), dtype=np.uint8)
+    out = np.zeros(ns * ntr, dtype=np.float32)
+
+    def call(order, dest, width, fmt=5, out_len=out.size):
+        o = np.asarray(order, dtype=np.int32)
+        d = np.asarray(dest, dtype=np.int64)
+        w = np.asarray(width, dtype=np.int32)
+        return L.ertm_segy_decode(section.ctypes.data, ntr, ns, fmt, o.size, o.ctypes.data, d.ctypes.data,
+                                  w.ctypes.data, out.ctypes.data, out_len, None)
+    assert call([0, 1, 2], [0, 1, 2], [3, 3, 3]) == 0
+    assert call([0, 3], [0, 1], [3, 3]) != 0                 # trace 3 of 3
+    assert call([0, -1], [0, 1], [3, 3]) != 0
+    assert call([0, 1], [0, 22], [3, 3]) != 0                # 22 + 7·3 beyond 24 floats
+    assert call([0], [0], [0]) != 0
+    assert call([0], [0], [1], fmt=3) != 0
+    assert "outside" in _lib.last_error() or "format" in _lib.last_error()
+    bad = C.c_int32(0)
+    assert L.ertm_segy_encode(None, 1, 1, 5, C.addressof(bad), C.addressof(bad), None) != 0
