@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from .exceptions import ImagingError
-from .imaging import RTMImager, ShotMigrator, postprocess_image
+from .imaging import RTMImager, ShotMigrator
 from .types import ImageResult
 
 
@@ -34,7 +34,7 @@ class _Prepared:
     store: Any
     start_step: int
     cfg: _lib.MigrateConfig
-    record: np.ndarray
+    record: list[np.ndarray]                     # per component, (nt, nrec) float32
     wavelet: np.ndarray
     modes: tuple[str, ...]
     acc: Any = None
@@ -60,6 +60,9 @@ class BatchMigrator:
     def __init__(self, imager: RTMImager, *, memory_budget: int | None = None) -> None:
         self.imager = imager
         self.memory_budget = memory_budget
+        # per shot of the last migrate_shots call: its post-processed images,
+        # (n_modes, nz, nx) float32 on the device (the host images are copies)
+        self.device_images: list = []
 
     def _budget(self) -> int:
         if self.memory_budget is not None:
@@ -76,13 +79,17 @@ class BatchMigrator:
         if len(model_list) != len(shots):
             raise ImagingError("one model per shot (or one model for all)")
         results: list[list[ImageResult] | None] = [None] * len(shots)
+        self.device_images = [None] * len(shots)
         group: list[tuple[int, _Prepared]] = []
         used = 0
         budget = self._budget()
+        checked: set[int] = set()
         for k, (shot, model) in enumerate(zip(shots, model_list)):
             try:
                 shot.validate()
-                model.validate()
+                if id(model) not in checked:        # one model often serves every shot
+                    model.validate()
+                    checked.add(id(model))
             except ValueError as exc:
                 raise ImagingError(f"invalid imaging input: {exc}") from exc
             mig = ShotMigrator(self.imager, model)
@@ -106,7 +113,7 @@ class BatchMigrator:
         pairs, store, start = mig._prepare(shot.source, shot.receivers, modes, len(w))
         names = list(record)
         cfg = mig._config(pairs, names, store, start, len(w))
-        rec = np.ascontiguousarray(np.stack([np.asarray(record[n], dtype=np.float32) for n in names]))
+        rec = [np.ascontiguousarray(record[n], dtype=np.float32) for n in names]
         return _Prepared(mig, shot, pairs, store, start, cfg, rec, w, modes)
 
     def _run(self, group: list[tuple[int, _Prepared]], results: list) -> None:
@@ -117,7 +124,9 @@ class BatchMigrator:
         for i, (_, p) in enumerate(group):
             g = p.mig.model.grid
             p.acc = torch.zeros((3, len(p.pairs), g.nz, g.nx), dtype=torch.float64, device="cuda")
-            rec = torch.from_numpy(p.record).cuda()
+            rec = torch.empty((len(p.record),) + p.record[0].shape, dtype=torch.float32, device="cuda")
+            for c, comp in enumerate(p.record):         # one copy per component, no host-side stacking
+                rec[c].copy_(torch.from_numpy(comp))
             keep.append(rec)
             s = shots[i]
             s.fwd = p.mig.prop.handle
@@ -129,14 +138,28 @@ class BatchMigrator:
             s.illum = _lib.ptr(p.acc[1])
             s.rillum = _lib.ptr(p.acc[2])
         _lib.check(_lib.lib().ertm_migrate_batch(len(group), shots), "migrate_batch")
+        L = _lib.lib()
         for k, p in group:
             p.mig.prop._psi_allocated = p.mig.back._psi_allocated = True
             im = self.imager
             cond = str(im.config.condition).lower()
             out = []
-            acc = p.acc.cpu().numpy()
+            # post-processing reads the accumulators where they are; only the
+            # float32 images come back to the host
+            g = p.mig.model.grid
+            a = p.mig._post_args()
+            img = torch.empty((len(p.modes), g.nz, g.nx), dtype=torch.float32, device="cuda")
+            for j in range(len(p.modes)):
+                _lib.check(L.ertm_postprocess(g.nz, g.nx, float(a["dx"]), float(a["dz"]), _lib.ptr(p.acc[0, j]),
+                                              _lib.ptr(p.acc[1, j]), _lib.ptr(p.acc[2, j]), int(a["by_illum"]),
+                                              int(a["by_rillum"]), float(a["eps"]), int(bool(a["laplacian"])),
+                                              float(a["lowpass_fraction"]), int(a["npml"]),
+                                              int(a["boundary"] == "cpml"), _lib.ptr(img[j]), None), "postprocess")
+            host = img.cpu().numpy()
+            p.acc = None
+            self.device_images[k] = img
             for j, m in enumerate(p.modes):
-                image = postprocess_image(acc[0, j], acc[1, j], acc[2, j], **p.mig._post_args())
+                image = host[j]
                 res = ImageResult(image=image, grid=p.mig.model.grid, mode=m,
                                   meta=im._meta(p.mig.spec, p.mig.engine, p.shot, p.store, cond, p.start_step,
                                                 p.mig.prop, p.mig.back, m))

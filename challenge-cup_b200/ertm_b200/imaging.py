@@ -208,8 +208,13 @@ class RTMImager:
             comps["primary"] = shot.data
         out: dict[str, np.ndarray] = {}
         for name, arr in comps.items():
-            data = np.asarray(arr, dtype=np.float64)
-            if abs(float(shot.dt) - spec.dt) > 1e-12 and data.shape[0] > 1:
+            data = np.asarray(arr)
+            resample = abs(float(shot.dt) - spec.dt) > 1e-12 and data.shape[0] > 1
+            if resample or preprocess is not None or data.dtype not in (np.float32, np.float64):
+                # the reference works on a float64 copy; without resampling or a
+                # hook the float32 samples pass unchanged (injection casts to float32)
+                data = np.asarray(arr, dtype=np.float64)
+            if resample:
                 if preprocess is None:
                     # device sinc resampling: the record is cast to float32 for
                     # injection anyway, so one float32 rounding of the float64

@@ -91,17 +91,18 @@ class ShardResult:
     per_shot: list          # per local shot: list of ImageResult (one per mode)
 
 
-def _device_partial(images_per_mode: Sequence[Sequence[np.ndarray]], shape, normalize: bool):
-    """float64 partial sums (n_modes, nz, nx) on the current GPU."""
+def _device_partial(images_per_mode: Sequence[Sequence[Any]], shape, normalize: bool):
+    """float64 partial sums (n_modes, nz, nx) on the current GPU; the images
+    are float32 host arrays or contiguous device tensors."""
     import torch
     L = _lib.lib()
     n = int(np.prod(shape))
     out = torch.zeros((len(images_per_mode),) + tuple(shape), dtype=torch.float64, device="cuda")
     for k, imgs in enumerate(images_per_mode):
-        arrs = [np.ascontiguousarray(im, dtype=np.float32) for im in imgs]
+        arrs = [im if hasattr(im, "data_ptr") else np.ascontiguousarray(im, dtype=np.float32) for im in imgs]
         if not arrs:
             continue
-        ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        ptrs = (C.c_void_p * len(arrs))(*[_lib.ptr(a) for a in arrs])
         _lib.check(L.ertm_stack_partial(len(arrs), n, C.cast(ptrs, C.c_void_p), int(bool(normalize)),
                                         _lib.ptr(out[k]), None), "stack partial")
     return out
@@ -140,10 +141,11 @@ class ShotParallelMigrator:
             shape = (g.nz, g.nx) if g is not None else (0, 0)
             import torch
             return ShardResult(torch.zeros((len(modes),) + shape, dtype=torch.float64, device="cuda"), 0, [])
-        per_shot = BatchMigrator(self.imager, memory_budget=self.memory_budget).migrate_shots(
-            shots, models, modes=modes, wavelets=wavelets)
+        bm = BatchMigrator(self.imager, memory_budget=self.memory_budget)
+        per_shot = bm.migrate_shots(shots, models, modes=modes, wavelets=wavelets)
         shape = per_shot[0][0].image.shape
-        partial = _device_partial([[r[k].image for r in per_shot] for k in range(len(modes))], shape, normalize)
+        # the images are still on the device: stack them there
+        partial = _device_partial([[d[k] for d in bm.device_images] for k in range(len(modes))], shape, normalize)
         return ShardResult(partial, len(per_shot), per_shot)
 
     def migrate_job(self, shots: Sequence[Any], models: Any, *, modes: tuple[str, ...] | None = None,
