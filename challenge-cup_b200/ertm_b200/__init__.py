@@ -11,20 +11,25 @@ from __future__ import annotations
 
 __version__ = "0.1.0"
 
+from . import segy
 from .config import ImagingConfig, QConfig, SolverConfig
-from .exceptions import ConfigError, ERTMError, ImagingError, PipelineError, SolverError
+from .data import NumpyDataStore
+from .exceptions import ConfigError, DataError, ERTMError, ImagingError, PipelineError, SolverError
 from .imaging import RTMImager, build_imager
+from .preprocess import prepare_shot
 from .propagation import (AcousticPropagator, ElasticPropagator, PropagationSpec, QOptions,
                           ViscoacousticPropagator, build_propagator, check_stability, forward_shot, run_forward,
                           source_wavelet)
+from .qcomp import QCompensator, attenuate_record, build_compensator
 from .solver import FiniteDifferenceSolver, build_solver
 from .stacking import stack_images
 from .types import ElasticModel, GridSpec, ImageResult, ReceiverSpec, ShotRecord, SourceSpec
 
 __all__ = [
-    "AcousticPropagator", "ConfigError", "ERTMError", "ElasticModel", "ElasticPropagator",
+    "AcousticPropagator", "ConfigError", "DataError", "ERTMError", "ElasticModel", "ElasticPropagator",
     "FiniteDifferenceSolver", "GridSpec", "ImageResult", "ImagingConfig", "ImagingError", "PipelineError",
     "PropagationSpec", "QConfig", "QOptions", "RTMImager", "ReceiverSpec", "ShotRecord", "SolverConfig",
     "SolverError", "SourceSpec", "ViscoacousticPropagator", "build_imager", "build_propagator", "build_solver",
     "check_stability", "forward_shot", "run_forward", "source_wavelet", "stack_images",
+    "NumpyDataStore", "QCompensator", "attenuate_record", "build_compensator", "prepare_shot", "segy",
 ]

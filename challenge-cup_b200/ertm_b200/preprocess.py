@@ -18,13 +18,9 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from .exceptions import ERTMError
+from .exceptions import DataError
 
 _MIN_SAMPLES = 3
-
-
-class DataError(ERTMError):
-    """Invalid record data (the reference's ertm.exceptions.DataError)."""
 
 
 def _f32(a) -> np.ndarray:

@@ -17,11 +17,10 @@ import numpy as np
 
 from . import _lib
 from .config import QConfig
-from .exceptions import ERTMError
+from .exceptions import DataError
 
-
-class DataError(ERTMError):
-    """Invalid record data (the reference's ertm.exceptions.DataError)."""
+__all__ = ["DataError", "QCompensator", "attenuate_record", "build_compensator", "compensation_response",
+           "q_response", "time_varying_filter"]
 
 
 def q_response(freqs: np.ndarray, travel_time: float, q: float, f_ref: float, *, strength: float = 1.0,
