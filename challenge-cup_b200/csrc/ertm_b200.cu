@@ -580,14 +580,16 @@ SplitStreams& split_streams(int lane = 0) { return lane_streams().split[lane]; }
 // none of the boundary code's registers (more resident warps per SM).  The
 // boundary-frame launch of each phase runs on the side stream, concurrently
 // with the interior launch; the two join before the next phase.
-template <int M, int BZ, int R, class WS>
+// The frame launch may use a lower tile (BZF × RF rows) than the interior one:
+// more, shorter blocks for the boundary work.
+template <int M, int BZ, int R, int BZF = BZ, int RF = R, class WS>
 void launch_step_split(int engine, const DevProp* d, const WS& inner, int n_in, const WS& frame, int n_fr,
                        cudaStream_t st, int lane, const TmaGlobal* tm) {
   SplitStreams& ss = split_streams(lane);
   for (int phase = 0; phase < 2; ++phase) {
     CK(cudaEventRecord(ss.fork, st));
     CK(cudaStreamWaitEvent(ss.side, ss.fork, 0));
-    launch_phase<M, BZ, R, TILES_FRAME>(engine, phase, d, frame, n_fr, ss.side);
+    launch_phase<M, BZF, RF, TILES_FRAME>(engine, phase, d, frame, n_fr, ss.side);
     if (tm) launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st, *tm);
     else launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st);
     CK(cudaEventRecord(ss.join, ss.side));
@@ -648,6 +650,20 @@ int plan_interior(const DevProp& h, int tz, StepWork& w) {
 // (a single 401×601 grid, say) the single launch per phase is faster.
 constexpr int64_t kSplitMinTiles = 148 * 16;
 std::atomic<int> g_tile_split{0};   // 0 automatic, 1 never, 2 whenever there are interior tiles
+std::atomic<int> g_frame_rows{0};   // frame tile height in split launches: 0 as the interior's, or 8 / 16
+
+// A frame work in tiles of tzf rows around an interior rectangle planned in
+// tiles of tz rows (tz a multiple of tzf): the rectangle's rows and the hole
+// scale by q = tz / tzf, and the hole becomes q frame tiles (the frame kernel
+// numbers them after the side columns).  Returns the frame tile count.
+int frame_work(const DevProp& h, int tz, int tzf, int interior_tiles, StepWork& b) {
+  const int q = tz / tzf;
+  b.tiles = ((h.nxp + TILE_X - 1) / TILE_X) * ((h.nzp + tzf - 1) / tzf);
+  b.ti0 *= q;
+  b.ti1 *= q;
+  if (b.hole_i >= 0) b.hole_i *= q;
+  return b.tiles - q * interior_tiles;
+}
 
 // One step of the works ws.w[0..n) (tile heights tz; tile0/tiles/tiles_x set):
 // split into interior and boundary launches where that pays, else one launch
@@ -662,6 +678,8 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
     WS inner = ws, frame = ws;
     int n_in = 0, n_fr = 0, ki = 0, kf = 0;
     const Prop* inner_props[MAX_BATCH_WORKS];
+    const int fr = g_frame_rows.load();
+    const int tzf = (fr == 8 || fr == 16) && fr < tz ? fr : tz;
     for (int k = 0; k < n; ++k) {
       StepWork w = ws_work(ws, k);
       const int in = plan_interior(hosts[k]->h, tz, w);
@@ -675,8 +693,9 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
       }
       StepWork b = w;
       b.tile0 = n_fr;
-      ws_work(frame, kf++) = b;
-      n_fr += w.tiles - in;
+      ws_work(frame, kf) = b;
+      n_fr += frame_work(hosts[k]->h, tz, tzf, in, ws_work(frame, kf));
+      ++kf;
     }
     if (n_in > 0 && (n_in >= kSplitMinTiles || split_mode == 2)) {
       ws_count(inner, ki);
@@ -686,7 +705,10 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
       bool maps = g_tma.load() != 0;
       for (int k = 0; k < ki && maps; ++k) maps = inner_props[k]->h.tmap != nullptr;
       const TmaGlobal* tm = maps ? &tm_global : nullptr;
-      if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
+      if (tz == 32 && tzf == 8) launch_step_split<4, 16, 2, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
+      else if (tz == 32 && tzf == 16) launch_step_split<4, 16, 2, 16, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
+      else if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
+      else if (tz == 16 && tzf == 8) launch_step_split<4, 16, 1, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
       else if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
       else launch_step_split<4, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
       return;
@@ -1856,6 +1878,13 @@ int32_t ertm_set_tick_lanes(int32_t lanes) {
   return guarded([&] {
     REQUIRE(lanes >= 0 && lanes <= 2, "tick lanes must be 0 (automatic), 1 or 2");
     g_tick_lanes.store(lanes);
+  });
+}
+
+int32_t ertm_set_frame_rows(int32_t rows) {
+  return guarded([&] {
+    REQUIRE(rows == 0 || rows == 8 || rows == 16, "frame tile height must be 0 (the interior's), 8 or 16");
+    g_frame_rows.store(rows);
   });
 }
 

@@ -276,7 +276,9 @@ __device__ __forceinline__ TileLoc tile_loc(const StepWork& w, int block, int tz
       const int q = k / side, c = k - q * side;
       return {(w.ti0 + q) * tz, (c < w.tj0 ? c : w.tj1 + (c - w.tj0)) * TILE_X};
     }
-    return {w.hole_i * tz, w.hole_j * TILE_X};
+    // the hole: one tile, or the several lower frame tiles of one interior tile
+    k -= (w.ti1 - w.ti0) * side;
+    return {(w.hole_i + k) * tz, w.hole_j * TILE_X};
   }
 }
 

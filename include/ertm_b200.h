@@ -133,6 +133,10 @@ int32_t ertm_set_tick_lanes(int32_t lanes);
  * one, its backward step on the other), 1 alternates shots (both steps of a
  * shot on one lane).  Results do not depend on it. */
 int32_t ertm_set_lane_assign(int32_t mode);
+/* Tile height of the boundary-frame launches when interior tiles run in
+ * launches of their own: 0 the interior's, 8 or 16 rows (used when lower than
+ * the interior's).  Results do not depend on it. */
+int32_t ertm_set_frame_rows(int32_t rows);
 /* Online autotuning of batched ticks (default on): the first ticks of each
  * group shape (engine, order, works, size class) try tile heights 8/16/32,
  * split off/on and one or two lanes, timed with CUDA events; the fastest is

@@ -232,20 +232,24 @@ def split_always(eb):
     _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
 
 
+@pytest.mark.parametrize("frame_rows", [0, 8])
 @pytest.mark.parametrize("tma", [1, 0])
 @pytest.mark.parametrize("engine,boundary,mechanism,tile_rows", [
     ("acoustic", "cpml", "explosive", 16), ("acoustic", "free", "explosive", 8),
     ("elastic", "free", "explosive", 16), ("elastic", "cpml", "force_z", 8), ("elastic", "free", "shear", 32),
     ("viscoacoustic", "cpml", "explosive", 16)])
-def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, boundary, mechanism, tile_rows, tma):
+def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, boundary, mechanism, tile_rows, tma,
+                                                     frame_rows):
     """Interior tiles and the boundary frame in separate launches (the source
-    node's tile, inside the interior rectangle, goes with the frame), interior
-    tiles staged by TMA or by cp.async: GPU == oracle on a grid with an
-    interior rectangle of several tiles."""
+    node's tile, inside the interior rectangle, goes with the frame, as one
+    tile or as several lower frame tiles), interior tiles staged by TMA or by
+    cp.async: GPU == oracle on a grid with an interior rectangle of several
+    tiles."""
     from ertm_b200 import _lib
     from ertm_b200.propagation import PropagationSpec, QOptions, run_forward
     _lib.check(_lib.lib().ertm_set_tile_rows(tile_rows), "tile rows")
     _lib.check(_lib.lib().ertm_set_tma(tma), "tma")
+    _lib.check(_lib.lib().ertm_set_frame_rows(frame_rows), "frame rows")
     try:
         rng = np.random.default_rng(11)
         nz, nx = 150, 200
@@ -267,6 +271,7 @@ def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, b
     finally:
         _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
         _lib.check(_lib.lib().ertm_set_tma(0), "tma")
+        _lib.check(_lib.lib().ertm_set_frame_rows(0), "frame rows")
     assert _lib.lib().ertm_stage_timeouts() == 0
     for n in comps:
         if engine == "viscoacoustic":
@@ -296,18 +301,25 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
     imager = RTMImager(ImagingConfig(condition="normalized", checkpoint_mb=2.0),
                        SolverConfig(nt=260, dt=4e-4, boundary="free", engine="elastic"))
     out = {}
-    for mode, lanes, assign in ((1, 1, 0), (2, 1, 0), (2, 2, 0), (1, 2, 0), (2, 2, 1), (1, 2, 1)):
+    cases = ((1, 1, 0, 0, 0), (2, 1, 0, 0, 0), (2, 2, 0, 0, 0), (1, 2, 0, 0, 0), (2, 2, 1, 0, 0), (1, 2, 1, 0, 0),
+             (2, 2, 0, 32, 8), (2, 1, 0, 32, 16), (2, 2, 1, 16, 8))
+    for mode, lanes, assign, rows, frame_rows in cases:
         _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
         _lib.check(_lib.lib().ertm_set_tick_lanes(lanes), "lanes")
         _lib.check(_lib.lib().ertm_set_lane_assign(assign), "lane assignment")
+        _lib.check(_lib.lib().ertm_set_tile_rows(rows), "tile rows")
+        _lib.check(_lib.lib().ertm_set_frame_rows(frame_rows), "frame rows")
         try:
-            out[mode, lanes, assign] = BatchMigrator(imager).migrate_shots(shots, model, modes=("pp", "ps"))
+            out[mode, lanes, assign, rows, frame_rows] = BatchMigrator(imager).migrate_shots(
+                shots, model, modes=("pp", "ps"))
         finally:
             _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
             _lib.check(_lib.lib().ertm_set_tick_lanes(0), "lanes")
             _lib.check(_lib.lib().ertm_set_lane_assign(0), "lane assignment")
-    for key in ((2, 1, 0), (2, 2, 0), (1, 2, 0), (2, 2, 1), (1, 2, 1)):
-        for a, b in zip(out[1, 1, 0], out[key]):
+            _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
+            _lib.check(_lib.lib().ertm_set_frame_rows(0), "frame rows")
+    for key in cases[1:]:
+        for a, b in zip(out[cases[0]], out[key]):
             for x1, x2 in zip(a, b):
                 assert np.array_equal(x1.image, x2.image), (key, x1.mode)
 
