@@ -547,7 +547,7 @@ struct SplitStreams {
 // Per device: stream pairs for the lanes of a batched tick (lane 0 runs on
 // the caller's stream; lane k > 0 on its own stream) and, per lane, the side
 // stream of its boundary-frame launches.
-constexpr int kLanes = 2;
+constexpr int kLanes = 4;
 struct LaneStreams {
   SplitStreams split[kLanes];          // frame-launch side streams, per lane
   cudaStream_t lane[kLanes] = {};      // lane streams (lane[0] unused: the caller's)
@@ -1446,10 +1446,10 @@ void tune_collect() {
   }
 }
 
-// One (engine, order) group of a tick.  Large groups may run as two lanes (the
-// works alternate between them, each lane on its own stream): the stress
+// One (engine, order) group of a tick.  Large groups may run as two or four
+// lanes (the works taken in turn, each lane on its own stream): the stress
 // phase of one lane, bound by the latency of its epilogue loads, then
-// overlaps the velocity phase of the other, bound by instruction issue.
+// overlaps the velocity phase of another, bound by instruction issue.
 void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStream_t st, double& bytes) {
   if (items.empty()) return;
   const Prop& P0 = items[0]->fwd ? *items[0]->run->F : *items[0]->run->B;
@@ -1483,8 +1483,8 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
       if (ts->cands.empty()) {
         for (int tz : {16, 32, 8})
           for (int split : {1, 2})
-            for (int lanes : {1, 2}) {
-              if (lanes == 2 && c1 - c0 < 2) continue;
+            for (int lanes : {1, 2}) {             // four lanes measured slower on the benchmark job
+              if (lanes > 1 && (int)(c1 - c0) < lanes) continue;
               ts->cands.push_back({tz, split, lanes});
             }
         ts->sum_ms.assign(ts->cands.size(), 0.0);
@@ -1502,14 +1502,14 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
     const int tz = cfg.tz;
     const int lanes = cfg.lanes;
     WorkSetB ws[kLanes]{};
-    int tile0[kLanes] = {0, 0};
+    int tile0[kLanes] = {};
     const Prop* hosts[kLanes][MAX_BATCH_WORKS];
     const bool by_shot = g_lane_assign.load() == 1;
     int shot_no = 0;
     for (size_t k = c0; k < c1; ++k) {
       const Prop& P = items[k]->fwd ? *items[k]->run->F : *items[k]->run->B;
       if (k > c0 && items[k]->run != items[k - 1]->run) ++shot_no;
-      const int l = lanes == 2 ? (by_shot ? (shot_no & 1) : (int)((k - c0) & 1)) : 0;
+      const int l = lanes > 1 ? (by_shot ? shot_no : (int)(k - c0)) % lanes : 0;
       StepWork w = items[k]->w;
       w.tile0 = tile0[l];
       w.tiles_x = (P.h.nxp + TILE_X - 1) / TILE_X;
@@ -1529,13 +1529,22 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
     if (lanes == 1) {
       launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0, cfg.split);
     } else {
+      // every lane starts after what precedes the tick on the caller's stream
+      // and the caller's stream waits for every lane; lanes without works are
+      // skipped
       LaneStreams& ls = lane_streams();
-      CK(cudaEventRecord(ls.fork[1], st));
-      CK(cudaStreamWaitEvent(ls.lane[1], ls.fork[1], 0));
-      launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0, cfg.split);
-      launch_works(M, tz, engine, table, ws[1], ws[1].n, hosts[1], ls.lane[1], 1, cfg.split);
-      CK(cudaEventRecord(ls.join[1], ls.lane[1]));
-      CK(cudaStreamWaitEvent(st, ls.join[1], 0));
+      for (int l = 1; l < lanes; ++l) {
+        if (ws[l].n == 0) continue;
+        CK(cudaEventRecord(ls.fork[l], st));
+        CK(cudaStreamWaitEvent(ls.lane[l], ls.fork[l], 0));
+      }
+      if (ws[0].n > 0) launch_works(M, tz, engine, table, ws[0], ws[0].n, hosts[0], st, 0, cfg.split);
+      for (int l = 1; l < lanes; ++l) {
+        if (ws[l].n == 0) continue;
+        launch_works(M, tz, engine, table, ws[l], ws[l].n, hosts[l], ls.lane[l], l, cfg.split);
+        CK(cudaEventRecord(ls.join[l], ls.lane[l]));
+        CK(cudaStreamWaitEvent(st, ls.join[l], 0));
+      }
     }
     if (cand >= 0) {
       std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1876,7 +1885,7 @@ int32_t ertm_set_tile_split(int32_t mode) {
 
 int32_t ertm_set_tick_lanes(int32_t lanes) {
   return guarded([&] {
-    REQUIRE(lanes >= 0 && lanes <= 2, "tick lanes must be 0 (automatic), 1 or 2");
+    REQUIRE(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4, "tick lanes must be 0 (automatic), 1, 2 or 4");
     g_tick_lanes.store(lanes);
   });
 }

@@ -32,7 +32,7 @@ def main(argv=None) -> None:
     ap.add_argument("--tile-rows", type=int, default=0, help="stencil tile height 8/16/32 (0: automatic)")
     ap.add_argument("--split", type=int, default=0,
                     help="interior tiles in launches of their own: 0 automatic, 1 never, 2 always")
-    ap.add_argument("--lanes", type=int, default=0, help="batched ticks in 1 or 2 stream lanes (0: automatic)")
+    ap.add_argument("--lanes", type=int, default=0, help="batched ticks in 1, 2 or 4 stream lanes (0: automatic)")
     ap.add_argument("--autotune", type=int, default=1, help="online autotuning of batched ticks (1 on, 0 off)")
     ap.add_argument("--frame-rows", type=int, default=0,
                     help="frame tile height in split launches: 0 the interior's, 8 or 16")

@@ -126,8 +126,9 @@ int32_t ertm_set_tile_rows(int32_t rows);
  * results are the same either way; the knob is for tuning and tests. */
 int32_t ertm_set_tile_split(int32_t mode);
 /* Batched ticks: the works of a large (engine, order) group in one lane or
- * alternated over two lanes on separate streams (0 = automatic: two when the
- * group has at least 4 works and enough tiles).  Results are identical. */
+ * taken in turn by two or four lanes on separate streams (0 = automatic: two
+ * when the group has at least 4 works and enough tiles, or the autotuner's
+ * choice of one or two).  Results are identical. */
 int32_t ertm_set_tick_lanes(int32_t lanes);
 /* With two lanes: 0 alternates works between them (a shot's replay step on
  * one, its backward step on the other), 1 alternates shots (both steps of a

@@ -302,7 +302,7 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
                        SolverConfig(nt=260, dt=4e-4, boundary="free", engine="elastic"))
     out = {}
     cases = ((1, 1, 0, 0, 0), (2, 1, 0, 0, 0), (2, 2, 0, 0, 0), (1, 2, 0, 0, 0), (2, 2, 1, 0, 0), (1, 2, 1, 0, 0),
-             (2, 2, 0, 32, 8), (2, 1, 0, 32, 16), (2, 2, 1, 16, 8))
+             (2, 2, 0, 32, 8), (2, 1, 0, 32, 16), (2, 2, 1, 16, 8), (2, 4, 0, 0, 0), (1, 4, 1, 32, 0))
     for mode, lanes, assign, rows, frame_rows in cases:
         _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
         _lib.check(_lib.lib().ertm_set_tick_lanes(lanes), "lanes")
