@@ -420,44 +420,54 @@ namespace ertm {
 // ---------------------------------------------------------------------------
 // Sinc resampling: out[o, s] = Σ_t w[o, t] · in[clamp(off0[o] + t), s] with the
 // weights and first offsets computed on the host (numerics.py:371-384).
+// Records kernels below: grid x over traces (128 per block), grid y over time
+// samples (grid-stride), so no thread divides an index.
 __global__ void k_resample(const float* __restrict__ in, int64_t n_in, int64_t ntr, const double* __restrict__ w,
                            const int64_t* __restrict__ off0, int taps, int64_t n_out, float* __restrict__ out) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_out * ntr) return;
-  const int64_t o = idx / ntr, s = idx - o * ntr;
-  double acc = 0.0;
-  for (int t = 0; t < taps; ++t) {
-    int64_t k = off0[o] + t;
-    k = k < 0 ? 0 : (k >= n_in ? n_in - 1 : k);
-    acc = dadd(acc, dmul(w[o * taps + t], (double)in[k * ntr + s]));
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ntr) return;
+  const float* __restrict__ col = in + s;
+  for (int64_t o = blockIdx.y; o < n_out; o += gridDim.y) {
+    const int64_t k0 = off0[o];
+    const double* __restrict__ wo = w + o * taps;
+    double acc = 0.0;
+#pragma unroll 4
+    for (int t = 0; t < taps; ++t) {
+      int64_t k = k0 + t;
+      k = k < 0 ? 0 : (k >= n_in ? n_in - 1 : k);
+      acc = dadd(acc, dmul(wo[t], (double)col[k * ntr]));
+    }
+    out[o * ntr + s] = __double2float_rn(acc);
   }
-  out[idx] = __double2float_rn(acc);
 }
 
 // Direct-wave mute (preprocess.py:121-173): weight 0.5 − 0.5·cos(π·ramp) with
 // ramp = clip((t − start_r)/(end_r − start_r), 0, 1) per receiver r.
 __global__ void k_mute(const float* __restrict__ in, int64_t nt, int64_t ntr, const double* __restrict__ t,
                        const double* __restrict__ start, const double* __restrict__ end, float* __restrict__ out) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nt * ntr) return;
-  const int64_t i = idx / ntr, r = idx - i * ntr;
-  double ramp = __ddiv_rn(dsub(t[i], start[r]), dsub(end[r], start[r]));
-  ramp = ramp < 0.0 ? 0.0 : (ramp > 1.0 ? 1.0 : ramp);
-  const double wgt = dsub(0.5, dmul(0.5, cos(dmul(3.141592653589793, ramp))));
-  out[idx] = __double2float_rn(dmul((double)in[idx], wgt));
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ntr) return;
+  const double s0 = start[r], span = dsub(end[r], start[r]);
+  for (int64_t i = blockIdx.y; i < nt; i += gridDim.y) {
+    double ramp = __ddiv_rn(dsub(t[i], s0), span);
+    ramp = ramp < 0.0 ? 0.0 : (ramp > 1.0 ? 1.0 : ramp);
+    const double wgt = dsub(0.5, dmul(0.5, cos(dmul(3.141592653589793, ramp))));
+    out[i * ntr + r] = __double2float_rn(dmul((double)in[i * ntr + r], wgt));
+  }
 }
 
 // End taper (preprocess.py:176-191): the first w samples times ramp[k], the
 // last w times ramp[w−1−k], in that order (both when they overlap).
 __global__ void k_taper(const float* __restrict__ in, int64_t nt, int64_t ntr, const double* __restrict__ ramp,
                         int64_t w, float* __restrict__ out) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nt * ntr) return;
-  const int64_t i = idx / ntr;
-  double x = (double)in[idx];
-  if (i < w) x = dmul(x, ramp[i]);
-  if (i >= nt - w) x = dmul(x, ramp[nt - 1 - i]);
-  out[idx] = __double2float_rn(x);
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ntr) return;
+  for (int64_t i = blockIdx.y; i < nt; i += gridDim.y) {
+    double x = (double)in[i * ntr + r];
+    if (i < w) x = dmul(x, ramp[i]);
+    if (i >= nt - w) x = dmul(x, ramp[nt - 1 - i]);
+    out[i * ntr + r] = __double2float_rn(x);
+  }
 }
 
 // Two-component rotation (preprocess.py:36-67): vx' = c·vx + s·vz,

@@ -165,6 +165,12 @@ FftPair stft_fft(int L, int64_t batch, cudaStream_t st) {
 
 size_t round64(size_t n) { return (n + 63) / 64 * 64; }
 
+// Grid of the record kernels: x over traces (blocks of 128), y over samples
+// (at most 65535 rows of blocks; the kernels stride over the rest).
+dim3 records_grid(int64_t ntr, int64_t n_samples) {
+  return dim3((unsigned)((ntr + 127) / 128), (unsigned)std::min<int64_t>(std::max<int64_t>(n_samples, 1), 65535));
+}
+
 // Device allocation that frees itself (stream-ordered).
 struct DevBuf {
   void* p = nullptr;
@@ -2445,9 +2451,8 @@ int32_t ertm_resample(const float* in, int64_t n_in, int64_t ntr, const double* 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     InArray a(in, (size_t)n_in * ntr * 4, st), W(w, (size_t)n_out * taps * 8, st), O(off0, (size_t)n_out * 8, st);
     OutArray b(out, (size_t)n_out * ntr * 4, st);
-    const int64_t n = n_out * ntr;
-    k_resample<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), n_in, ntr, W.as<double>(),
-                                                            O.as<int64_t>(), taps, n_out, b.as<float>());
+    k_resample<<<records_grid(ntr, n_out), 128, 0, st>>>(a.as<float>(), n_in, ntr, W.as<double>(), O.as<int64_t>(),
+                                                        taps, n_out, b.as<float>());
     ++g_launches;
     CK(cudaGetLastError());
     b.finish();
@@ -2463,9 +2468,8 @@ int32_t ertm_mute(const float* in, int64_t nt, int64_t ntr, const double* t, con
     InArray a(in, (size_t)nt * ntr * 4, st), T(t, (size_t)nt * 8, st), S(start, (size_t)ntr * 8, st),
         E(end, (size_t)ntr * 8, st);
     OutArray b(out, (size_t)nt * ntr * 4, st);
-    const int64_t n = nt * ntr;
-    k_mute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), nt, ntr, T.as<double>(), S.as<double>(),
-                                                        E.as<double>(), b.as<float>());
+    k_mute<<<records_grid(ntr, nt), 128, 0, st>>>(a.as<float>(), nt, ntr, T.as<double>(), S.as<double>(),
+                                                 E.as<double>(), b.as<float>());
     ++g_launches;
     CK(cudaGetLastError());
     b.finish();
@@ -2480,8 +2484,7 @@ int32_t ertm_taper(const float* in, int64_t nt, int64_t ntr, const double* ramp,
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     InArray a(in, (size_t)nt * ntr * 4, st), R(ramp, (size_t)w * 8, st);
     OutArray b(out, (size_t)nt * ntr * 4, st);
-    const int64_t n = nt * ntr;
-    k_taper<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.as<float>(), nt, ntr, R.as<double>(), w, b.as<float>());
+    k_taper<<<records_grid(ntr, nt), 128, 0, st>>>(a.as<float>(), nt, ntr, R.as<double>(), w, b.as<float>());
     ++g_launches;
     CK(cudaGetLastError());
     b.finish();
