@@ -130,6 +130,74 @@ __device__ __forceinline__ void stage_cells_n(float* const (&s)[NF], const float
   }
 }
 
+// Row ranges of the same copies (local tile rows: [RLO, RHI) of the halo tile,
+// rows 0 … TZ+2M; of the cell tile, rows 0 … TZ), for tiles staged in two
+// commit groups.
+template <int M, int TZ, int NT, int NF, int RLO, int RHI>
+__device__ __forceinline__ void stage_n_rows(float* const (&s)[NF], const float* const (&g)[NF], int nzp, int ld,
+                                             int i0, int j0) {
+  using T = TileShape<M, TZ>;
+  constexpr int C0 = RLO * (T::W / 4), CH = (RHI - RLO) * (T::W / 4);
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (CH + NT - 1) / NT; ++it) {
+    const int idx = C0 + tid + it * NT;
+    if (CH % NT != 0 && idx >= C0 + CH) break;
+    const int r = idx / (T::W / 4);
+    const int ch = idx - r * (T::W / 4);
+    const int gi = i0 - M + r, gj = j0 - T::OFF + 4 * ch;
+    const bool ok = gi >= 0 && gi < nzp && gj >= 0 && gj < ld;
+    const size_t off = ok ? (size_t)gi * ld + gj : 0;
+    const int so = r * T::W + 4 * ch;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) cp_async16(s[f] + so, g[f] + off, ok);
+  }
+}
+
+template <int TZ, int NT, int NF, int RLO, int RHI>
+__device__ __forceinline__ void stage_cells_n_rows(float* const (&s)[NF], const float* const (&g)[NF], int nzp, int ld,
+                                                   int i0, int j0) {
+  constexpr int C0 = RLO * 8, CH = (RHI - RLO) * 8;
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < (CH + NT - 1) / NT; ++it) {
+    const int idx = C0 + tid + it * NT;
+    if (CH % NT != 0 && idx >= C0 + CH) break;
+    const int r = idx >> 3, ch = idx & 7;
+    const int gi = i0 + r;
+    const bool ok = gi < nzp;
+    const size_t off = ok ? (size_t)gi * ld + j0 + 4 * ch : 0;
+    const int so = r * 32 + 4 * ch;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) cp_async16(s[f] + so, g[f] + off, ok);
+  }
+}
+
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Interior tiles of two row halves: the copies the first half needs (halo rows
+// i0−M … i0+TZ/2+M, cell rows i0 … i0+TZ/2) form one commit group, the rest a
+// second, so the first half computes while the second half's copies are in
+// flight.  No wait here: the kernel waits for one group (cp_async_wait_one +
+// __syncthreads) before the first half and for both before the second.
+template <int M, int TZ, int NT, int NH, int NC>
+__device__ __forceinline__ void stage_tile_halves(const DevProp& P, int i0, int j0, float* const (&hd)[NH],
+                                                  const int (&hf)[NH], float* const (&cd)[NC], const int (&cf)[NC]) {
+  constexpr int HALF = TZ / 2;
+  const float* hg[NH];
+  const float* cg[NC];
+#pragma unroll
+  for (int k = 0; k < NH; ++k) hg[k] = P.f[hf[k]];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) cg[k] = cf[k] >= 0 ? P.f[cf[k]] : P.coef[~cf[k]];
+  stage_n_rows<M, TZ, NT, NH, 0, HALF + 2 * M>(hd, hg, P.nzp, P.ld, i0, j0);
+  stage_cells_n_rows<TZ, NT, NC, 0, HALF>(cd, cg, P.nzp, P.ld, i0, j0);
+  cp_async_commit();
+  stage_n_rows<M, TZ, NT, NH, HALF + 2 * M, TZ + 2 * M>(hd, hg, P.nzp, P.ld, i0, j0);
+  stage_cells_n_rows<TZ, NT, NC, HALF, TZ>(cd, cg, P.nzp, P.ld, i0, j0);
+  cp_async_commit();
+}
+
 // ---------------------------------------------------------------------------
 // TMA staging (interior tiles): one thread issues a tiled bulk copy per array
 // (halo boxes of 40 × (TZ+2M) floats at x = j0 − 4, cell boxes of 32 × TZ at
@@ -752,22 +820,37 @@ k_elastic_velocity(const DevProp* __restrict__ props, const WS ws, const __grid_
   float* const psx0 = P.psix[0]; float* const psx1 = P.psix[1];
   float* const psz0 = P.psiz[0]; float* const psz1 = P.psiz[1];
   const float* const azp = P.az; const float* const bzp = P.bz;
+  // interior 32-row tiles staged in two halves (see stage_tile_halves)
+  constexpr bool HALVES = KIND == TILES_INTERIOR && !TM::kOn && R == 2;
   {
     float* const hd[3] = {sxx_s, szz_s, sxz_s};
     const int hf[3] = {E_SXX, E_SZZ, E_SXZ};
     float* const cd[4] = {c_vx, c_vz, c_irx, c_irz};
     const int cf[4] = {E_VX, E_VZ, ~CE_IRX, ~CE_IRZ};
-    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    if constexpr (HALVES) {
+      stage_tile_halves<M, TZ, XT * BZ>(P, L.i0, L.j0, hd, hf, cd, cf);
+    } else {
+      if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    }
   }
   (void)irx;
   (void)irz;
   const int j = L.j0 + 4 * threadIdx.x;
+  if (HALVES && (j >= G.nxp || !G.interior(L.i0, L.j0, TZ))) {
+    cp_async_wait_all();   // never exit with copies into this block's shared memory in flight
+    return;
+  }
   if (j >= G.nxp) return;
   if (KIND == TILES_INTERIOR && !G.interior(L.i0, L.j0, TZ)) return;   // the host plans only interior tiles here
   if (KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ))) {
     if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
+      if constexpr (HALVES) {
+        if (r == 0) cp_async_wait_one();
+        else cp_async_wait_all();
+        __syncthreads();
+      }
       const int rr = threadIdx.y + BZ * r;
       const int ro = (rr + M) * T::W + 4 * threadIdx.x;
       const size_t g = (size_t)(L.i0 + rr) * G.ld + j;
@@ -1098,12 +1181,17 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
   float* const psz2 = P.psiz[2]; float* const psz3 = P.psiz[3];
   const float* const azp = P.az; const float* const bzp = P.bz;
   const int mech = P.mech;
+  constexpr bool HALVES = KIND == TILES_INTERIOR && !TM::kOn && R == 2;
   {
     float* const hd[2] = {svx, svz};
     const int hf[2] = {E_VX, E_VZ};
     float* const cd[6] = {c_xx, c_zz, c_xz, c_lam, c_l2m, c_mu};
     const int cf[6] = {E_SXX, E_SZZ, E_SXZ, ~CE_LAM, ~CE_L2M, ~CE_MUXZ};
-    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    if constexpr (HALVES) {
+      stage_tile_halves<M, TZ, XT * BZ>(P, L.i0, L.j0, hd, hf, cd, cf);
+    } else {
+      if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    }
   }
   (void)clam;
   (void)cl2m;
@@ -1117,10 +1205,19 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
   const bool want_curl = epi && E.sep == 1 && E.need_s;
   const bool valid = KIND != TILES_INTERIOR || G.interior(L.i0, L.j0, TZ);   // the host plans only interior tiles there
   const bool inner = KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ));
+  if (HALVES && !(j < G.nxp && valid)) {
+    cp_async_wait_all();   // never exit with copies into this block's shared memory in flight
+    return;
+  }
   if (j < G.nxp && inner && valid) {
     if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
+      if constexpr (HALVES) {
+        if (r == 0) cp_async_wait_one();
+        else cp_async_wait_all();
+        __syncthreads();
+      }
       const int rr = threadIdx.y + BZ * r;
       const int i = L.i0 + rr;
       const int ro = (rr + M) * T::W + 4 * threadIdx.x;
