@@ -710,23 +710,38 @@ k_pressure_velocity(const DevProp* __restrict__ props, const WS ws, const __grid
   const float* const azp = P.az; const float* const bzp = P.bz;
   if ((w.flags & STEP_PEAK) && blockIdx.x == w.tile0 && threadIdx.x == 0 && threadIdx.y == 0)
     *P.peak = 0.f;  // the stress phase of this step reduces into it
+  // interior 32-row tiles staged in two halves (see stage_tile_halves)
+  constexpr bool HALVES = KIND == TILES_INTERIOR && !TM::kOn && R == 2;
   {
     float* const hd[1] = {sp};
     const int hf[1] = {A_P};
     float* const cd[4] = {c_vx, c_vz, c_irx, c_irz};
     const int cf[4] = {A_VX, A_VZ, ~CA_IRX, ~CA_IRZ};
-    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    if constexpr (HALVES) {
+      stage_tile_halves<M, TZ, XT * BZ>(P, L.i0, L.j0, hd, hf, cd, cf);
+    } else {
+      if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    }
   }
   (void)irx;
   (void)irz;
   const int j = L.j0 + 4 * threadIdx.x;
 #define CELL(arr, rr) ld4(arr + (rr) * 32 + 4 * threadIdx.x)
+  if (HALVES && (j >= G.nxp || !G.interior(L.i0, L.j0, TZ))) {
+    cp_async_wait_all();   // never exit with copies into this block's shared memory in flight
+    return;
+  }
   if (j >= G.nxp) return;
   if (KIND == TILES_INTERIOR && !G.interior(L.i0, L.j0, TZ)) return;   // the host plans only interior tiles here
   if (KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ))) {
     if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
+      if constexpr (HALVES) {
+        if (r == 0) cp_async_wait_one();
+        else cp_async_wait_all();
+        __syncthreads();
+      }
       const int rr = threadIdx.y + BZ * r;
       const float* row = sp + (rr + M) * T::W + 4 * threadIdx.x;
       const size_t g = (size_t)(L.i0 + rr) * G.ld + j;
@@ -1003,12 +1018,17 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_c
   float* const psx = P.psix[1];
   float* const psz = P.psiz[1];
   const float* const azp = P.az; const float* const bzp = P.bz;
+  constexpr bool HALVES = KIND == TILES_INTERIOR && !TM::kOn && R == 2;
   {
     float* const hd[2] = {svx, svz};
     const int hf[2] = {A_VX, A_VZ};
     float* const cd[2] = {c_a, c_b};
     const int cf[2] = {VISCO ? V_EPS : A_P, VISCO ? ~CV_KR : ~CA_KAPPA};
-    if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    if constexpr (HALVES) {
+      stage_tile_halves<M, TZ, XT * BZ>(P, L.i0, L.j0, hd, hf, cd, cf);
+    } else {
+      if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
+    }
   }
   (void)cA;
   const int j = L.j0 + 4 * threadIdx.x;
@@ -1019,10 +1039,19 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_c
   float peak = 0.f;
   const bool valid = KIND != TILES_INTERIOR || G.interior(L.i0, L.j0, TZ);   // the host plans only interior tiles there
   const bool inner = KIND == TILES_INTERIOR || (KIND == TILES_ALL && G.interior(L.i0, L.j0, TZ));
+  if (HALVES && !(jok && valid)) {
+    cp_async_wait_all();   // never exit with copies into this block's shared memory in flight
+    return;
+  }
   if (jok && inner && valid) {
     if constexpr (KIND != TILES_FRAME) {
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
+      if constexpr (HALVES) {
+        if (r == 0) cp_async_wait_one();
+        else cp_async_wait_all();
+        __syncthreads();
+      }
       const int rr = threadIdx.y + BZ * r;
       const int i = L.i0 + rr;
       const int ro = (rr + M) * T::W + 4 * threadIdx.x;
