@@ -16,6 +16,7 @@ Output: tests/precision/<config>.npz.  The device side of the comparison is
 tests/test_gpu_precision.py.
 
     python tests/precision/make_fp64.py [config ...]     # acoustic elastic4c visco uneven
+    python tests/precision/make_fp64.py --float32 visco  # the same in float32 wavefields (<config>_f32.npz)
 """
 
 from __future__ import annotations
@@ -73,7 +74,7 @@ def _oracle_q(qcfg, compensation: bool):
 
 
 def run_shot(args) -> dict:
-    config, k = args
+    config, k, dtype = args
     _paths()
     import oracle as orc
     from ertm_b200 import workloads
@@ -85,7 +86,7 @@ def run_shot(args) -> dict:
     record = orc.run_forward(wl.model, wl.sources[0], wl.receivers, spec, engine=wl.engine,
                              components=list(wl.components), q=q_fwd)
     t1 = time.perf_counter()
-    sv = SimpleNamespace(dt=wl.dt, nt=wl.nt, order=8, boundary=wl.boundary, dtype="float64", engine=wl.engine,
+    sv = SimpleNamespace(dt=wl.dt, nt=wl.nt, order=8, boundary=wl.boundary, dtype=dtype, engine=wl.engine,
                          npml=wl.npml)
     q = _oracle_q(imager.q_config, bool(imager.q_config.enabled)) if wl.engine == "viscoacoustic" else None
     images = {}
@@ -94,16 +95,17 @@ def run_shot(args) -> dict:
         images[m] = np.asarray(orc.migrate(record, wl.dt, wl.sources[0], wl.receivers, wl.model, sv, im, q),
                                dtype=np.float64)
     return {"config": config, "k": k, "images": images, "forward_s": t1 - t0,
-            "migrate_s": time.perf_counter() - t1}
+            "migrate_s": time.perf_counter() - t1, "dtype": dtype}
 
 
-def save(config: str, results: list[dict]) -> None:
+def save(config: str, results: list[dict], suffix: str = "") -> None:
     import oracle as orc
     shots, step, stack, over = CASES[config]
     rs = sorted(results, key=lambda r: r["k"])
     modes = sorted({m for r in rs for m in r["images"]})
     meta = {"shots": shots, "step": step, "stacked": stack, "modes": modes, "overrides": over,
-            "forward_s": [r["forward_s"] for r in rs], "migrate_s": [r["migrate_s"] for r in rs]}
+            "forward_s": [r["forward_s"] for r in rs], "migrate_s": [r["migrate_s"] for r in rs],
+            "wavefields": rs[0]["dtype"]}
     out = {}
     for m in modes:
         if stack:
@@ -113,21 +115,25 @@ def save(config: str, results: list[dict]) -> None:
             for r in rs:
                 if m in r["images"]:
                     out[f"{m}_{r['k']}"] = r["images"][m][::step, ::step].astype(np.float32)
-    np.savez_compressed(HERE / f"{config}.npz", meta=json.dumps(meta), **out)
+    np.savez_compressed(HERE / f"{config}{suffix}.npz", meta=json.dumps(meta), **out)
     print(config, json.dumps(meta), flush=True)
 
 
-def main(configs) -> None:
+def main(configs, dtype: str = "float64") -> None:
     _paths()
-    tasks = [(c, k) for c in configs for k in range(len(CASES[c][0]))]
+    tasks = [(c, k, dtype) for c in configs for k in range(len(CASES[c][0]))]
     ctx = mp.get_context("spawn")
     done: dict[str, list] = {c: [] for c in configs}
+    suffix = "" if dtype == "float64" else "_f32"
     with ctx.Pool(min(len(tasks), mp.cpu_count())) as pool:
         for r in pool.imap_unordered(run_shot, tasks):
             done[r["config"]].append(r)
             if len(done[r["config"]]) == len(CASES[r["config"]][0]):
-                save(r["config"], done[r["config"]])
+                save(r["config"], done[r["config"]], suffix)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or list(CASES))
+    # --float32: the oracle's migrate in float32 wavefields (the reference's own
+    # precision), written as <config>_f32.npz beside the float64 images
+    args = [a for a in sys.argv[1:] if a != "--float32"]
+    main(args or list(CASES), "float32" if "--float32" in sys.argv[1:] else "float64")
