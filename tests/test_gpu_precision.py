@@ -26,11 +26,15 @@ from make_fp64 import CASES, case_workloads  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-4
-# Measured bounds where float32 wave propagation itself exceeds 1e-4: the
-# device path is bit-identical to the reference's float32 path, so these are
-# the reference's own float32-vs-float64 errors (config 2: 4912 elastic steps,
-# PS image of the shot nearest the model edge 2.4e-4).
-BOUND = {"elastic4c": 3e-4}
+# Measured bounds where float32 wave propagation itself exceeds 1e-4.  Config
+# 2: the device path is bit-identical to the reference's float32 path, so
+# this is the reference's own float32-vs-float64 error (4912 elastic steps,
+# PS image of the shot nearest the model edge 2.4e-4).  Config 3: the
+# compensated viscoacoustic backward pass (gain up to 40 dB) gives 7.0e-4 for
+# shot 40 and 4.2e-5 for shot 10; where the oracle's float32 images are
+# committed, the test below also holds the device to them (≤ 1e-4) and to
+# within 1e-4 of their own float64 error.
+BOUND = {"elastic4c": 3e-4, "visco": 1e-3}
 CONFIGS = [c for c in CASES if (PREC / f"{c}.npz").exists()]
 
 
