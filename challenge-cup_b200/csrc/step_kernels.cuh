@@ -490,6 +490,42 @@ __device__ __forceinline__ void image_tile_f64(const Epilogue& E, const GEO& G, 
   }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
+// Before the stencil of an interior tile: pull into L2 the lines that the
+// float64 imaging epilogue will read-modify-write at the end of the block (the
+// tile's physical cells of every accumulator this step touches) and the stored
+// source fields it reads, so those loads hit L2 instead of DRAM.  Only
+// addresses of the tile's physical cells are touched.
+template <int TZ, int NT, class GEO>
+__device__ __forceinline__ void prefetch_image_tile(const Epilogue& E, const GEO& G, int i0, int j0) {
+  if (E.kind != EPI_IMAGE || E.kahan) return;
+  const int ja = max(j0, G.pad), jb = min(j0 + TILE_X, G.pad + G.nx);
+  const int ia = max(i0, G.pad), ib = min(i0 + TZ, G.pad + G.nz);
+  if (ja >= jb || ia >= ib) return;
+  const void* arr[3 * MAX_EPI_IMAGES + 2];
+  int esz[3 * MAX_EPI_IMAGES + 2];
+  int na = 0;
+  for (int k = 0; k < E.n_images && k < MAX_EPI_IMAGES; ++k) {
+    if (E.illum && E.ill[k]) { arr[na] = E.ill[k]; esz[na++] = 8; }
+    if (E.rillum && E.ril[k]) { arr[na] = E.ril[k]; esz[na++] = 8; }
+    if (E.cross && E.num[k]) { arr[na] = E.num[k]; esz[na++] = 8; }
+  }
+  for (int q = 0; q < 2; ++q)
+    if (E.src[q]) { arr[na] = E.src[q]; esz[na++] = 4; }
+  const int tid = threadIdx.y * XT + threadIdx.x;
+  const int rows = ib - ia;
+  for (int w = tid; w < rows * na; w += NT) {
+    const int a = w / rows, i = ia + w - a * rows;
+    const char* row = static_cast<const char*>(arr[a]) + ((size_t)(i - G.pad) * G.nx + (ja - G.pad)) * esz[a];
+    const int bytes = (jb - ja) * esz[a];
+    for (int b = 0; b < bytes; b += 128) prefetch_l2(row + b);
+    prefetch_l2(row + bytes - 1);
+  }
+}
+
 template <int TZ, int NT, class GEO>
 __device__ __forceinline__ void epilogue_tile(const Epilogue& E, const GEO& G, int i0, int j0, const float* e_p,
                                               const float* e_s, size_t npix) {
@@ -1026,6 +1062,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_c
     const int cf[2] = {VISCO ? V_EPS : A_P, VISCO ? ~CV_KR : ~CA_KAPPA};
     if constexpr (HALVES) {
       stage_tile_halves<M, TZ, XT * BZ>(P, L.i0, L.j0, hd, hf, cd, cf);
+      prefetch_image_tile<TZ, XT * BZ>(w.epi, G, L.i0, L.j0);
     } else {
       if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
     }
@@ -1218,6 +1255,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
     const int cf[6] = {E_SXX, E_SZZ, E_SXZ, ~CE_LAM, ~CE_L2M, ~CE_MUXZ};
     if constexpr (HALVES) {
       stage_tile_halves<M, TZ, XT * BZ>(P, L.i0, L.j0, hd, hf, cd, cf);
+      prefetch_image_tile<TZ, XT * BZ>(w.epi, G, L.i0, L.j0);
     } else {
       if (!stage_tile<M, TZ, XT * BZ>(tm, w.slot, P, L.i0, L.j0, hd, hf, cd, cf, &tma_bar)) return;
     }
