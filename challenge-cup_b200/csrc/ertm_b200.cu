@@ -590,14 +590,24 @@ SplitStreams& split_streams(int lane = 0) { return lane_streams().split[lane]; }
 // more, shorter blocks for the boundary work.
 template <int M, int BZ, int R, int BZF = BZ, int RF = R, class WS>
 void launch_step_split(int engine, const DevProp* d, const WS& inner, int n_in, const WS& frame, int n_fr,
-                       cudaStream_t st, int lane, const TmaGlobal* tm) {
+                       cudaStream_t st, int lane, const TmaGlobal* tm, const WS* march = nullptr, int n_march = 0) {
   SplitStreams& ss = split_streams(lane);
   for (int phase = 0; phase < 2; ++phase) {
     CK(cudaEventRecord(ss.fork, st));
     CK(cudaStreamWaitEvent(ss.side, ss.fork, 0));
     launch_phase<M, BZF, RF, TILES_FRAME>(engine, phase, d, frame, n_fr, ss.side);
-    if (tm) launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st, *tm);
-    else launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st);
+    if (phase == 0 && march) {
+      if constexpr (M == 4) {
+        if (n_march > 0) {
+          k_elastic_velocity_march<M, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
+          ++g_launches;
+        }
+      }
+    } else if (tm) {
+      launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st, *tm);
+    } else {
+      launch_phase<M, BZ, R, TILES_INTERIOR>(engine, phase, d, inner, n_in, st);
+    }
     CK(cudaEventRecord(ss.join, ss.side));
     CK(cudaStreamWaitEvent(st, ss.join, 0));
   }
@@ -657,6 +667,16 @@ int plan_interior(const DevProp& h, int tz, StepWork& w) {
 constexpr int64_t kSplitMinTiles = 148 * 16;
 std::atomic<int> g_tile_split{0};   // 0 automatic, 1 never, 2 whenever there are interior tiles
 std::atomic<int> g_frame_rows{0};   // frame tile height in split launches: 0 as the interior's, or 8 / 16
+std::atomic<int> g_march{0};        // elastic velocity phase of 32-row interiors: 1 marching column strips
+
+// Blocks of the marching velocity launch for an interior rectangle planned in
+// 32-row tiles: strips × segments of at most MARCH_SEG 16-row chunks (the
+// kernel's march_loc splits the same way).
+int march_blocks(const StepWork& w) {
+  const int chunks = 2 * (w.ti1 - w.ti0);
+  const int nseg = (chunks + MARCH_SEG - 1) / MARCH_SEG;
+  return (w.tj1 - w.tj0) * nseg;
+}
 
 // A frame work in tiles of tzf rows around an interior rectangle planned in
 // tiles of tz rows (tz a multiple of tzf): the rectangle's rows and the hole
@@ -711,9 +731,23 @@ void launch_works(int M, int tz, int engine, const DevProp* d, WS& ws, int n, co
       bool maps = g_tma.load() != 0;
       for (int k = 0; k < ki && maps; ++k) maps = inner_props[k]->h.tmap != nullptr;
       const TmaGlobal* tm = maps ? &tm_global : nullptr;
-      if (tz == 32 && tzf == 8) launch_step_split<4, 16, 2, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
-      else if (tz == 32 && tzf == 16) launch_step_split<4, 16, 2, 16, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
-      else if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
+      // the elastic velocity phase of 32-row interiors may march down column strips
+      WS march = inner;
+      int n_march = 0;
+      const bool use_march = g_march.load() == 1 && engine == ENGINE_ELASTIC && tz == 32 && !tm;
+      if (use_march) {
+        for (int k = 0; k < ki; ++k) {
+          StepWork& m = ws_work(march, k);
+          m.tile0 = n_march;
+          n_march += march_blocks(m);
+        }
+      }
+      const WS* mp = use_march ? &march : nullptr;
+      if (tz == 32 && tzf == 8)
+        launch_step_split<4, 16, 2, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm, mp, n_march);
+      else if (tz == 32 && tzf == 16)
+        launch_step_split<4, 16, 2, 16, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm, mp, n_march);
+      else if (tz == 32) launch_step_split<4, 16, 2>(engine, d, inner, n_in, frame, n_fr, st, lane, tm, mp, n_march);
       else if (tz == 16 && tzf == 8) launch_step_split<4, 16, 1, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
       else if (tz == 16) launch_step_split<4, 16, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
       else launch_step_split<4, 8, 1>(engine, d, inner, n_in, frame, n_fr, st, lane, tm);
@@ -1893,6 +1927,13 @@ int32_t ertm_set_tick_lanes(int32_t lanes) {
   return guarded([&] {
     REQUIRE(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4, "tick lanes must be 0 (automatic), 1, 2 or 4");
     g_tick_lanes.store(lanes);
+  });
+}
+
+int32_t ertm_set_march(int32_t enable) {
+  return guarded([&] {
+    REQUIRE(enable == 0 || enable == 1, "march must be 0 or 1");
+    g_march.store(enable);
   });
 }
 

@@ -1450,4 +1450,165 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
 
 #undef CELL
 
+// ---------------------------------------------------------------------------
+// Elastic velocity phase of the interior rectangle, marching down column
+// strips.  A block (8 × 16 threads) owns 32 columns of the rectangle over a
+// segment of 16-row chunks (the rectangle's rows in order, about MARCH_SEG
+// chunks per block) and walks it top to bottom: while one chunk computes, the
+// next chunk's rows are in flight (cp.async, two stages).  σxz and σzz, read
+// with a z-halo, live in a 64-row ring, so every row is copied in once per
+// segment instead of once per tile with its halo; σxx (x-halo only) and the
+// per-cell operands are double-buffered per chunk.  The arithmetic is the
+// interior tile kernel's, expression for expression.  The source node's
+// 32-row tile (the hole) is left to the frame launch: its two chunks are
+// skipped.
+// ---------------------------------------------------------------------------
+constexpr int MARCH_CH = 16;     // rows per chunk: one per thread row
+constexpr int MARCH_SEG = 8;     // chunks per block, at most
+constexpr int MARCH_RING = 64;   // ring rows (power of two ≥ 2·MARCH_CH + 2M + MARCH_CH)
+
+struct MarchLoc {
+  int j0, a0, n, hole_c;   // strip column, first row, chunks, first hole chunk (relative; out of range: none)
+};
+
+// Blocks of a work: (tj1 − tj0) strips × nseg segments; the host counts them
+// the same way (march_blocks).
+__device__ __forceinline__ MarchLoc march_loc(const StepWork& w, int block) {
+  const int ncols = w.tj1 - w.tj0;
+  const int chunks = 2 * (w.ti1 - w.ti0);
+  const int nseg = (chunks + MARCH_SEG - 1) / MARCH_SEG;
+  const int len = (chunks + nseg - 1) / nseg;
+  const int k = block - w.tile0;
+  const int seg = k / ncols, col = k - seg * ncols;
+  const int c0 = seg * len;
+  MarchLoc L;
+  L.j0 = (w.tj0 + col) * TILE_X;
+  L.a0 = w.ti0 * 32 + c0 * MARCH_CH;
+  L.n = min(len, chunks - c0);
+  L.hole_c = (w.hole_i >= 0 && w.tj0 + col == w.hole_j) ? 2 * (w.hole_i - w.ti0) - c0 : -1000;
+  return L;
+}
+
+// Rows [r_lo, r_hi) of one field with a 4-column halo each side into a ring
+// of 40-float rows (slot = row mod MARCH_RING).
+template <int NT>
+__device__ __forceinline__ void march_ring_rows(float* s, const float* __restrict__ g, int nzp, int ld, int r_lo,
+                                                int r_hi, int j0) {
+  const int tid = threadIdx.y * XT + threadIdx.x;
+  const int n = (r_hi - r_lo) * 10;
+  for (int idx = tid; idx < n; idx += NT) {
+    const int q = idx / 10;
+    const int r = r_lo + q, ch = idx - q * 10;
+    const int gj = j0 - 4 + 4 * ch;
+    const bool ok = r >= 0 && r < nzp && gj >= 0 && gj < ld;
+    cp_async16(s + (r & (MARCH_RING - 1)) * 40 + 4 * ch, ok ? g + (size_t)r * ld + gj : g, ok);
+  }
+}
+
+// One chunk's σxx rows (x-halo, 16 × 40) and per-cell operands (16 × 32 each).
+template <int NT>
+__device__ __forceinline__ void march_chunk_rows(float* sx, float* const (&cd)[4], const float* __restrict__ gx,
+                                                 const float* const (&cg)[4], int nzp, int ld, int a, int j0) {
+  const int tid = threadIdx.y * XT + threadIdx.x;
+  for (int idx = tid; idx < MARCH_CH * 10; idx += NT) {
+    const int q = idx / 10;
+    const int r = a + q, ch = idx - q * 10;
+    const int gj = j0 - 4 + 4 * ch;
+    const bool ok = r < nzp && gj >= 0 && gj < ld;
+    cp_async16(sx + q * 40 + 4 * ch, ok ? gx + (size_t)r * ld + gj : gx, ok);
+  }
+  for (int idx = tid; idx < MARCH_CH * 8; idx += NT) {
+    const int q = idx >> 3, ch = idx & 7;
+    const int r = a + q;
+    const bool ok = r < nzp;
+    const size_t off = ok ? (size_t)r * ld + j0 + 4 * ch : 0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) cp_async16(cd[f] + q * 32 + 4 * ch, cg[f] + off, ok);
+  }
+}
+
+template <int M, class WS>
+__global__ void __launch_bounds__(XT* MARCH_CH)
+k_elastic_velocity_march(const DevProp* __restrict__ props, const WS ws) {
+  static_assert(M == 4, "the march covers the 8th-order stencil");
+  static_assert(MARCH_RING >= 2 * MARCH_CH + 2 * M + MARCH_CH, "ring too short for two chunks in flight");
+  __shared__ __align__(128) float ring_xz[MARCH_RING * 40];
+  __shared__ __align__(128) float ring_zz[MARCH_RING * 40];
+  __shared__ __align__(128) float sxx_b[2][MARCH_CH * 40];
+  __shared__ __align__(128) float cell_b[2][4][MARCH_CH * 32];
+  constexpr int NT = XT * MARCH_CH;
+  const StepWork& w = ws.get(blockIdx.x);
+  const DevProp& P = props[w.prop];
+  const Geo G(P);
+  const MarchLoc L = march_loc(w, blockIdx.x);
+  if (L.n <= 0) return;
+  float* const vx = P.f[E_VX];
+  float* const vz = P.f[E_VZ];
+  const float* const gxx = P.f[E_SXX];
+  const float* const gzz = P.f[E_SZZ];
+  const float* const gxz = P.f[E_SXZ];
+  const float* const cg[4] = {P.f[E_VX], P.f[E_VZ], P.coef[CE_IRX], P.coef[CE_IRZ]};
+  const int j0 = L.j0;
+  // chunk 0: its ring rows with the top halo, its σxx and cell rows
+  march_ring_rows<NT>(ring_xz, gxz, G.nzp, G.ld, L.a0 - M, L.a0 + MARCH_CH + M, j0);
+  march_ring_rows<NT>(ring_zz, gzz, G.nzp, G.ld, L.a0 - M, L.a0 + MARCH_CH + M, j0);
+  {
+    float* const cd[4] = {cell_b[0][0], cell_b[0][1], cell_b[0][2], cell_b[0][3]};
+    march_chunk_rows<NT>(sxx_b[0], cd, gxx, cg, G.nzp, G.ld, L.a0, j0);
+  }
+  cp_async_commit();
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = j0 + 4 * tx;
+#pragma unroll 1
+  for (int c = 0; c < L.n; ++c) {
+    const int a = L.a0 + c * MARCH_CH;
+    const int b = c & 1;
+    if (c + 1 < L.n) {   // the next chunk: 16 new ring rows, its σxx and cell rows
+      march_ring_rows<NT>(ring_xz, gxz, G.nzp, G.ld, a + MARCH_CH + M, a + 2 * MARCH_CH + M, j0);
+      march_ring_rows<NT>(ring_zz, gzz, G.nzp, G.ld, a + MARCH_CH + M, a + 2 * MARCH_CH + M, j0);
+      float* const cd[4] = {cell_b[b ^ 1][0], cell_b[b ^ 1][1], cell_b[b ^ 1][2], cell_b[b ^ 1][3]};
+      march_chunk_rows<NT>(sxx_b[b ^ 1], cd, gxx, cg, G.nzp, G.ld, a + MARCH_CH, j0);
+    }
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    if (c != L.hole_c && c != L.hole_c + 1) {
+      const int i = a + ty;
+      const size_t g = (size_t)i * G.ld + j;
+      const float4 cvx = ld4(cell_b[b][0] + ty * 32 + 4 * tx), cvz = ld4(cell_b[b][1] + ty * 32 + 4 * tx);
+      const float4 cirx = ld4(cell_b[b][2] + ty * 32 + 4 * tx), cirz = ld4(cell_b[b][3] + ty * 32 + 4 * tx);
+      float v[12], z[4][2 * M + 1];
+      float4 ox, oz;
+      row12(sxx_b[b] + ty * 40 + 4 * tx, v);
+#pragma unroll
+      for (int k = 0; k <= 2 * M; ++k) {
+        const float4 q = ld4(ring_xz + ((i + k - M) & (MARCH_RING - 1)) * 40 + 4 + 4 * tx);
+        z[0][k] = q.x; z[1][k] = q.y; z[2][k] = q.z; z[3][k] = q.w;
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const float da = G.dxf(sum_plus<M>(v, 4 + cc, G.c));
+        const float db = G.dzf(sum_minus<M>(z[cc], M, G.c));
+        set_comp(ox, cc, fadd(comp(cvx, cc), fmul(fmul(G.dt, comp(cirx, cc)), fadd(da, db))));
+      }
+      st4(vx + g, ox);
+      row12(ring_xz + (i & (MARCH_RING - 1)) * 40 + 4 * tx, v);
+#pragma unroll
+      for (int k = 0; k <= 2 * M; ++k) {
+        const float4 q = ld4(ring_zz + ((i + k - M) & (MARCH_RING - 1)) * 40 + 4 + 4 * tx);
+        z[0][k] = q.x; z[1][k] = q.y; z[2][k] = q.z; z[3][k] = q.w;
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const float da = G.dxf(sum_minus<M>(v, 4 + cc, G.c));
+        const float db = G.dzf(sum_plus<M>(z[cc], M, G.c));
+        set_comp(oz, cc, fadd(comp(cvz, cc), fmul(fmul(G.dt, comp(cirz, cc)), fadd(da, db))));
+      }
+      st4(vz + g, oz);
+    }
+    __syncthreads();   // the next iteration refills this chunk's buffers
+  }
+  cp_async_wait_all();
+}
+
 }  // namespace ertm
