@@ -849,8 +849,8 @@ void lowpass_field(Prop& P, float* f, double cutoff) {
 
 // Algorithmic HBM bytes of one propagator step: each state array read and
 // written once, each per-cell coefficient read once, CPML strips read and
-// written (SURVEY-style accounting; the viscoacoustic a_l count as per-cell
-// coefficients although they are read from a per-Q table here).
+// written (the viscoacoustic a_l count as per-cell coefficients although
+// they are read from a per-Q table here).
 double step_bytes(const Prop& P) {
   const double npad = (double)P.h.nzp * P.h.nxp;
   const int n_state = P.h.n_fields;
@@ -859,9 +859,9 @@ double step_bytes(const Prop& P) {
   return npad * (8.0 * n_state + 4.0 * n_coef) + 8.0 * strips;
 }
 
-// Algorithmic bytes of a fused epilogue over the physical cells (SURVEY §8d:
-// each imaging accumulator is read and written once per step, 16 B; the
-// replayed source field is written once and read once, 4 B each).
+// Algorithmic bytes of a fused epilogue over the physical cells: each
+// imaging accumulator is read and written once per step, 16 B; the replayed
+// source field is written once and read once, 4 B each.
 double epilogue_bytes(const Epilogue& e, size_t npix) {
   double per = 0.0;
   switch (e.kind) {
