@@ -5,9 +5,13 @@ Run in a container that holds the reference checkout (read-only):
     python tests/golden/make_golden.py [/path/to/reference]
 
 It imports the reference's own ``ertm`` package (numerics, propagation,
-imaging, viscoelastic, pipeline.stack_images restated inline because
-``ertm.pipeline`` needs matplotlib), feeds it small seeded inputs and writes
-the inputs and outputs to ``tests/golden/*.npz``.  The committed fixtures
+imaging, viscoelastic, preprocess, qcomp, data; pipeline.stack_images
+restated inline because ``ertm.pipeline`` needs matplotlib), feeds it small
+seeded inputs and writes the inputs and outputs to ``tests/golden/*.npz``;
+the ``store`` case also keeps the three .npz files the reference's
+NumpyDataStore wrote, under ``tests/golden/store/``.  Cases by name:
+
+    python tests/golden/make_golden.py /path/to/reference qcomp store  The committed fixtures
 pin both the CPU oracle and the CUDA path; nothing at test time reads the
 reference tree.
 """
