@@ -1464,19 +1464,19 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
 // skipped.
 // ---------------------------------------------------------------------------
 constexpr int MARCH_CH = 16;     // rows per chunk: one per thread row
-constexpr int MARCH_SEG = 8;     // chunks per block, at most
 constexpr int MARCH_RING = 64;   // ring rows (power of two ≥ 2·MARCH_CH + 2M + MARCH_CH)
 
 struct MarchLoc {
   int j0, a0, n, hole_c;   // strip column, first row, chunks, first hole chunk (relative; out of range: none)
 };
 
-// Blocks of a work: (tj1 − tj0) strips × nseg segments; the host counts them
-// the same way (march_blocks).
+// Blocks of a work: (tj1 − tj0) strips × nseg segments of at most SEG
+// chunks; the host counts them the same way (march_blocks).
+template <int SEG>
 __device__ __forceinline__ MarchLoc march_loc(const StepWork& w, int block) {
   const int ncols = w.tj1 - w.tj0;
   const int chunks = 2 * (w.ti1 - w.ti0);
-  const int nseg = (chunks + MARCH_SEG - 1) / MARCH_SEG;
+  const int nseg = (chunks + SEG - 1) / SEG;
   const int len = (chunks + nseg - 1) / nseg;
   const int k = block - w.tile0;
   const int seg = k / ncols, col = k - seg * ncols;
@@ -1527,7 +1527,7 @@ __device__ __forceinline__ void march_chunk_rows(float* sx, float* const (&cd)[4
   }
 }
 
-template <int M, class WS>
+template <int M, int SEG, class WS>
 __global__ void __launch_bounds__(XT* MARCH_CH)
 k_elastic_velocity_march(const DevProp* __restrict__ props, const WS ws) {
   static_assert(M == 4, "the march covers the 8th-order stencil");
@@ -1540,7 +1540,7 @@ k_elastic_velocity_march(const DevProp* __restrict__ props, const WS ws) {
   const StepWork& w = ws.get(blockIdx.x);
   const DevProp& P = props[w.prop];
   const Geo G(P);
-  const MarchLoc L = march_loc(w, blockIdx.x);
+  const MarchLoc L = march_loc<SEG>(w, blockIdx.x);
   if (L.n <= 0) return;
   float* const vx = P.f[E_VX];
   float* const vz = P.f[E_VZ];

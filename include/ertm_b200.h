@@ -138,10 +138,11 @@ int32_t ertm_set_lane_assign(int32_t mode);
  * launches of their own: 0 the interior's, 8 or 16 rows (used when lower than
  * the interior's).  Results do not depend on it. */
 int32_t ertm_set_frame_rows(int32_t rows);
-/* 1: the elastic velocity phase of 32-row interior rectangles marches down
- * column strips (16-row chunks, next chunk's copies in flight, z-halo rows
- * in a ring) instead of one block per tile; 0 (default): tiles.  Results do
- * not depend on it. */
+/* 2, 4 or 8 (1 = 8): the elastic velocity phase of 32-row interior
+ * rectangles marches down column strips in segments of at most that many
+ * 16-row chunks (next chunk's copies in flight, z-halo rows in a ring)
+ * instead of one block per tile (default 4); 0: tiles.  Results do not depend
+ * on it. */
 int32_t ertm_set_march(int32_t enable);
 /* Online autotuning of batched ticks (default on): the first ticks of each
  * group shape (engine, order, works, size class) try tile heights 8/16/32,

@@ -232,7 +232,7 @@ def split_always(eb):
     _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
 
 
-@pytest.mark.parametrize("march", [0, 1])
+@pytest.mark.parametrize("march", [0, 4, 8])
 @pytest.mark.parametrize("frame_rows", [0, 8])
 @pytest.mark.parametrize("tma", [1, 0])
 @pytest.mark.parametrize("engine,boundary,mechanism,tile_rows", [
@@ -274,7 +274,7 @@ def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, b
         _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
         _lib.check(_lib.lib().ertm_set_tma(0), "tma")
         _lib.check(_lib.lib().ertm_set_frame_rows(0), "frame rows")
-        _lib.check(_lib.lib().ertm_set_march(0), "march")
+        _lib.check(_lib.lib().ertm_set_march(4), "march")
     assert _lib.lib().ertm_stage_timeouts() == 0
     for n in comps:
         if engine == "viscoacoustic":
@@ -306,14 +306,14 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
     out = {}
     cases = ((1, 1, 0, 0, 0), (2, 1, 0, 0, 0), (2, 2, 0, 0, 0), (1, 2, 0, 0, 0), (2, 2, 1, 0, 0), (1, 2, 1, 0, 0),
              (2, 2, 0, 32, 8), (2, 1, 0, 32, 16), (2, 2, 1, 16, 8), (2, 4, 0, 0, 0), (1, 4, 1, 32, 0),
-             (2, 2, 0, 32, 0, 1), (2, 1, 0, 32, 16, 1))
+             (2, 2, 0, 32, 0, 8), (2, 1, 0, 32, 16, 2), (2, 2, 0, 32, 0, 0))
     for mode, lanes, assign, rows, frame_rows, *rest in cases:
         _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
         _lib.check(_lib.lib().ertm_set_tick_lanes(lanes), "lanes")
         _lib.check(_lib.lib().ertm_set_lane_assign(assign), "lane assignment")
         _lib.check(_lib.lib().ertm_set_tile_rows(rows), "tile rows")
         _lib.check(_lib.lib().ertm_set_frame_rows(frame_rows), "frame rows")
-        _lib.check(_lib.lib().ertm_set_march(rest[0] if rest else 0), "march")
+        _lib.check(_lib.lib().ertm_set_march(rest[0] if rest else 4), "march")
         try:
             out[(mode, lanes, assign, rows, frame_rows, *rest)] = BatchMigrator(imager).migrate_shots(
                 shots, model, modes=("pp", "ps"))
@@ -323,7 +323,7 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
             _lib.check(_lib.lib().ertm_set_lane_assign(0), "lane assignment")
             _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
             _lib.check(_lib.lib().ertm_set_frame_rows(0), "frame rows")
-            _lib.check(_lib.lib().ertm_set_march(0), "march")
+            _lib.check(_lib.lib().ertm_set_march(4), "march")
     for key in cases[1:]:
         for a, b in zip(out[cases[0]], out[key]):
             for x1, x2 in zip(a, b):
