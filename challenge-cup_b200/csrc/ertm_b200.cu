@@ -590,6 +590,8 @@ SplitStreams& split_streams(int lane = 0) { return lane_streams().split[lane]; }
 // column strips in segments of at most that many 16-row chunks (4: measured
 // fastest on the benchmark job, tick 78.3 → 75.9 µs).
 std::atomic<int> g_march{4};
+// Elastic stress phase of 32-row interiors marching as well (same segments): 0 off, 1 on.
+std::atomic<int> g_march_stress{0};
 
 // The frame launch may use a lower tile (BZF × RF rows) than the interior one:
 // more, shorter blocks for the boundary work.
@@ -608,6 +610,16 @@ void launch_step_split(int engine, const DevProp* d, const WS& inner, int n_in, 
           if (seg == 2) k_elastic_velocity_march<M, 2, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
           else if (seg == 4) k_elastic_velocity_march<M, 4, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
           else k_elastic_velocity_march<M, 8, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
+          ++g_launches;
+        }
+      }
+    } else if (phase == 1 && march && g_march_stress.load() == 1) {
+      if constexpr (M == 4) {
+        if (n_march > 0) {
+          const int seg = g_march.load();
+          if (seg == 2) k_elastic_stress_march<M, 2, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
+          else if (seg == 4) k_elastic_stress_march<M, 4, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
+          else k_elastic_stress_march<M, 8, WS><<<n_march, dim3(XT, MARCH_CH), 0, st>>>(d, *march);
           ++g_launches;
         }
       }
@@ -1942,6 +1954,13 @@ int32_t ertm_set_march(int32_t enable) {
     REQUIRE(enable == 0 || enable == 1 || enable == 2 || enable == 4 || enable == 8,
             "march must be 0 (tiles) or 2, 4, 8 chunks per segment (1: 8)");
     g_march.store(enable == 1 ? 8 : enable);
+  });
+}
+
+int32_t ertm_set_march_stress(int32_t enable) {
+  return guarded([&] {
+    REQUIRE(enable == 0 || enable == 1, "march_stress must be 0 or 1");
+    g_march_stress.store(enable);
   });
 }
 

@@ -1611,4 +1611,145 @@ k_elastic_velocity_march(const DevProp* __restrict__ props, const WS ws) {
   cp_async_wait_all();
 }
 
+// Six per-cell operand rows of one chunk (16 × 32 each).
+template <int NT>
+__device__ __forceinline__ void march_cells6(float (&cd)[6][MARCH_CH * 32], const float* const (&cg)[6], int nzp,
+                                             int ld, int a, int j0) {
+  const int tid = threadIdx.y * XT + threadIdx.x;
+#pragma unroll
+  for (int it = 0; it < MARCH_CH * 8 / NT; ++it) {
+    const int idx = tid + it * NT;
+    const int q = idx >> 3, ch = idx & 7;
+    const int r = a + q;
+    const bool ok = r < nzp;
+    const size_t off = ok ? (size_t)r * ld + j0 + 4 * ch : 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) cp_async16(cd[f] + q * 32 + 4 * ch, cg[f] + off, ok);
+  }
+}
+
+// Elastic stress phase of the interior rectangle, marching like the velocity
+// kernel above: vx and vz (read with both halos) in 64-row rings, the six
+// per-cell operands double-buffered per chunk, and the fused epilogue run per
+// 16-row chunk (it works cell by cell, so chunks give the tile's result).  P
+// and S for the epilogue reuse the chunk's σxx / σzz operand buffers: each
+// thread has read its own old values before it writes there.  Interior
+// rectangles hold neither the source node nor the free-surface row.
+template <int M, int SEG, class WS>
+__global__ void __launch_bounds__(XT* MARCH_CH, 5)
+k_elastic_stress_march(const DevProp* __restrict__ props, const WS ws) {
+  static_assert(M == 4, "the march covers the 8th-order stencil");
+  __shared__ __align__(128) float ring_vx[MARCH_RING * 40];
+  __shared__ __align__(128) float ring_vz[MARCH_RING * 40];
+  __shared__ __align__(128) float cell_b[2][6][MARCH_CH * 32];
+  constexpr int NT = XT * MARCH_CH;
+  const StepWork& w = ws.get(blockIdx.x);
+  const DevProp& P = props[w.prop];
+  const Geo G(P);
+  const MarchLoc L = march_loc<SEG>(w, blockIdx.x);
+  if (L.n <= 0) return;
+  float* const sxx = P.f[E_SXX];
+  float* const szz = P.f[E_SZZ];
+  float* const sxz = P.f[E_SXZ];
+  const float* const gvx = P.f[E_VX];
+  const float* const gvz = P.f[E_VZ];
+  const float* const cg[6] = {P.f[E_SXX], P.f[E_SZZ], P.f[E_SXZ], P.coef[CE_LAM], P.coef[CE_L2M], P.coef[CE_MUXZ]};
+  const int j0 = L.j0;
+  const size_t npix = (size_t)G.nz * G.nx;
+  const Epilogue& E = w.epi;
+  const bool epi = E.kind != EPI_NONE;
+  const bool want_curl = epi && E.sep == 1 && E.need_s;
+  march_ring_rows<NT>(ring_vx, gvx, G.nzp, G.ld, L.a0 - M, L.a0 + MARCH_CH + M, j0);
+  march_ring_rows<NT>(ring_vz, gvz, G.nzp, G.ld, L.a0 - M, L.a0 + MARCH_CH + M, j0);
+  march_cells6<NT>(cell_b[0], cg, G.nzp, G.ld, L.a0, j0);
+  cp_async_commit();
+  prefetch_image_tile<MARCH_CH, NT>(E, G, L.a0, j0);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = j0 + 4 * tx;
+#pragma unroll 1
+  for (int c = 0; c < L.n; ++c) {
+    const int a = L.a0 + c * MARCH_CH;
+    const int b = c & 1;
+    if (c + 1 < L.n) {
+      march_ring_rows<NT>(ring_vx, gvx, G.nzp, G.ld, a + MARCH_CH + M, a + 2 * MARCH_CH + M, j0);
+      march_ring_rows<NT>(ring_vz, gvz, G.nzp, G.ld, a + MARCH_CH + M, a + 2 * MARCH_CH + M, j0);
+      march_cells6<NT>(cell_b[b ^ 1], cg, G.nzp, G.ld, a + MARCH_CH, j0);
+    }
+    cp_async_commit();
+    if (c + 1 < L.n) prefetch_image_tile<MARCH_CH, NT>(E, G, a + MARCH_CH, j0);
+    cp_async_wait_one();
+    __syncthreads();
+    const bool run = c != L.hole_c && c != L.hole_c + 1;
+    if (run) {
+      const int i = a + ty;
+      const size_t g = (size_t)i * G.ld + j;
+      const int co = ty * 32 + 4 * tx;
+      const float4 cxx = ld4(cell_b[b][0] + co), czz = ld4(cell_b[b][1] + co), cxz = ld4(cell_b[b][2] + co);
+      const float4 clam = ld4(cell_b[b][3] + co), cl2m = ld4(cell_b[b][4] + co), cmu = ld4(cell_b[b][5] + co);
+      float v[12], z[4][2 * M + 1];
+      float exx[4], ezz[4], f1[4], f2[4], ca[4], cb[4];
+      row12(ring_vx + (i & (MARCH_RING - 1)) * 40 + 4 * tx, v);
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) exx[cc] = G.dxf(sum_minus<M>(v, 4 + cc, G.c));
+      row12(ring_vz + (i & (MARCH_RING - 1)) * 40 + 4 * tx, v);
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) f2[cc] = G.dxf(sum_plus<M>(v, 4 + cc, G.c));
+      if (want_curl) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) cb[cc] = G.dxf(sum_minus<M>(v, 4 + cc, G.c));
+      }
+#pragma unroll
+      for (int k = 0; k <= 2 * M; ++k) {
+        const float4 q = ld4(ring_vx + ((i + k - M) & (MARCH_RING - 1)) * 40 + 4 + 4 * tx);
+        z[0][k] = q.x; z[1][k] = q.y; z[2][k] = q.z; z[3][k] = q.w;
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) f1[cc] = G.dzf(sum_plus<M>(z[cc], M, G.c));
+      if (want_curl) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) ca[cc] = G.dzf(sum_minus<M>(z[cc], M, G.c));
+      }
+#pragma unroll
+      for (int k = 0; k <= 2 * M; ++k) {
+        const float4 q = ld4(ring_vz + ((i + k - M) & (MARCH_RING - 1)) * 40 + 4 + 4 * tx);
+        z[0][k] = q.x; z[1][k] = q.y; z[2][k] = q.z; z[3][k] = q.w;
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) ezz[cc] = G.dzf(sum_minus<M>(z[cc], M, G.c));
+      float4 oxx, ozz, oxz;
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const float lam = comp(clam, cc), l2m = comp(cl2m, cc);
+        set_comp(oxx, cc, fadd(comp(cxx, cc), fmul(G.dt, fadd(fmul(l2m, exx[cc]), fmul(lam, ezz[cc])))));
+        set_comp(ozz, cc, fadd(comp(czz, cc), fmul(G.dt, fadd(fmul(lam, exx[cc]), fmul(l2m, ezz[cc])))));
+        set_comp(oxz, cc, fadd(comp(cxz, cc), fmul(fmul(G.dt, comp(cmu, cc)), fadd(f1[cc], f2[cc]))));
+      }
+      st4(sxx + g, oxx);
+      st4(szz + g, ozz);
+      st4(sxz + g, oxz);
+      if (epi) {
+        float4 pv4, sv4;
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          if (E.sep == 0) {
+            set_comp(pv4, cc, fmul(0.5f, fadd(comp(oxx, cc), comp(ozz, cc))));
+            set_comp(sv4, cc, comp(oxz, cc));
+          } else {
+            set_comp(pv4, cc, fadd(exx[cc], ezz[cc]));
+            set_comp(sv4, cc, want_curl ? fsub(ca[cc], cb[cc]) : 0.f);
+          }
+        }
+        st4(cell_b[b][0] + co, pv4);   // P over this thread's old σxx slot
+        st4(cell_b[b][1] + co, sv4);   // S over its old σzz slot
+      }
+    }
+    if (epi && run) {
+      __syncthreads();
+      epilogue_tile<MARCH_CH, NT>(E, G, a, j0, cell_b[b][0], cell_b[b][1], npix);
+    }
+    __syncthreads();   // the next iteration refills this chunk's buffers
+  }
+  cp_async_wait_all();
+}
+
 }  // namespace ertm

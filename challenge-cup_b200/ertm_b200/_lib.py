@@ -79,6 +79,7 @@ _SIGNATURES = {
     "ertm_set_lane_assign": (_I32, [_I32]),
     "ertm_set_frame_rows": (_I32, [_I32]),
     "ertm_set_march": (_I32, [_I32]),
+    "ertm_set_march_stress": (_I32, [_I32]),
     "ertm_set_autotune": (_I32, [_I32]),
     "ertm_set_tma": (_I32, [_I32]),
     "ertm_stage_timeouts": (C.c_int64, []),

@@ -2,7 +2,7 @@
 the process, for ncu launch lists and kernel captures.
 
     PYTHONPATH=challenge-cup_b200 python -m ertm_b200.profiling \\
-        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--autotune 1] [--lane-assign 0] [--frame-rows 0] [--march 4] [--tma 0] [--save x.npy]
+        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--autotune 1] [--lane-assign 0] [--frame-rows 0] [--march 4] [--march-stress 0] [--tma 0] [--save x.npy]
 
 The job is what ``bench.py`` times: every shot of the workload migrated
 (batched lockstep ticks, or one shot at a time with ``--path plain``) and the
@@ -36,6 +36,7 @@ def main(argv=None) -> None:
     ap.add_argument("--autotune", type=int, default=1, help="online autotuning of batched ticks (1 on, 0 off)")
     ap.add_argument("--march", type=int, default=4,
                     help="elastic velocity interiors: 0 tiles, or 2/4/8 chunks per marching segment")
+    ap.add_argument("--march-stress", type=int, default=0, help="elastic stress interiors march as well (1)")
     ap.add_argument("--frame-rows", type=int, default=0,
                     help="frame tile height in split launches: 0 the interior's, 8 or 16")
     ap.add_argument("--lane-assign", type=int, default=0,
@@ -59,6 +60,7 @@ def main(argv=None) -> None:
     _lib.check(L.ertm_set_lane_assign(args.lane_assign), "lane assignment")
     _lib.check(L.ertm_set_frame_rows(args.frame_rows), "frame rows")
     _lib.check(L.ertm_set_march(args.march), "march")
+    _lib.check(L.ertm_set_march_stress(args.march_stress), "march stress")
     _lib.check(L.ertm_set_tma(args.tma), "tma")
     wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt, **({"n_shots": args.shots} if args.shots else {}))
     imager, solver = workloads.imager_for(wl)

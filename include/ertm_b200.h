@@ -144,6 +144,11 @@ int32_t ertm_set_frame_rows(int32_t rows);
  * instead of one block per tile (default 4); 0: tiles.  Results do not depend
  * on it. */
 int32_t ertm_set_march(int32_t enable);
+/* 1: the elastic stress phase of those interiors marches too, in the same
+ * segments, with the fused imaging epilogue run per 16-row chunk; 0
+ * (default): tiles.  Takes effect while ertm_set_march is non-zero.  Results
+ * do not depend on it. */
+int32_t ertm_set_march_stress(int32_t enable);
 /* Online autotuning of batched ticks (default on): the first ticks of each
  * group shape (engine, order, works, size class) try tile heights 8/16/32,
  * split off/on and one or two lanes, timed with CUDA events; the fastest is

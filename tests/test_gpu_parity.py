@@ -232,7 +232,7 @@ def split_always(eb):
     _lib.check(_lib.lib().ertm_set_tile_split(0), "split")
 
 
-@pytest.mark.parametrize("march", [0, 4, 8])
+@pytest.mark.parametrize("march,march_stress", [(0, 0), (4, 0), (8, 0), (4, 1)])
 @pytest.mark.parametrize("frame_rows", [0, 8])
 @pytest.mark.parametrize("tma", [1, 0])
 @pytest.mark.parametrize("engine,boundary,mechanism,tile_rows", [
@@ -240,7 +240,7 @@ def split_always(eb):
     ("elastic", "free", "explosive", 16), ("elastic", "cpml", "force_z", 8), ("elastic", "free", "shear", 32),
     ("viscoacoustic", "cpml", "explosive", 16)])
 def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, boundary, mechanism, tile_rows, tma,
-                                                     frame_rows, march):
+                                                     frame_rows, march, march_stress):
     """Interior tiles and the boundary frame in separate launches (the source
     node's tile, inside the interior rectangle, goes with the frame, as one
     tile or as several lower frame tiles), interior tiles staged by TMA or by
@@ -252,6 +252,7 @@ def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, b
     _lib.check(_lib.lib().ertm_set_tma(tma), "tma")
     _lib.check(_lib.lib().ertm_set_frame_rows(frame_rows), "frame rows")
     _lib.check(_lib.lib().ertm_set_march(march), "march")
+    _lib.check(_lib.lib().ertm_set_march_stress(march_stress), "march stress")
     try:
         rng = np.random.default_rng(11)
         nz, nx = 150, 200
@@ -275,6 +276,7 @@ def test_interior_and_boundary_launches_match_oracle(eb, split_always, engine, b
         _lib.check(_lib.lib().ertm_set_tma(0), "tma")
         _lib.check(_lib.lib().ertm_set_frame_rows(0), "frame rows")
         _lib.check(_lib.lib().ertm_set_march(4), "march")
+        _lib.check(_lib.lib().ertm_set_march_stress(0), "march stress")
     assert _lib.lib().ertm_stage_timeouts() == 0
     for n in comps:
         if engine == "viscoacoustic":
@@ -306,7 +308,7 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
     out = {}
     cases = ((1, 1, 0, 0, 0), (2, 1, 0, 0, 0), (2, 2, 0, 0, 0), (1, 2, 0, 0, 0), (2, 2, 1, 0, 0), (1, 2, 1, 0, 0),
              (2, 2, 0, 32, 8), (2, 1, 0, 32, 16), (2, 2, 1, 16, 8), (2, 4, 0, 0, 0), (1, 4, 1, 32, 0),
-             (2, 2, 0, 32, 0, 8), (2, 1, 0, 32, 16, 2), (2, 2, 0, 32, 0, 0))
+             (2, 2, 0, 32, 0, 8), (2, 1, 0, 32, 16, 2), (2, 2, 0, 32, 0, 0), (2, 2, 0, 32, 0, 4, 1))
     for mode, lanes, assign, rows, frame_rows, *rest in cases:
         _lib.check(_lib.lib().ertm_set_tile_split(mode), "split")
         _lib.check(_lib.lib().ertm_set_tick_lanes(lanes), "lanes")
@@ -314,6 +316,7 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
         _lib.check(_lib.lib().ertm_set_tile_rows(rows), "tile rows")
         _lib.check(_lib.lib().ertm_set_frame_rows(frame_rows), "frame rows")
         _lib.check(_lib.lib().ertm_set_march(rest[0] if rest else 4), "march")
+        _lib.check(_lib.lib().ertm_set_march_stress(rest[1] if len(rest) > 1 else 0), "march stress")
         try:
             out[(mode, lanes, assign, rows, frame_rows, *rest)] = BatchMigrator(imager).migrate_shots(
                 shots, model, modes=("pp", "ps"))
@@ -324,6 +327,7 @@ def test_batched_images_equal_with_and_without_split_launches(eb):
             _lib.check(_lib.lib().ertm_set_tile_rows(0), "tile rows")
             _lib.check(_lib.lib().ertm_set_frame_rows(0), "frame rows")
             _lib.check(_lib.lib().ertm_set_march(4), "march")
+            _lib.check(_lib.lib().ertm_set_march_stress(0), "march stress")
     for key in cases[1:]:
         for a, b in zip(out[cases[0]], out[key]):
             for x1, x2 in zip(a, b):
