@@ -308,39 +308,6 @@ __global__ void k_stab_scale(const DevProp* props, int pi, StabState* st, double
   }
 }
 
-// Radial wavenumber taper 1 − (k − c)/0.15 clipped to [0, 1], applied to a
-// half spectrum (numerics.py:424-442); the 1/(nz·nx) inverse-FFT scale is
-// folded in.
-__global__ void k_lowpass_apply(double2* spec, int nz, int nx, double dz, double dx, double cutoff) {
-  const int nxh = nx / 2 + 1;
-  const int jx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int iz = blockIdx.y * blockDim.y + threadIdx.y;
-  if (iz >= nz || jx >= nxh) return;
-  const int kzi = iz < (nz + 1) / 2 ? iz : iz - nz;
-  const int kxi = jx < (nx + 1) / 2 ? jx : jx - nx;
-  const double kz = (double)kzi * (1.0 / (nz * dz)) / (0.5 / dz);
-  const double kx = (double)kxi * (1.0 / (nx * dx)) / (0.5 / dx);
-  const double rad = sqrt(kz * kz + kx * kx);
-  double h = 1.0 - (rad - cutoff) / 0.15;
-  h = h < 0.0 ? 0.0 : (h > 1.0 ? 1.0 : h);
-  h /= (double)nz * (double)nx;
-  double2& v = spec[(size_t)iz * nxh + jx];
-  v.x *= h;
-  v.y *= h;
-}
-
-// padded float32 field (pitch ld) ↔ dense float64 (nzp, nxp)
-__global__ void k_f32_to_f64(const float* src, int ld, double* dst, int nz, int nx) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i < nz && j < nx) dst[(size_t)i * nx + j] = (double)src[(size_t)i * ld + j];
-}
-__global__ void k_f64_to_f32(const double* src, float* dst, int ld, int nz, int nx) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i < nz && j < nx) dst[(size_t)i * ld + j] = __double2float_rn(src[(size_t)i * nx + j]);
-}
-
 // ---------------------------------------------------------------------------
 // image post-processing (imaging.py:326-331, 476-502; numerics.py:398-404)
 // ---------------------------------------------------------------------------
@@ -384,11 +351,17 @@ __global__ void k_mask_cast(const double* a, float* out, int nz, int nx, int npm
 }
 
 // stack_images (pipeline.py:133-161): per-image max|·| then normalised mean.
+// The maximum propagates NaN as np.max does (pipeline.py:147): |NaN| has its
+// sign bit clear and its bits order above +inf as unsigned words, so the
+// atomicMax of the bit patterns keeps it, and k_stack_add then leaves the
+// image undivided (`scale > 0` is false for NaN).
+__device__ __forceinline__ float max_nan(float m, float v) { return (v > m || v != v) ? v : m; }
+
 __global__ void k_absmax_f32(const float* a, int64_t n, unsigned int* out_bits) {
   float m = 0.f;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-    m = fmaxf(m, fabsf(a[k]));
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    m = max_nan(m, fabsf(a[k]));
+  for (int o = 16; o > 0; o >>= 1) m = max_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(m));
 }
 

@@ -25,6 +25,8 @@
 
 #include "../../include/ertm_b200.h"
 #include "aux_kernels.cuh"
+#include "line_fft.cuh"
+#include "line_fft_plan.h"
 #include "step_kernels.cuh"
 
 using namespace ertm;
@@ -122,26 +124,10 @@ struct StencilProfile {
 };
 StencilProfile g_prof;
 
-// cuFFT plans for the image low-pass, cached by shape (and stream).
 struct FftPair {
   cufftHandle fwd = 0, inv = 0;
 };
-std::map<std::tuple<int, int, cudaStream_t>, FftPair> g_fft_plans;
 std::mutex g_fft_mutex;
-
-FftPair image_fft(int nz, int nx, cudaStream_t st) {
-  std::lock_guard<std::mutex> lock(g_fft_mutex);
-  auto key = std::make_tuple(nz, nx, st);
-  auto it = g_fft_plans.find(key);
-  if (it != g_fft_plans.end()) return it->second;
-  FftPair p;
-  CKFFT(cufftPlan2d(&p.fwd, nz, nx, CUFFT_D2Z));
-  CKFFT(cufftPlan2d(&p.inv, nz, nx, CUFFT_Z2D));
-  CKFFT(cufftSetStream(p.fwd, st));
-  CKFFT(cufftSetStream(p.inv, st));
-  g_fft_plans[key] = p;
-  return p;
-}
 
 // Batched 1-D plans of the short-time Q filter (L-point frames, `batch` of
 // them), cached by frame length, batch and stream.
@@ -198,6 +184,145 @@ struct DevBuf {
 
 void upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st));
+}
+
+// --------------------------------------------------------------------------
+// Wavenumber low-pass with NumPy's FFT arithmetic (line_fft.cuh)
+// --------------------------------------------------------------------------
+// Plans per device and transform length: factors and twiddles from the host
+// plan; for a Bluestein length, the kernel's forward transform is computed
+// once by the device passes themselves and mirrored as the library mirrors
+// it (the upper half of the spectrum reuses the lower half's values).
+struct LineFftPlan {
+  FftPlanDev dev{};
+  DevBuf tables;
+};
+std::map<std::pair<int, int>, std::unique_ptr<LineFftPlan>> g_line_plans;
+std::mutex g_line_mutex;
+
+constexpr int kLineThreads = 256;
+constexpr size_t kLineSmemMax = 227 * 1024;       // opt-in dynamic shared memory per CTA
+constexpr int64_t kLineScratchCtas = 296;         // CTAs of a launch whose lines do not fit in shared memory
+
+void launch_lines(const FftPlanDev& plan, bool fwd, int load, const void* src, int64_t src_pitch, int64_t lines,
+                  double2* dst, double fct, double dz, double dx, double cutoff, cudaStream_t st) {
+  static std::mutex attr_mutex;
+  static std::map<int, bool> attr_set;
+  {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(attr_mutex);
+    if (!attr_set[dev]) {
+      CK(cudaFuncSetAttribute(k_fft_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLineSmemMax));
+      CK(cudaFuncSetAttribute(k_fft_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLineSmemMax));
+      attr_set[dev] = true;
+    }
+  }
+  LineJob J{};
+  J.plan = plan;
+  J.load = load;
+  J.lines = lines;
+  J.src = src;
+  J.src_pitch = src_pitch;
+  J.dst = dst;
+  J.fct = fct;
+  J.dz = dz;
+  J.dx = dx;
+  J.cutoff = cutoff;
+  const size_t smem = (size_t)2 * plan.n2 * sizeof(double2);
+  DevBuf scratch;
+  unsigned grid;
+  if (smem <= kLineSmemMax) {
+    J.use_smem = 1;
+    grid = (unsigned)std::min<int64_t>(lines, 1 << 20);
+  } else {
+    J.use_smem = 0;
+    grid = (unsigned)std::min<int64_t>(lines, kLineScratchCtas);
+    scratch = DevBuf((size_t)grid * smem, st);
+    J.scratch = scratch.as<double2>();
+  }
+  const size_t dyn = J.use_smem ? smem : 0;
+  if (fwd) k_fft_lines<true><<<grid, kLineThreads, dyn, st>>>(J);
+  else k_fft_lines<false><<<grid, kLineThreads, dyn, st>>>(J);
+  ++g_launches;
+  CK(cudaGetLastError());
+}
+
+const FftPlanDev& line_plan(int n, cudaStream_t st) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_line_mutex);
+  auto it = g_line_plans.find({dev, n});
+  if (it != g_line_plans.end()) return it->second->dev;
+  using namespace fftplan;
+  REQUIRE(n >= 1, "FFT length must be positive");
+  const bool blue = use_bluestein((size_t)n);
+  const size_t n2 = blue ? good_size_cmplx(2 * (size_t)n - 1) : (size_t)n;
+  const CooleyTukey ct(n2);
+  REQUIRE(ct.fct.size() <= (size_t)kFftMaxFactors, "FFT length has too many factors");
+  std::vector<CxH> bk, kernel;
+  if (blue) bluestein_chirp((size_t)n, n2, bk, kernel);
+  const size_t ntw = ct.tw.size(), nbk = bk.size(), nbkf = blue ? n2 : 0;
+  auto L = std::make_unique<LineFftPlan>();
+  L->tables = DevBuf(std::max<size_t>(1, ntw + nbk + nbkf) * sizeof(double2), st);
+  double2* tw = L->tables.as<double2>();
+  upload(tw, ct.tw.data(), ntw * sizeof(double2), st);
+  upload(tw + ntw, bk.data(), nbk * sizeof(double2), st);
+  FftPlanDev& d = L->dev;
+  d.n = n;
+  d.n2 = (int)n2;
+  d.blue = blue ? 1 : 0;
+  d.nfact = (int)ct.fct.size();
+  for (size_t f = 0; f < ct.fct.size(); ++f) {
+    d.fct[f] = ct.fct[f];
+    d.twoff[f] = ct.twoff[f];
+    d.twsoff[f] = ct.twsoff[f];
+  }
+  d.tw = tw;
+  d.bk = tw + ntw;
+  d.bkf = tw + ntw + nbk;
+  if (blue) {
+    // the kernel's transform: one line through the length-n2 Cooley-Tukey plan
+    FftPlanDev inner = d;
+    inner.n = (int)n2;
+    inner.blue = 0;
+    DevBuf line(n2 * sizeof(double2), st);
+    upload(line.p, kernel.data(), n2 * sizeof(double2), st);
+    launch_lines(inner, true, LINE_LOAD_C, line.p, (int64_t)n2, 1, line.as<double2>(), 1.0, 0.0, 0.0, 0.0, st);
+    std::vector<CxH> spec(n2), full(n2);
+    CK(cudaMemcpyAsync(spec.data(), line.p, n2 * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t m = 0; m < n2; ++m) full[m] = spec[std::min(m, n2 - m)];
+    upload(const_cast<double2*>(d.bkf), full.data(), n2 * sizeof(double2), st);
+  }
+  CK(cudaStreamSynchronize(st));
+  const FftPlanDev& out = L->dev;
+  g_line_plans[{dev, n}] = std::move(L);
+  return out;
+}
+
+// numerics.py:424-442 on an (nz, nx) array: Re(ifft2(fft2(a) · taper)), the
+// transforms along x then z as numpy.fft.fft2/ifft2 take them.  Input: real
+// float32 rows of pitch in_pitch (a padded field) or float64 (an image);
+// output likewise (float32 rounded to nearest).  A and B hold nz·nx complex
+// values each.  In place (out == in) is allowed.
+void lowpass2d(int nz, int nx, double dz, double dx, double cutoff, const void* in, bool in_f32, int64_t in_pitch,
+               void* out, bool out_f32, int64_t out_pitch, double2* A, double2* B, cudaStream_t st) {
+  const FftPlanDev& px = line_plan(nx, st);
+  const FftPlanDev& pz = line_plan(nz, st);
+  const dim3 tb(32, 8);
+  auto tgrid = [](int rows, int cols) { return dim3((cols + 31) / 32, (rows + 31) / 32); };
+  launch_lines(px, true, in_f32 ? LINE_LOAD_F32 : LINE_LOAD_F64, in, in_pitch, nz, A, 1.0, 0, 0, 0, st);
+  k_transpose_lines<T_COMPLEX><<<tgrid(nz, nx), tb, 0, st>>>(A, nz, nx, B, 0);
+  launch_lines(pz, true, LINE_LOAD_C, B, nz, nx, B, 1.0, 0, 0, 0, st);
+  k_transpose_lines<T_COMPLEX><<<tgrid(nx, nz), tb, 0, st>>>(B, nx, nz, A, 0);
+  launch_lines(px, false, LINE_LOAD_C_TAPER, A, nx, nz, A, 1.0 / (double)nx, dz, dx, cutoff, st);
+  k_transpose_lines<T_COMPLEX><<<tgrid(nz, nx), tb, 0, st>>>(A, nz, nx, B, 0);
+  launch_lines(pz, false, LINE_LOAD_C, B, nz, nx, B, 1.0 / (double)nz, 0, 0, 0, st);
+  if (out_f32) k_transpose_lines<T_REAL_F32><<<tgrid(nx, nz), tb, 0, st>>>(B, nx, nz, out, out_pitch);
+  else k_transpose_lines<T_REAL_F64><<<tgrid(nx, nz), tb, 0, st>>>(B, nx, nz, out, out_pitch);
+  g_launches += 4;
+  CK(cudaGetLastError());
 }
 
 int comp_offsets(int comp, double& xo, double& zo) {
@@ -259,14 +384,9 @@ struct Prop {
   int n_coef = 0;
   mutable std::map<int, std::array<CUtensorMap, 3>> tma;   // tensor maps per tile height (see prop_tma)
   DevBuf tma_dev;                // the same maps in device memory for tile heights 8, 16, 32
-  // cuFFT for the compensated viscoacoustic low-pass
-  cufftHandle fwd_plan = 0, inv_plan = 0;
-  DevBuf fft_real, fft_spec;
+  // complex work arrays of the compensated viscoacoustic low-pass (nzp·nxp each)
+  DevBuf lp_a, lp_b;
 
-  ~Prop() {
-    if (fwd_plan) cufftDestroy(fwd_plan);
-    if (inv_plan) cufftDestroy(inv_plan);
-  }
   DevProp* dp() const { return d_desc.as<DevProp>(); }
   int n_fields() const { return h.n_fields; }
   float* field(int slot) const { return h.f[slot]; }
@@ -847,23 +967,16 @@ int tiles_for(const DevProp& h, int tz) { return ((h.nxp + TILE_X - 1) / TILE_X)
 template <int M>
 void launch_epilogue_M(const Prop& P, const Epilogue& E);
 
+// The wavenumber low-pass of a padded float32 field in place (the
+// compensated viscoacoustic stabilisation, propagation.py:744-749).
 void lowpass_field(Prop& P, float* f, double cutoff) {
   const int nz = P.h.nzp, nx = P.h.nxp;
-  if (!P.fwd_plan) {
-    CKFFT(cufftPlan2d(&P.fwd_plan, nz, nx, CUFFT_D2Z));
-    CKFFT(cufftPlan2d(&P.inv_plan, nz, nx, CUFFT_Z2D));
-    CKFFT(cufftSetStream(P.fwd_plan, P.st));
-    CKFFT(cufftSetStream(P.inv_plan, P.st));
-    P.fft_real = DevBuf((size_t)nz * nx * sizeof(double), P.st);
-    P.fft_spec = DevBuf((size_t)nz * (nx / 2 + 1) * sizeof(double2), P.st);
+  if (!P.lp_a.p) {
+    P.lp_a = DevBuf((size_t)nz * nx * sizeof(double2), P.st);
+    P.lp_b = DevBuf((size_t)nz * nx * sizeof(double2), P.st);
   }
-  const dim3 b2(32, 8), g2((nx + 31) / 32, (nz + 7) / 8), gh((nx / 2 + 1 + 31) / 32, (nz + 7) / 8);
-  g_launches += 5;  // conversion, D2Z, filter, Z2D, conversion
-  k_f32_to_f64<<<g2, b2, 0, P.st>>>(f, P.h.ld, P.fft_real.as<double>(), nz, nx);
-  CKFFT(cufftExecD2Z(P.fwd_plan, P.fft_real.as<double>(), P.fft_spec.as<cufftDoubleComplex>()));
-  k_lowpass_apply<<<gh, b2, 0, P.st>>>(P.fft_spec.as<double2>(), nz, nx, P.cfg.dz, P.cfg.dx, cutoff);
-  CKFFT(cufftExecZ2D(P.inv_plan, P.fft_spec.as<cufftDoubleComplex>(), P.fft_real.as<double>()));
-  k_f64_to_f32<<<g2, b2, 0, P.st>>>(P.fft_real.as<double>(), f, P.h.ld, nz, nx);
+  lowpass2d(nz, nx, P.cfg.dz, P.cfg.dx, cutoff, f, true, P.h.ld, f, true, P.h.ld, P.lp_a.as<double2>(),
+            P.lp_b.as<double2>(), P.st);
 }
 
 // Algorithmic HBM bytes of one propagator step: each state array read and
@@ -1834,21 +1947,41 @@ struct StackScratch {
   double* sum = nullptr;
   unsigned int* scale = nullptr;
 };
-std::map<int, StackScratch> g_stack_scratch;
+std::map<std::pair<int, CUcontext>, StackScratch> g_stack_scratch;
 std::mutex g_stack_mutex;
 
+// The calling thread's current driver context (through the runtime's
+// driver entry point, so the library needs no link against libcuda).
+CUcontext current_context() {
+  static PFN_cuCtxGetCurrent_v4000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    CK(cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q));
+    REQUIRE(q == cudaDriverEntryPointSuccess && p, "cuCtxGetCurrent is not available");
+    return reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+  }();
+  CUcontext c = nullptr;
+  REQUIRE(fn(&c) == CUDA_SUCCESS, "cuCtxGetCurrent failed");
+  return c;
+}
+
 // Device addresses of the scratch arrays for the current device; looked up
-// once per device (the host-side names are not device addresses).
+// once per device and context (the host-side names are not device
+// addresses).  Keying on the context as well means a device reset, which
+// gives the device a new primary context, leads to a fresh lookup instead of
+// addresses in a context that no longer exists.
 StackScratch stack_scratch() {
   int dev = 0;
   CK(cudaGetDevice(&dev));
+  CK(cudaFree(nullptr));   // makes the device's primary context current (allocates nothing)
+  const std::pair<int, CUcontext> key{dev, current_context()};
   std::lock_guard<std::mutex> lock(g_stack_mutex);
-  auto it = g_stack_scratch.find(dev);
+  auto it = g_stack_scratch.find(key);
   if (it != g_stack_scratch.end()) return it->second;
   StackScratch s;
   CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&s.sum), g_stack_sum));
   CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&s.scale), g_stack_scale));
-  g_stack_scratch[dev] = s;
+  g_stack_scratch[key] = s;
   return s;
 }
 
@@ -2496,18 +2629,30 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
     }
     g_launches += 2 + (laplacian ? 1 : 0);
     if (lowpass < 1.0) {
-      DevBuf spec((size_t)nz * (nx / 2 + 1) * 16, st);
-      const FftPair fp = image_fft(nz, nx, st);
-      CKFFT(cufftExecD2Z(fp.fwd, cur, spec.as<cufftDoubleComplex>()));
-      const dim3 gh((nx / 2 + 1 + 31) / 32, (nz + 7) / 8);
-      k_lowpass_apply<<<gh, b2, 0, st>>>(spec.as<double2>(), nz, nx, dz, dx, lowpass);
-      ++g_launches;
-      CKFFT(cufftExecZ2D(fp.inv, spec.as<cufftDoubleComplex>(), other));
+      DevBuf wa((size_t)n * sizeof(double2), st), wb((size_t)n * sizeof(double2), st);
+      lowpass2d(nz, nx, dz, dx, lowpass, cur, false, nx, other, false, nx, wa.as<double2>(), wb.as<double2>(), st);
       std::swap(cur, other);
     }
     k_mask_cast<<<g2, b2, 0, st>>>(cur, o.as<float>(), nz, nx, npml, top_mask);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t ertm_lowpass_wavenumber(int32_t nz, int32_t nx, double dx, double dz, double cutoff, const double* in,
+                                double* out, void* stream) {
+  return guarded([&] {
+    REQUIRE(nz >= 1 && nx >= 1 && in && out, "bad arguments");
+    REQUIRE(cutoff > 0.0 && cutoff <= 1.0, "cutoff fraction must lie in (0, 1]");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)nz * nx;
+    InArray a(in, n * 8, st);
+    OutArray b(out, n * 8, st);
+    DevBuf wa(n * sizeof(double2), st), wb(n * sizeof(double2), st);
+    lowpass2d(nz, nx, dz, dx, cutoff, a.as<double>(), false, nx, b.d, false, nx, wa.as<double2>(),
+              wb.as<double2>(), st);
+    b.finish();
     CK(cudaStreamSynchronize(st));
   });
 }
@@ -2681,8 +2826,10 @@ int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int3
       CK(cudaMemsetAsync(sc.p, 0, 4, st));
       if (normalize) k_absmax_f32<<<std::min<unsigned>(g, 1184), 256, 0, st>>>(img.as<float>(), n, sc.as<unsigned>());
       k_stack_add<<<g, 256, 0, st>>>(img.as<float>(), n, sc.as<unsigned>(), normalize, acc.as<double>());
+      g_launches += normalize ? 2 : 1;
     }
     k_stack_finish<<<g, 256, 0, st>>>(acc.as<double>(), n, n_images, o.as<float>());
+    ++g_launches;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
     CK(cudaStreamSynchronize(st));
@@ -2748,6 +2895,7 @@ int32_t ertm_stack_noalloc(int32_t n_images, int64_t n, const float* const* imag
     if (normalize) {
       const unsigned g = (unsigned)std::min<int64_t>((n + 255) / 256, 1184);
       for (int k = 0; k < n_images; ++k) k_absmax_f32<<<g, 256, 0, st>>>(images[k], n, S.scale + k);
+      g_launches += n_images;
     }
     for (int64_t off = 0; off < n; off += kStackChunk) {
       const int64_t len = std::min<int64_t>(kStackChunk, n - off);
@@ -2756,6 +2904,7 @@ int32_t ertm_stack_noalloc(int32_t n_images, int64_t n, const float* const* imag
       for (int k = 0; k < n_images; ++k)
         k_stack_add<<<g, 256, 0, st>>>(images[k] + off, len, S.scale + k, normalize, S.sum);
       k_stack_finish<<<g, 256, 0, st>>>(S.sum, len, n_images, out + off);
+      g_launches += n_images + 1;
     }
     CK(cudaGetLastError());
   });

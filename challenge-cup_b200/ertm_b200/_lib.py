@@ -112,6 +112,7 @@ _SIGNATURES = {
     "ertm_stack": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
     "ertm_stack_noalloc": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
     "ertm_stack_partial": (_I32, [_I32, C.c_int64, _P, _I32, _P, _P]),
+    "ertm_lowpass_wavenumber": (_I32, [_I32, _I32, C.c_double, C.c_double, C.c_double, _P, _P, _P]),
     "ertm_resample": (_I32, [_P, C.c_int64, C.c_int64, _P, _P, _I32, C.c_int64, _P, _P]),
     "ertm_mute": (_I32, [_P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
     "ertm_taper": (_I32, [_P, C.c_int64, C.c_int64, _P, C.c_int64, _P, _P]),

@@ -126,3 +126,23 @@ def resample_sinc(data: np.ndarray, dt_in: float, dt_out: float, *, axis: int = 
     if squeeze:
         out = out[:, 0]
     return out.T if axis == 1 else out
+
+
+def lowpass_wavenumber(field: np.ndarray, dx: float, dz: float, cutoff_fraction: float = 0.85) -> np.ndarray:
+    """Wavenumber low-pass (numerics.py:424-442) on the device.
+
+    ``Re(ifft2(fft2(field) · taper))`` with the radial taper
+    ``clip(1 − (k − cutoff)/0.15, 0, 1)`` over Nyquist-normalised wavenumbers.
+    The CUDA transforms follow numpy.fft's arithmetic, so the float64 result
+    equals the reference's bit for bit.  Returns a new float64 array."""
+    if not 0.0 < cutoff_fraction <= 1.0:
+        raise ValueError(f"cutoff_fraction must lie in (0, 1], got {cutoff_fraction}")
+    from . import _lib
+    a = np.ascontiguousarray(field, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError(f"lowpass_wavenumber takes a 2-D field, got {a.ndim}-D")
+    out = np.empty_like(a)
+    nz, nx = a.shape
+    _lib.check(_lib.lib().ertm_lowpass_wavenumber(nz, nx, float(dx), float(dz), float(cutoff_fraction),
+                                                  a.ctypes.data, out.ctypes.data, None), "lowpass_wavenumber")
+    return out

@@ -261,6 +261,14 @@ int32_t ertm_session_active(void* session);
 int64_t ertm_session_ticks(void* session);
 int32_t ertm_session_destroy(void* session);
 
+/* lowpass_wavenumber (numerics.py:424-442): out = Re(ifft2(fft2(in) · taper))
+ * of an (nz, nx) float64 array, the radial taper 1 − (k − cutoff)/0.15
+ * clipped to [0, 1] over the Nyquist-normalised wavenumbers.  The transforms
+ * reproduce numpy.fft's arithmetic, so the result equals the reference's bit
+ * for bit.  Host or device pointers; in place allowed. */
+int32_t ertm_lowpass_wavenumber(int32_t nz, int32_t nx, double dx, double dz, double cutoff, const double* in,
+                                double* out, void* stream);
+
 /* Normalisation and _postprocess (imaging.py:326-333, 476-502): image =
  * num/(illum+eps)/(rillum+eps) as selected, Laplacian, wavenumber low-pass
  * (lowpass < 1), PML mask of width npml (top too when top_mask). */
