@@ -1,16 +1,19 @@
 #!/usr/bin/env python
 """Benchmark of the B200 RTM hot path.
 
-Default workload (one GPU): elastic P-SV borehole 4C RTM with PP and PS
-imaging — 401×601 grid at 5 m, 8 surface shots, 100 well receivers, 4912
-steps (1.5 s at the CFL dt), normalized condition, divcurl separation.  A
-benchmark step migrates all shots of the job (PP and PS from one
-forward/replay/backward pass per shot) and stacks them.
+Default workload (one GPU): the viscoacoustic GSLS configuration with Q
+compensation - 2001×801 grid at 5 m, L = 3 relaxation mechanisms, layered
+vp 1800-4000 m/s and Q 30-200, 64 surface shots 150 m apart with 400
+receivers each, 4706 steps (1.6 s at dt 0.34 ms), 30 Hz Ricker, normalized
+condition, compensation with α_c = 1, 40 dB gain budget and f_max 60 Hz.
+The job's 64 shots are migrated four per benchmark step (the step's shots
+advance together in lockstep ticks) and each step's images are stacked; the
+steps cycle through the job's shots.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-    torchrun --nproc-per-node N bench.py --gpus N ...   (weak scaling: a job
-        of 8·N shots sharded over the ranks; one NCCL all-reduce of the
-        float64 stack per job)
+    python bench.py --gpus N ...      (no torchrun: the benchmark starts N
+        ranks itself, one per GPU; weak scaling - every rank migrates its own
+        shots per step, one NCCL all-reduce of the float64 stack per step)
 
 One JSON line is printed by rank 0.
 """
@@ -20,6 +23,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -33,24 +37,42 @@ import numpy as np  # noqa: E402
 
 METRIC = "shots/s & Gcell-updates/s batched vs plain on 1 B200; p99 latency @ 1e-4 err"
 FALLBACK_HBM_GBS = 6650.0
+SHOTS_PER_STEP = {"visco": 4, "elastic4c": 8, "acoustic": 3}
 
 
-def parse_args() -> argparse.Namespace:
+def parse_args(argv=None) -> argparse.Namespace:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--config", default="elastic4c")
+    ap.add_argument("--config", default="visco", choices=sorted(SHOTS_PER_STEP))
     ap.add_argument("--nt", type=int, default=None, help="override the number of time steps (profiling runs)")
-    ap.add_argument("--shots", type=int, default=None, help="override shots per rank")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--shots", type=int, default=None, help="override the shots per rank and step")
+    ap.add_argument("--plain-steps", type=int, default=3, help="timed steps of the plain one-shot arm")
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=48)
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs in the serving run (0: no serving run)")
+    ap.add_argument("--serve-scale", choices=("short", "full"), default="short",
+                    help="short: grids up to 1024x512, nt 500-2000, 1-4 shots (seconds); full: the serving "
+                         "configuration (grids up to 4096x2048, nt 1000-8000, 1-16 shots, minutes)")
+    ap.add_argument("--uneven-shots", type=int, default=24,
+                    help="shots of the uneven batch (256-shot configuration) timed batched vs plain (0: skip)")
     ap.add_argument("--no-adjacent", action="store_true",
                     help="skip timing the steps either side of the path (preprocessing, Q filter, SEG-Y, stack)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
+
+
+def launch_ranks(args) -> int:
+    """`--gpus N` without a launcher: start N ranks (one per GPU) through
+    torch.distributed.run on 127.0.0.1 and return rank 0's exit status."""
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 # ---------------------------------------------------------------------------
@@ -163,27 +185,37 @@ def committed_traffic(name: str) -> float | None:
 # ---------------------------------------------------------------------------
 # workload helpers
 # ---------------------------------------------------------------------------
-def build_workload(args, world: int):
-    """The job's workload: the configuration's shots per GPU times the world
-    size (weak scaling), every rank building the same seeded job."""
+def build_workload(args):
+    """The configuration's whole job (every rank builds the same seeded job)."""
     from ertm_b200 import workloads
     kw = {"nt": args.nt} if args.nt else {}
-    make = workloads.WORKLOADS[args.config]
-    wl = make(seed=0, **kw, **({"n_shots": args.shots} if args.shots else {}))
-    if world > 1:
-        wl = make(seed=0, n_shots=len(wl.sources) * world, **kw)
-    return wl
+    return workloads.WORKLOADS[args.config](seed=0, **kw)
+
+
+def shots_per_step(args) -> int:
+    return int(args.shots or SHOTS_PER_STEP[args.config])
+
+
+def step_shots(args, n_job: int, world: int, rank: int, k: int) -> list[int]:
+    """Job shot indices this rank migrates in step k (warm-up steps
+    included): the step takes the next shots_per_step·world shots of the job
+    in order, wrapping around, and rank r takes its contiguous share."""
+    s = shots_per_step(args)
+    base = k * s * world + rank * s
+    return [(base + j) % n_job for j in range(s)]
 
 
 def job_config(wl, args, world: int) -> dict:
     g = wl.model.grid
+    s = shots_per_step(args)
     return {"workload": wl.name, "config": args.config, "nx": g.nx, "nz": g.nz, "dx": g.dx, "nt": wl.nt,
             "dt": wl.dt, "engine": wl.engine, "modes": list(wl.modes), "condition": wl.condition,
-            "separation": wl.separation, "shots_per_job": len(wl.sources), "receivers": wl.receivers.nrec,
-            "components": list(wl.components), "accumulation": "fp64",
-            "l2": "flushed between steps (256 MiB write)",
-            "path": "batched: all shots of a rank in lockstep ticks (form b)",
-            "parallelism": f"shots sharded over {world} GPU(s), one float64 all-reduce of the stack per job"}
+            "separation": wl.separation, "shots_per_job": len(wl.sources), "shots_per_step": s * world,
+            "receivers": wl.receivers.nrec, "components": list(wl.components), "q": wl.q or None,
+            "checkpoint_mb": wl.checkpoint_mb, "accumulation": "fp64",
+            "l2": "flushed between steps (256 MiB write); each step's inputs exceed L2 as well",
+            "path": f"batched: a step's {s} shot(s) per GPU in lockstep ticks (form b), images stacked per step",
+            "parallelism": f"shots sharded over {world} GPU(s), one float64 all-reduce of the stack per step"}
 
 
 def imager_for(wl):
@@ -214,12 +246,12 @@ def step_bytes(prop) -> float:
 # ---------------------------------------------------------------------------
 # CPU oracle sample (baseline)
 # ---------------------------------------------------------------------------
-def cpu_sample(config: str, nt_sample: int) -> dict:
-    """Time the CPU oracle (NumPy restatement of the reference) migrating one
-    shot of the workload for nt_sample steps; extrapolate to the full job."""
+def cpu_sample(config: str, nt_sample: int, nt_override: int | None = None) -> dict:
+    """Time the CPU oracle (NumPy restatement of the reference, single
+    thread) migrating one shot of the workload for nt_sample steps."""
     import oracle as orc
     from ertm_b200 import workloads
-    wl = workloads.WORKLOADS[config](seed=0)
+    wl = workloads.WORKLOADS[config](seed=0, **({"nt": nt_override} if nt_override else {}))
     imager, solver = imager_for(wl)
     nrec = wl.receivers.nrec
     rng = np.random.default_rng(5)
@@ -235,46 +267,65 @@ def cpu_sample(config: str, nt_sample: int) -> dict:
                             gain_budget_db=wl.q["gain_budget_db"])
     t0 = time.perf_counter()
     orc.migrate(comps, wl.dt, wl.sources[0], wl.receivers, wl.model, sv, imager.config, q)
-    secs = time.perf_counter() - t0
-    migrates_per_shot = len(wl.modes)      # the reference runs one RTMImager per mode
-    per_shot = secs * (wl.nt / nt_sample) * migrates_per_shot
-    return {"per_shot_s": per_shot, "sample_s": secs, "nt_sample": nt_sample, "nt": wl.nt,
-            "migrates_per_shot": migrates_per_shot, "cells": wl.cells}
+    return {"secs": time.perf_counter() - t0, "nt_sample": nt_sample, "nt": wl.nt, "cells": wl.cells,
+            "migrates_per_shot": len(wl.modes)}      # the reference runs one RTMImager per imaging mode
 
 
-def _cpu_worker(args):
-    config, nt_sample = args
+def per_shot_seconds(short: list[dict], long: list[dict]) -> dict:
+    """Split sample timings of two lengths into set-up and per-step cost and
+    extrapolate one whole shot: setup + per_step · nt, times the migrates a
+    shot needs.  Steps of the samples that never reach a periodic low-pass
+    (every 20th backward step from step 40) leave its FFT cost out, which
+    favours the CPU."""
+    n1, n2 = short[0]["nt_sample"], long[0]["nt_sample"]
+    t1 = statistics.mean(r["secs"] for r in short)
+    t2 = statistics.mean(r["secs"] for r in long)
+    per_step = max(t2 - t1, 1e-9) / (n2 - n1)
+    setup = max(t1 - n1 * per_step, 0.0)
+    r = long[0]
+    return {"per_shot_s": (setup + per_step * r["nt"]) * r["migrates_per_shot"], "setup_s": setup,
+            "per_step_s": per_step, "n1": n1, "n2": n2, "nt": r["nt"], "cells": r["cells"],
+            "migrates_per_shot": r["migrates_per_shot"]}
+
+
+def _cpu_worker(task):
     sys.path[:0] = [str(ROOT), str(ROOT / "challenge-cup_b200")]
-    return cpu_sample(config, nt_sample)
+    return cpu_sample(*task)
 
 
 def run_reference(args, dist: Dist) -> None:
+    """The reference's CPU implementation of the path (the NumPy oracle port:
+    the reference is pure Python) on every host core of rank 0's machine."""
     if dist.rank != 0:
         return
     import multiprocessing as mp
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
     cores = os.cpu_count() or 1
-    nt_sample = max(8, args.cpu_sample_steps // 4)
+    n1, n2 = 4, 16
     ctx = mp.get_context("spawn")
-    times = []
+    walls, shorts, longs = [], [], []
     with ctx.Pool(cores) as pool:
         for i in range(args.warmup + args.steps):
+            tasks = [(args.config, n1 if c % 2 == 0 else n2, args.nt) for c in range(cores)]
             t0 = time.perf_counter()
-            res = pool.map(_cpu_worker, [(args.config, nt_sample)] * cores)
+            res = pool.map(_cpu_worker, tasks)
             if i >= args.warmup:
-                times.append((time.perf_counter() - t0, res))
-    wall = sum(t for t, _ in times) / len(times)
-    per_shot = statistics.mean(r["per_shot_s"] for _, rs in times for r in rs)
-    value = cores / per_shot
-    cells = times[0][1][0]["cells"]
-    nt = times[0][1][0]["nt"]
-    sample = (f"{cores} spawned processes, each migrating one shot of the workload for {nt_sample} of {nt} "
-              f"steps with the NumPy oracle; extrapolated linearly in steps, x{times[0][1][0]['migrates_per_shot']}"
-              f" migrates per shot (one per imaging mode)")
+                walls.append(time.perf_counter() - t0)
+                shorts += [r for r in res if r["nt_sample"] == n1]
+                longs += [r for r in res if r["nt_sample"] == n2]
+    est = per_shot_seconds(shorts, longs or shorts)
+    value = cores / est["per_shot_s"]
+    sample = (f"{cores} spawned single-threaded processes per step, each migrating one shot of the workload for "
+              f"{n1} or {n2} of {est['nt']} steps with the NumPy oracle; set-up ({est['setup_s']:.2f} s) and "
+              f"per-step cost ({est['per_step_s'] * 1e3:.0f} ms) separated from the two lengths and extrapolated "
+              f"to the whole shot, x{est['migrates_per_shot']} migrates per shot (one per imaging mode)")
+    wl = build_workload(args)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": job_config(build_workload(args, dist.world), args, dist.world),
-            "gcell_updates_per_s": value * 3 * nt * cells * times[0][1][0]["migrates_per_shot"] / 1e9,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(walls) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": job_config(wl, args, args.gpus),
+            "gcell_updates_per_s": value * 3 * est["nt"] * est["cells"] * est["migrates_per_shot"] / 1e9,
             "cpu_baseline": {"value": value, "unit": "shots/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -283,13 +334,23 @@ def run_reference(args, dist: Dist) -> None:
 # ---------------------------------------------------------------------------
 # serving (form c)
 # ---------------------------------------------------------------------------
-def serving_run(n_jobs: int) -> dict:
+SERVE_SCALES = {
+    # seconds: grids 256x256..1024x512, nt 500-2000, 1-4 shots
+    "short": dict(max_scale=(4.0, 2.0), nt_range=(500, 2000), max_shots=4),
+    # the serving configuration: grids 256x256..4096x2048, nt 1000-8000, 1-16 shots
+    "full": dict(max_scale=(16.0, 8.0), nt_range=(1000, 8000), max_shots=16),
+}
+
+
+def serving_run(n_jobs: int, scale: str = "short", fractions=(0.5, 0.8)) -> dict:
     """The serving loop on a stream of mixed jobs: once with every job queued
-    at t=0 (saturation), then with Poisson arrivals at 50 % and 80 % of the
-    saturated job rate; per-shot latency = shot completion - job submission."""
+    at t=0 (saturation), then with Poisson arrivals at the given fractions of
+    the saturated job rate; per-shot latency = shot completion - job
+    submission.  Jobs are admitted by their device footprint under the
+    server's budget (170 GB, at most 90 % of free memory)."""
     from ertm_b200 import workloads
     from ertm_b200.serving import RTMServer, percentile
-    spec = dict(max_scale=(4.0, 2.0), nt_range=(500, 2000), max_shots=4)
+    spec = SERVE_SCALES[scale]
     jobs = workloads.serving_jobs(seed=1, n_jobs=n_jobs, **spec)
     n_shots = sum(len(j.shots) for j in jobs)
     cells = sum(3 * j.model.grid.nx * j.model.grid.nz * j.imager.solver_config.nt * len(j.shots) for j in jobs)
@@ -329,17 +390,22 @@ def serving_run(n_jobs: int) -> dict:
         wall = time.perf_counter() - t0
         return {"shots_per_s": n_shots / wall, "wall_s": wall}
 
-    run([0.0] * len(jobs))                      # warm-up (division checks, FFT plans, memory pool)
+    # warm-up (division checks, FFT plans, memory pool): the whole stream when
+    # it takes seconds, its first jobs when it takes minutes
+    run([0.0] * (len(jobs) if scale == "short" else min(len(jobs), 3)))
     sat = run([0.0] * len(jobs))
     job_rate = len(jobs) / sat["wall_s"]
     plain_line = plain()
     rng = np.random.default_rng(7)
-    out = {"workload": (f"{n_jobs} jobs, engine uniform over acoustic/elastic/viscoacoustic, grid 256x256..1024x512 "
-                        f"log-uniform at 5-10 m, nt 500-2000, 1-4 shots, normalized, seeded noise records"),
+    sx, sz = spec["max_scale"]
+    out = {"workload": (f"{n_jobs} jobs, engine uniform over acoustic/elastic/viscoacoustic, grid 256x256.."
+                        f"{int(256 * sx)}x{int(256 * sz)} log-uniform at 5-10 m, nt {spec['nt_range'][0]}-"
+                        f"{spec['nt_range'][1]}, 1-{spec['max_shots']} shots, normalized, seeded noise records"),
+           "scale": scale,
            "shots": n_shots, "gcell_updates": cells / 1e9, "saturation": sat,
            "saturation_gcell_updates_per_s": cells / sat["wall_s"] / 1e9,
            "plain": plain_line, "served_over_plain": sat["shots_per_s"] / plain_line["shots_per_s"]}
-    for frac in (0.5, 0.8):
+    for frac in fractions:
         lam = frac * job_rate
         arrivals = np.cumsum(rng.exponential(1.0 / lam, len(jobs)))
         out[f"poisson_{int(frac * 100)}pct"] = {"lambda_jobs_per_s": lam, **run(list(arrivals))}
@@ -500,13 +566,69 @@ def adjacent_rows_run(wl, peak: float, cpu: bool) -> dict:
     return rows
 
 
+def uneven_run(n_shots: int) -> dict:
+    """A bounded sample of the uneven batch (the 256-shot configuration: 4
+    seeded models of 501×301 … 2401×1201, acoustic or elastic, nt 1500-6000,
+    10-30 Hz): its first n_shots shots migrated in lockstep ticks (memory
+    grouped) and one at a time through the plain path; images compared."""
+    import torch
+
+    from ertm_b200 import workloads
+    from ertm_b200.batch import DeviceShot, migrate_device_items
+    from ertm_b200.imaging import ShotMigrator
+    from ertm_b200.propagation import source_wavelet
+    wls = workloads.uneven_batch(seed=0, n_shots=256)[:n_shots]
+    items, plain_in, cells = [], [], 0
+    for wl in wls:
+        imager, solver = imager_for(wl)
+        shot = synthesize(wl, solver, wl.sources)[0]
+        names = list(wl.components)
+        rec = torch.from_numpy(np.stack([shot.components[n] for n in names])).cuda()
+        w = source_wavelet(wl.sources[0], wl.dt, wl.nt)
+        items.append(DeviceShot(ShotMigrator(imager, wl.model), wl.sources[0], wl.receivers, rec, names, w,
+                                tuple(wl.modes)))
+        plain_in.append(ShotMigrator(imager, wl.model))
+        cells += 3 * wl.nt * wl.cells
+    torch.cuda.synchronize()
+
+    def batched():
+        return migrate_device_items(items)
+
+    def plain():
+        return [pm.migrate_device(it.source, it.receivers, it.record, it.names, it.wavelet, modes=it.modes)
+                for pm, it in zip(plain_in, items)]
+
+    out = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        fn()                                   # warm-up: tables, division checks, plans
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        imgs = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"ms": ms, "shots_per_s": len(items) / (ms / 1e3), "gcell_updates_per_s": cells / (ms / 1e3) / 1e9,
+                     "images": imgs}
+    same = all(torch.equal(a, b) for a, b in zip(out["batched"].pop("images"), out["plain"].pop("images")))
+    kinds = {}
+    for wl in wls:
+        key = f"{wl.engine} {wl.model.grid.nx}x{wl.model.grid.nz}"
+        kinds[key] = kinds.get(key, 0) + 1
+    return {"workload": f"first {len(items)} of the 256 uneven shots (seeded): {kinds}, nt "
+                        f"{min(w.nt for w in wls)}-{max(w.nt for w in wls)}",
+            "gcell_updates": cells / 1e9, **out,
+            "batched_over_plain": out["batched"]["shots_per_s"] / out["plain"]["shots_per_s"],
+            "batched_equals_plain": bool(same)}
+
+
 def run_ours(args, dist: Dist) -> None:
     import ctypes as C
 
     import torch
 
     from ertm_b200 import _lib
-    from ertm_b200.batch import migrate_device_batch
+    from ertm_b200.batch import DeviceShot, migrate_device_items
     from ertm_b200.imaging import ShotMigrator
     from ertm_b200.parallel import ShotParallelMigrator, plan_shards, reduce_partial_sums, shot_cost
     from ertm_b200.propagation import source_wavelet
@@ -515,109 +637,117 @@ def run_ours(args, dist: Dist) -> None:
     dev = dist.local
     torch.cuda.set_device(dev)
     L = _lib.lib(dev)
-    wl = build_workload(args, dist.world)
+    wl = build_workload(args)
     imager, solver = imager_for(wl)
     g = wl.model.grid
-    n_total = len(wl.sources)
-    mine = plan_shards([shot_cost(g.nx, g.nz, wl.nt, wl.engine)] * n_total, dist.world)[dist.rank]
-    sources = [wl.sources[i] for i in mine]
-    shots = synthesize(wl, solver, sources)
+    n_job = len(wl.sources)
+    S = shots_per_step(args)
+    per_step = S * dist.world                       # shots of one step over all ranks
+    n_all = args.warmup + args.steps
+    plan = [step_shots(args, n_job, dist.world, dist.rank, k) for k in range(n_all)]
+    used = sorted({i for st in plan for i in st})
     names = list(wl.components)
-    rec_dev = [torch.from_numpy(np.stack([s.components[n] for n in names])).cuda() for s in shots]
-    wavelets = [source_wavelet(s, wl.dt, wl.nt) for s in sources]
     n_modes = len(wl.modes)
-    n_shots = len(sources)
     npix = g.nx * g.nz
+    # the shots' records from the GPU forward model (untimed set-up), kept on the device
+    recs = dict(zip(used, synthesize(wl, solver, [wl.sources[i] for i in used])))
+    rec_dev = {i: torch.from_numpy(np.stack([recs[i].components[n] for n in names])).cuda() for i in used}
+    wavelets = {i: source_wavelet(wl.sources[i], wl.dt, wl.nt) for i in used}
     plain_mig = ShotMigrator(imager, wl.model)                       # one propagator pair, reused
-    batch_migs = [ShotMigrator(imager, wl.model) for _ in range(n_shots)]  # one pair per shot
+    batch_migs = [ShotMigrator(imager, wl.model) for _ in range(S)]  # one pair per shot of a step
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
     partial = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float64, device="cuda")
 
     def stack(imgs, out):
-        """This rank's float64 partial stack, the job's one all-reduce, finish."""
+        """This rank's float64 partial stack, the step's one all-reduce, finish."""
         partial.zero_()
         for k in range(n_modes):
             ptrs = (C.c_void_p * len(imgs))(*[im[k].data_ptr() for im in imgs])
-            _lib.check(L.ertm_stack_partial(len(imgs), npix, C.cast(ptrs, C.c_void_p), int(n_total > 1),
+            _lib.check(L.ertm_stack_partial(len(imgs), npix, C.cast(ptrs, C.c_void_p), int(per_step > 1),
                                             partial[k].data_ptr(), None), "stack partial")
         if dist.world > 1:
             reduce_partial_sums(partial)
         for k in range(n_modes):
-            _lib.check(L.ertm_stack_finish(npix, partial[k].data_ptr(), n_total, out[k].data_ptr(), None),
+            _lib.check(L.ertm_stack_finish(npix, partial[k].data_ptr(), per_step, out[k].data_ptr(), None),
                        "stack finish")
         return out
 
     out_plain = torch.empty((n_modes, g.nz, g.nx), dtype=torch.float32, device="cuda")
     out_batch = torch.empty_like(out_plain)
 
-    def plain_job():
-        imgs = [plain_mig.migrate_device(src, wl.receivers, rec_dev[i], names, wavelets[i], modes=wl.modes)
-                for i, src in enumerate(sources)]
+    def plain_step(k):
+        imgs = [plain_mig.migrate_device(wl.sources[i], wl.receivers, rec_dev[i], names, wavelets[i],
+                                         modes=wl.modes) for i in plan[k]]
         return stack(imgs, out_plain)
 
-    def batch_job():
-        imgs = migrate_device_batch(imager, batch_migs, sources, [wl.receivers] * n_shots, rec_dev, names,
-                                    wavelets, modes=wl.modes)
-        return stack(imgs, out_batch)
+    def batch_step(k):
+        items = [DeviceShot(batch_migs[j], wl.sources[i], wl.receivers, rec_dev[i], names, wavelets[i],
+                            tuple(wl.modes)) for j, i in enumerate(plan[k])]
+        return stack(migrate_device_items(items), out_batch)
 
-    def timed(job, steps, profile: bool):
-        for _ in range(args.warmup):
-            job()
+    def timed(step, warm: list[int], steps: list[int], profile: bool):
+        for k in warm:
+            step(k)
         torch.cuda.synchronize()
         if profile:
             _lib.check(L.ertm_profile_stencil(1, 4), "profile")
         launches0 = L.ertm_launch_count()
-        times = []
+        times, first = [], None
         dist.barrier()
         torch.cuda.synchronize()
-        for _ in range(steps):
+        for k in steps:
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            job()
+            out = step(k)
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
+            if first is None:
+                first = out.clone()
         dist.barrier()
         torch.cuda.synchronize()
-        return times, int(L.ertm_launch_count() - launches0)
+        return times, int(L.ertm_launch_count() - launches0), first
 
-    # plain one-shot path (reported beside the batched form)
-    plain_times, _ = timed(plain_job, args.steps, False)
+    timed_steps = list(range(args.warmup, n_all))
+    # plain one-shot path (reported beside the batched form) on the first timed steps' shots
+    n_plain = max(1, min(args.plain_steps, args.steps))
+    plain_times, _, plain_first = timed(plain_step, [0], timed_steps[:n_plain], False)
     clocks = Clocks(dev)
     clocks.start()
-    times, launches = timed(batch_job, args.steps, True)
+    times, launches, batch_first = timed(batch_step, list(range(args.warmup)), timed_steps, True)
     clk = clocks.stop()
     tot, cnt, byt = C.c_double(), C.c_int64(), C.c_double()
     _lib.check(L.ertm_profile_read(C.byref(tot), C.byref(cnt), C.byref(byt)), "profile read")
     _lib.check(L.ertm_profile_stencil(0, 1), "profile off")
-    same = bool(torch.equal(out_plain, out_batch))
+    same = bool(torch.equal(plain_first, batch_first))
 
     total_ms = dist.max(float(sum(times)))
     plain_ms = dist.max(float(sum(plain_times)))
-    shots_total = n_total * args.steps
-    value = shots_total / (total_ms / 1e3)
-    plain_value = shots_total / (plain_ms / 1e3)
-    cell_updates = 3 * wl.nt * wl.cells * shots_total
+    value = per_step * args.steps / (total_ms / 1e3)
+    plain_value = per_step * n_plain / (plain_ms / 1e3)
+    cells_per_shot = 3 * wl.nt * wl.cells
 
-    # end to end through the public API: every rank is handed the whole job as
-    # host shot records (pinned), migrates its shard and gets the stacked host
-    # images back; host<->device copies are inside the timed region
-    pinned = [{n: torch.from_numpy(s.components[n]).pin_memory().numpy() for n in names} for s in shots]
-    host_shots = [None] * n_total
-    for j, i in enumerate(mine):
-        s = shots[j]
-        host_shots[i] = ShotRecord(data=pinned[j][names[0]], dt=s.dt, t=s.t, receivers=s.receivers, source=s.source,
-                                   components=pinned[j])
-    for i in range(n_total):        # other ranks' shots: only their shape enters the shard plan here
-        if host_shots[i] is None:
-            host_shots[i] = ShotRecord(data=np.zeros((wl.nt, wl.receivers.nrec), np.float32), dt=wl.dt,
-                                       t=np.arange(wl.nt) * wl.dt, receivers=wl.receivers, source=wl.sources[i],
-                                       components={n: np.zeros((wl.nt, wl.receivers.nrec), np.float32)
-                                                   for n in names})
+    # end to end through the public API: every rank is handed the step's
+    # shots as host records (pinned), migrates its shard and gets the stacked
+    # host images back; host<->device copies are inside the timed region
+    e2e_times, h2d, d2h = [], 0, 0
     spm = ShotParallelMigrator(imager, group=None)
-    e2e_times = []
-    for _ in range(args.e2e_steps):
+    for k in timed_steps[: max(0, args.e2e_steps)]:
+        glob = [(k * per_step + j) % n_job for j in range(per_step)]
+        costs = [shot_cost(g.nx, g.nz, wl.nt, wl.engine)] * per_step
+        mine = set(plan_shards(costs, dist.world)[dist.rank])
+        host_shots = []
+        for j, i in enumerate(glob):
+            if j in mine:
+                if i not in recs:
+                    recs[i] = synthesize(wl, solver, [wl.sources[i]])[0]
+                r = recs[i]
+                comps = {n: torch.from_numpy(r.components[n]).pin_memory().numpy() for n in names}
+            else:      # another rank's shot: only its shape enters the shard plan here
+                comps = {n: np.zeros((wl.nt, wl.receivers.nrec), np.float32) for n in names}
+            host_shots.append(ShotRecord(data=comps[names[0]], dt=wl.dt, t=np.arange(wl.nt) * wl.dt,
+                                         receivers=wl.receivers, source=wl.sources[i], components=comps))
         dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -627,17 +757,19 @@ def run_ours(args, dist: Dist) -> None:
         assert all(np.isfinite(r.image).all() for r in stacked)
     comp_bytes = len(names) * wl.nt * wl.receivers.nrec * 4
     model_bytes = 3 * npix * 4 * 2                      # vp, vs, rho per propagator, two propagators
-    # summed over the job's ranks: records, models and wavelets in; per-shot images and the stack out
-    # (accumulators are created, post-processed and stacked on the device)
-    h2d = n_total * (comp_bytes + model_bytes + wl.nt * 4)
-    d2h = n_total * n_modes * npix * 4 + dist.world * n_modes * npix * 4
+    # summed over the step's ranks: records, models and wavelets in; the stacked images out
+    # (per-shot accumulators are created, post-processed and stacked on the device)
+    h2d = per_step * (comp_bytes + model_bytes + wl.nt * 4)
+    d2h = dist.world * n_modes * npix * 4
     e2e_s = dist.max(statistics.mean(e2e_times)) if e2e_times else float("nan")
-    e2e_value = n_total / e2e_s
+    e2e_value = per_step / e2e_s
 
     tuned = L.ertm_autotune_report().decode().strip().splitlines()   # the batched job's shapes
+    uneven = uneven_run(args.uneven_shots) if dist.world == 1 and args.uneven_shots > 0 else None
     serving = None
     if dist.world == 1 and args.serve_jobs > 0:
-        serving = serving_run(args.serve_jobs)
+        fr = (0.5, 0.8) if args.serve_scale == "short" else (0.25, 0.5, 0.75, 1.0, 1.25)
+        serving = serving_run(args.serve_jobs, args.serve_scale, fr)
 
     peak, peak_kind = measured_hbm_peak()
     adjacent = None
@@ -647,35 +779,43 @@ def run_ours(args, dist: Dist) -> None:
     achieved = float(byt.value) / (float(tot.value) * 1e-3) / 1e9 if tot.value > 0 else 0.0
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        cs = cpu_sample(args.config, args.cpu_sample_steps)
-        cpu = {"value": 1.0 / cs["per_shot_s"], "unit": "shots/s", "cores": 1, "kind": "port",
-               "sample": (f"one shot, {cs['nt_sample']} of {cs['nt']} steps of the NumPy oracle migrate "
-                          f"({cs['sample_s']:.1f} s), extrapolated linearly in steps and x{cs['migrates_per_shot']} "
-                          f"for one migrate per imaging mode as the reference runs them")}
+        n2 = max(args.cpu_sample_steps, 8)
+        n1 = max(n2 // 3, 4)
+        est = per_shot_seconds([cpu_sample(args.config, n1, args.nt)], [cpu_sample(args.config, n2, args.nt)])
+        cpu = {"value": 1.0 / est["per_shot_s"], "unit": "shots/s", "cores": 1, "kind": "port",
+               "sample": (f"one shot of the workload, {n1} and {n2} of {est['nt']} steps of the NumPy oracle migrate "
+                          f"on one core; set-up ({est['setup_s']:.2f} s) and per-step cost "
+                          f"({est['per_step_s'] * 1e3:.0f} ms) separated from the two lengths, extrapolated to the "
+                          f"whole shot, x{est['migrates_per_shot']} for one migrate per imaging mode")}
+    traffic_ratio = committed_traffic(f"{wl.engine}_step")
     line = {
         "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded layered model with cavities and a fault; records from the GPU forward model",
+        "data": "synthetic: seeded layered model; records from the GPU forward model",
         "config": job_config(wl, args, dist.world),
-        "gcell_updates_per_s": cell_updates / (total_ms / 1e3) / 1e9,
-        "plain": {"value": plain_value, "unit": "shots/s", "ms_per_step": plain_ms / args.steps,
-                  "gcell_updates_per_s": cell_updates / (plain_ms / 1e3) / 1e9,
-                  "path": "one shot at a time, PP and PS from one pass"},
+        "gcell_updates_per_s": cells_per_shot * per_step * args.steps / (total_ms / 1e3) / 1e9,
+        "plain": {"value": plain_value, "unit": "shots/s", "ms_per_step": plain_ms / n_plain, "steps": n_plain,
+                  "gcell_updates_per_s": cells_per_shot * per_step * n_plain / (plain_ms / 1e3) / 1e9,
+                  "path": "one shot at a time, same kernels, same shots as the first timed batched steps"},
         "batched_over_plain": value / plain_value,
         "batched_equals_plain": same,
-        "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "steps": len(e2e_times), "path": "ShotParallelMigrator.migrate_job: host records in, stacked host "
+                                                 "images out, one step's shots per call"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (None if committed_traffic(f"{wl.engine}_step") is None else
-                                 committed_traffic(f"{wl.engine}_step") * float(byt.value) / max(int(cnt.value), 1)),
-                     "traffic_note": "DRAM bytes per tick: the ncu-measured DRAM/algorithmic ratio of a captured "
-                                     "16-step tick (profiles/) times this run's algorithmic bytes per tick",
+                     "traffic": (None if traffic_ratio is None else
+                                 traffic_ratio * float(byt.value) / max(int(cnt.value), 1)),
+                     "traffic_note": ("DRAM bytes per tick: the DRAM/algorithmic ratio ncu measured on a captured "
+                                      f"tick of this configuration (profiles/{wl.engine}_step.traffic) times this "
+                                      "run's algorithmic bytes per tick"),
                      "kernel": f"{wl.engine} velocity + stress launches of a batched tick (imaging epilogue fused)",
                      "bytes_definition": "per propagator step: Npad*(8*n_state + 4*n_coef) + 8*CPML strip cells*terms;"
                                          " per fused imaging epilogue: 16 B per accumulator, 4 B per replayed field",
                      "bytes_per_tick": float(byt.value) / max(int(cnt.value), 1), "tick_us": step_ms * 1e3,
                      "timed_ticks": int(cnt.value), "peak_source": peak_kind},
         "cpu_baseline": cpu,
+        "uneven": uneven,
         "serving": serving,
         "adjacent_rows": adjacent,
         "autotune": tuned,
@@ -689,6 +829,8 @@ def run_ours(args, dist: Dist) -> None:
 
 def main() -> None:
     args = parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args))
     # the reference arm is a CPU run on rank 0 alone: no process group, so the
     # other ranks exit at once instead of waiting for rank 0 in a collective
     dist = Dist(join=args.impl != "reference")

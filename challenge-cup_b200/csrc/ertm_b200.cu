@@ -200,12 +200,14 @@ struct LineFftPlan {
 std::map<std::pair<int, int>, std::unique_ptr<LineFftPlan>> g_line_plans;
 std::mutex g_line_mutex;
 
-constexpr int kLineThreads = 256;
 constexpr size_t kLineSmemMax = 227 * 1024;       // opt-in dynamic shared memory per CTA
+constexpr size_t kLineSmemWide = 113 * 1024;      // above this only one CTA fits an SM: use 512 threads
 constexpr int64_t kLineScratchCtas = 296;         // CTAs of a launch whose lines do not fit in shared memory
 
-void launch_lines(const FftPlanDev& plan, bool fwd, int load, const void* src, int64_t src_pitch, int64_t lines,
-                  double2* dst, double fct, double dz, double dx, double cutoff, cudaStream_t st) {
+// Launch the line transforms of J (J.plan, load, sources, lines set by the
+// caller): work buffers in shared memory when they fit, else per-CTA global
+// scratch; 512 threads for lines that leave one CTA per SM, 256 otherwise.
+void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
   static std::mutex attr_mutex;
   static std::map<int, bool> attr_set;
   {
@@ -213,37 +215,35 @@ void launch_lines(const FftPlanDev& plan, bool fwd, int load, const void* src, i
     CK(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lock(attr_mutex);
     if (!attr_set[dev]) {
-      CK(cudaFuncSetAttribute(k_fft_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLineSmemMax));
-      CK(cudaFuncSetAttribute(k_fft_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLineSmemMax));
+      const int m = (int)kLineSmemMax;
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
       attr_set[dev] = true;
     }
   }
-  LineJob J{};
-  J.plan = plan;
-  J.load = load;
-  J.lines = lines;
-  J.src = src;
-  J.src_pitch = src_pitch;
-  J.dst = dst;
-  J.fct = fct;
-  J.dz = dz;
-  J.dx = dx;
-  J.cutoff = cutoff;
-  const size_t smem = (size_t)2 * plan.n2 * sizeof(double2);
+  const size_t smem = (size_t)2 * J.plan.n2 * sizeof(double2);
   DevBuf scratch;
   unsigned grid;
   if (smem <= kLineSmemMax) {
     J.use_smem = 1;
-    grid = (unsigned)std::min<int64_t>(lines, 1 << 20);
+    grid = (unsigned)std::min<int64_t>(J.lines, 1 << 20);
   } else {
     J.use_smem = 0;
-    grid = (unsigned)std::min<int64_t>(lines, kLineScratchCtas);
+    grid = (unsigned)std::min<int64_t>(J.lines, kLineScratchCtas);
     scratch = DevBuf((size_t)grid * smem, st);
     J.scratch = scratch.as<double2>();
   }
   const size_t dyn = J.use_smem ? smem : 0;
-  if (fwd) k_fft_lines<true><<<grid, kLineThreads, dyn, st>>>(J);
-  else k_fft_lines<false><<<grid, kLineThreads, dyn, st>>>(J);
+  const bool wide = smem > kLineSmemWide;
+  if (fwd) {
+    if (wide) k_fft_lines<true, 512><<<grid, 512, dyn, st>>>(J);
+    else k_fft_lines<true, 256><<<grid, 256, dyn, st>>>(J);
+  } else {
+    if (wide) k_fft_lines<false, 512><<<grid, 512, dyn, st>>>(J);
+    else k_fft_lines<false, 256><<<grid, 256, dyn, st>>>(J);
+  }
   ++g_launches;
   CK(cudaGetLastError());
 }
@@ -288,7 +288,15 @@ const FftPlanDev& line_plan(int n, cudaStream_t st) {
     inner.blue = 0;
     DevBuf line(n2 * sizeof(double2), st);
     upload(line.p, kernel.data(), n2 * sizeof(double2), st);
-    launch_lines(inner, true, LINE_LOAD_C, line.p, (int64_t)n2, 1, line.as<double2>(), 1.0, 0.0, 0.0, 0.0, st);
+    LineJob J{};
+    J.plan = inner;
+    J.load = LINE_LOAD_C;
+    J.lines = 1;
+    J.seg_lines = 1;
+    J.nseg = 1;
+    J.cbuf[0] = line.as<double2>();
+    J.fct = 1.0;
+    launch_lines(J, true, st);
     std::vector<CxH> spec(n2), full(n2);
     CK(cudaMemcpyAsync(spec.data(), line.p, n2 * sizeof(double2), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -301,28 +309,69 @@ const FftPlanDev& line_plan(int n, cudaStream_t st) {
   return out;
 }
 
-// numerics.py:424-442 on an (nz, nx) array: Re(ifft2(fft2(a) · taper)), the
-// transforms along x then z as numpy.fft.fft2/ifft2 take them.  Input: real
-// float32 rows of pitch in_pitch (a padded field) or float64 (an image);
-// output likewise (float32 rounded to nearest).  A and B hold nz·nx complex
-// values each.  In place (out == in) is allowed.
-void lowpass2d(int nz, int nx, double dz, double dx, double cutoff, const void* in, bool in_f32, int64_t in_pitch,
-               void* out, bool out_f32, int64_t out_pitch, double2* A, double2* B, cudaStream_t st) {
+// numerics.py:424-442 on nseg arrays of shape (nz, nx): each becomes
+// Re(ifft2(fft2(a) · taper)), the transforms along x then z as
+// numpy.fft.fft2/ifft2 take them.  Inputs: real float32 rows of pitch
+// in_pitch (padded fields) or float64 (images); outputs likewise (float32
+// rounded to nearest); srcs[s] == dsts[s] is allowed.  All segments go
+// through the same launches; segment s works in A[s] and B[s], nz·nx complex
+// values each.
+void lowpass2d(int nz, int nx, double dz, double dx, double cutoff, int nseg, const void* const* srcs, bool in_f32,
+               int64_t in_pitch, void* const* dsts, bool out_f32, int64_t out_pitch, double2* const* A,
+               double2* const* B, cudaStream_t st) {
+  REQUIRE(nseg >= 1 && nseg <= kLineMaxSegs, "low-pass batch of 1.." + std::to_string(kLineMaxSegs) + " arrays");
   const FftPlanDev& px = line_plan(nx, st);
   const FftPlanDev& pz = line_plan(nz, st);
   const dim3 tb(32, 8);
-  auto tgrid = [](int rows, int cols) { return dim3((cols + 31) / 32, (rows + 31) / 32); };
-  launch_lines(px, true, in_f32 ? LINE_LOAD_F32 : LINE_LOAD_F64, in, in_pitch, nz, A, 1.0, 0, 0, 0, st);
-  k_transpose_lines<T_COMPLEX><<<tgrid(nz, nx), tb, 0, st>>>(A, nz, nx, B, 0);
-  launch_lines(pz, true, LINE_LOAD_C, B, nz, nx, B, 1.0, 0, 0, 0, st);
-  k_transpose_lines<T_COMPLEX><<<tgrid(nx, nz), tb, 0, st>>>(B, nx, nz, A, 0);
-  launch_lines(px, false, LINE_LOAD_C_TAPER, A, nx, nz, A, 1.0 / (double)nx, dz, dx, cutoff, st);
-  k_transpose_lines<T_COMPLEX><<<tgrid(nz, nx), tb, 0, st>>>(A, nz, nx, B, 0);
-  launch_lines(pz, false, LINE_LOAD_C, B, nz, nx, B, 1.0 / (double)nz, 0, 0, 0, st);
-  if (out_f32) k_transpose_lines<T_REAL_F32><<<tgrid(nx, nz), tb, 0, st>>>(B, nx, nz, out, out_pitch);
-  else k_transpose_lines<T_REAL_F64><<<tgrid(nx, nz), tb, 0, st>>>(B, nx, nz, out, out_pitch);
+  auto tgrid = [nseg](int rows, int cols) { return dim3((cols + 31) / 32, (rows + 31) / 32, nseg); };
+  auto job = [&](const FftPlanDev& p, int load, int seg_lines, double fct, double2* const* buf) {
+    LineJob J{};
+    J.plan = p;
+    J.load = load;
+    J.seg_lines = seg_lines;
+    J.nseg = nseg;
+    J.lines = (int64_t)nseg * seg_lines;
+    for (int k = 0; k < nseg; ++k) J.cbuf[k] = buf[k];
+    J.fct = fct;
+    J.dz = dz;
+    J.dx = dx;
+    J.cutoff = cutoff;
+    return J;
+  };
+  auto transpose = [&](double2* const* in, void* const* out) {
+    TransposeArgs T{};
+    for (int k = 0; k < nseg; ++k) {
+      T.in[k] = in[k];
+      T.out[k] = out[k];
+    }
+    return T;
+  };
+  void* const* Av = reinterpret_cast<void* const*>(A);
+  void* const* Bv = reinterpret_cast<void* const*>(B);
+  LineJob rows = job(px, in_f32 ? LINE_LOAD_F32 : LINE_LOAD_F64, nz, 1.0, A);
+  for (int k = 0; k < nseg; ++k) rows.src[k] = srcs[k];
+  rows.src_pitch = in_pitch;
+  launch_lines(rows, true, st);
+  k_transpose_lines<T_COMPLEX><<<tgrid(nz, nx), tb, 0, st>>>(transpose(A, Bv), nz, nx, 0);
+  launch_lines(job(pz, LINE_LOAD_C, nx, 1.0, B), true, st);
+  k_transpose_lines<T_COMPLEX><<<tgrid(nx, nz), tb, 0, st>>>(transpose(B, Av), nx, nz, 0);
+  launch_lines(job(px, LINE_LOAD_C_TAPER, nz, 1.0 / (double)nx, A), false, st);
+  k_transpose_lines<T_COMPLEX><<<tgrid(nz, nx), tb, 0, st>>>(transpose(A, Bv), nz, nx, 0);
+  launch_lines(job(pz, LINE_LOAD_C, nx, 1.0 / (double)nz, B), false, st);
+  if (out_f32) k_transpose_lines<T_REAL_F32><<<tgrid(nx, nz), tb, 0, st>>>(transpose(B, dsts), nx, nz, out_pitch);
+  else k_transpose_lines<T_REAL_F64><<<tgrid(nx, nz), tb, 0, st>>>(transpose(B, dsts), nx, nz, out_pitch);
   g_launches += 4;
   CK(cudaGetLastError());
+}
+
+// One array through lowpass2d.
+void lowpass2d_one(int nz, int nx, double dz, double dx, double cutoff, const void* in, bool in_f32, int64_t in_pitch,
+                   void* out, bool out_f32, int64_t out_pitch, double2* A, double2* B, cudaStream_t st) {
+  const void* srcs[1] = {in};
+  void* dsts[1] = {out};
+  double2* a[1] = {A};
+  double2* b[1] = {B};
+  lowpass2d(nz, nx, dz, dx, cutoff, 1, srcs, in_f32, in_pitch, dsts, out_f32, out_pitch, a, b, st);
 }
 
 int comp_offsets(int comp, double& xo, double& zo) {
@@ -967,16 +1016,46 @@ int tiles_for(const DevProp& h, int tz) { return ((h.nxp + TILE_X - 1) / TILE_X)
 template <int M>
 void launch_epilogue_M(const Prop& P, const Epilogue& E);
 
-// The wavenumber low-pass of a padded float32 field in place (the
-// compensated viscoacoustic stabilisation, propagation.py:744-749).
-void lowpass_field(Prop& P, float* f, double cutoff) {
-  const int nz = P.h.nzp, nx = P.h.nxp;
-  if (!P.lp_a.p) {
-    P.lp_a = DevBuf((size_t)nz * nx * sizeof(double2), P.st);
-    P.lp_b = DevBuf((size_t)nz * nx * sizeof(double2), P.st);
+// The compensated viscoacoustic low-pass (propagation.py:744-749): p and ε
+// of every propagator in `items`, in place, each with its cutoff at this
+// step.  Propagators of the same padded grid, spacing and cutoff share the
+// launches (two segments each); each keeps its own complex work arrays.
+struct LowpassItem {
+  Prop* P;
+  double cutoff;
+};
+
+void lowpass_props(const std::vector<LowpassItem>& items, cudaStream_t st) {
+  std::map<std::tuple<int, int, double, double, double>, std::vector<Prop*>> groups;
+  for (const LowpassItem& it : items)
+    groups[std::make_tuple(it.P->h.nzp, it.P->h.nxp, it.P->cfg.dz, it.P->cfg.dx, it.cutoff)].push_back(it.P);
+  for (auto& kv : groups) {
+    const int nz = std::get<0>(kv.first), nx = std::get<1>(kv.first);
+    const size_t cells = (size_t)nz * nx;
+    const std::vector<Prop*>& props = kv.second;
+    for (size_t c0 = 0; c0 < props.size(); c0 += kLineMaxSegs / 2) {
+      std::vector<const void*> srcs;
+      std::vector<void*> dsts;
+      std::vector<double2*> A, B;
+      for (size_t k = c0; k < std::min(props.size(), c0 + kLineMaxSegs / 2); ++k) {
+        Prop& P = *props[k];
+        if (!P.lp_a.p) {
+          P.lp_a = DevBuf(2 * cells * sizeof(double2), P.st);
+          P.lp_b = DevBuf(2 * cells * sizeof(double2), P.st);
+        }
+        const int fields[2] = {V_P, V_EPS};
+        for (int f = 0; f < 2; ++f) {
+          srcs.push_back(P.field(fields[f]));
+          dsts.push_back(P.field(fields[f]));
+          A.push_back(P.lp_a.as<double2>() + f * cells);
+          B.push_back(P.lp_b.as<double2>() + f * cells);
+        }
+      }
+      const Prop& P0 = *props[c0];
+      lowpass2d(nz, nx, P0.cfg.dz, P0.cfg.dx, std::get<4>(kv.first), (int)srcs.size(), srcs.data(), true, P0.h.ld,
+                dsts.data(), true, P0.h.ld, A.data(), B.data(), st);
+    }
   }
-  lowpass2d(nz, nx, P.cfg.dz, P.cfg.dx, cutoff, f, true, P.h.ld, f, true, P.h.ld, P.lp_a.as<double2>(),
-            P.lp_b.as<double2>(), P.st);
 }
 
 // Algorithmic HBM bytes of one propagator step: each state array read and
@@ -1045,7 +1124,10 @@ StepWork make_work(const Prop& P, double amp64, const float* wave, int t, const 
 // What follows the stress phase of a step: the force_z source on vz, the
 // compensated viscoacoustic amplitude cap / low-pass (propagation.py:726-749,
 // evaluated with the step index before its increment), and the increment.
-void after_step(Prop& P, double amp64, const float* wave, int t) {
+// With `defer`, a low-pass due at this step is appended there for the
+// caller to run (together with other propagators' low-passes) before
+// anything reads the fields again; otherwise it runs here.
+void after_step(Prop& P, double amp64, const float* wave, int t, std::vector<LowpassItem>* defer = nullptr) {
   const bool force_z = P.h.engine == ENGINE_ELASTIC && P.h.mech == MECH_FORCE_Z && P.h.src_iz >= 0;
   if (force_z && (wave || amp64 != 0.0)) {
     const int64_t idx = (int64_t)P.h.src_iz * P.h.ld + P.h.src_ix;
@@ -1065,8 +1147,8 @@ void after_step(Prop& P, double amp64, const float* wave, int t) {
         ++P.lowpass_steps;
         const double time = (double)s * P.cfg.dt;
         const double ratio = std::max(0.9 - 0.4 * std::min(time / 1.0, 1.0), 0.35);
-        lowpass_field(P, P.field(V_P), ratio);
-        lowpass_field(P, P.field(V_EPS), ratio);
+        if (defer) defer->push_back({&P, ratio});
+        else lowpass_props({{&P, ratio}}, P.st);
       }
     }
   }
@@ -1277,6 +1359,7 @@ struct ShotRun {
   bool excitation = false, kahan = false, want_ill = false, want_ril = false;
   bool need_src[2] = {false, false}, need_rcv_s = false;
   bool bwd_unfused = false, fwd_unfused = false;
+  int n_src = 1;               // source image fields stored per replayed step (P and/or S)
   DevBuf wave, rec, acc, ck, rbuf[2], running, peak;
   std::vector<int64_t> ck_step;
   InjectPlanHost* plan = nullptr;
@@ -1369,7 +1452,9 @@ void prepare_run(ShotRun& R, Prop& F, Prop& B, const ertm_migrate_config& cfg, c
   R.bwd_unfused = B.h.engine == ENGINE_VISCO && B.cfg.compensation;
   R.fwd_unfused = F.h.engine == ENGINE_ELASTIC && F.h.mech == MECH_FORCE_Z && cfg.separation == 1;
   if (!R.excitation) {
-    for (int k = 0; k < n_buffers; ++k) R.rbuf[k] = DevBuf((size_t)R.iv * 2 * npix * 4, st);
+    // only the source waves some image uses are stored: P, S or both per step
+    R.n_src = (R.need_src[0] ? 1 : 0) + (R.need_src[1] ? 1 : 0);
+    for (int k = 0; k < n_buffers; ++k) R.rbuf[k] = DevBuf((size_t)R.iv * R.n_src * npix * 4, st);
   } else {
     R.running = DevBuf(npix * 4, st);
     R.peak = DevBuf(npix * 4, st);
@@ -1400,11 +1485,11 @@ Epilogue replay_epilogue(const ShotRun& R, int b, int t) {
     e.step = t;
     return e;
   }
-  float* slot = R.rbuf[b & (R.rbuf[1].p ? 1 : 0)].as<float>() + (size_t)(t - R.s_of(b)) * 2 * R.npix;
+  float* slot = R.rbuf[b & (R.rbuf[1].p ? 1 : 0)].as<float>() + (size_t)(t - R.s_of(b)) * R.n_src * R.npix;
   e.kind = EPI_STORE;
   e.need_s = R.need_src[1] ? 1 : 0;
   e.out[0] = R.need_src[0] ? slot : nullptr;
-  e.out[1] = R.need_src[1] ? slot + R.npix : nullptr;
+  e.out[1] = R.need_src[1] ? slot + (R.need_src[0] ? R.npix : 0) : nullptr;
   return e;
 }
 
@@ -1418,13 +1503,13 @@ Epilogue backward_epilogue(const ShotRun& R, int b, int t) {
     e.step = t;
     return e;
   }
-  const float* slot = R.rbuf[b & (R.rbuf[1].p ? 1 : 0)].as<float>() + (size_t)(t - R.s_of(b)) * 2 * R.npix;
+  const float* slot = R.rbuf[b & (R.rbuf[1].p ? 1 : 0)].as<float>() + (size_t)(t - R.s_of(b)) * R.n_src * R.npix;
   e.kind = EPI_IMAGE;
   e.need_s = R.need_rcv_s ? 1 : 0;
   e.illum = R.want_ill ? 1 : 0;
   e.rillum = R.want_ril ? 1 : 0;
-  e.src[0] = slot;
-  e.src[1] = slot + R.npix;
+  e.src[0] = R.need_src[0] ? slot : nullptr;
+  e.src[1] = R.need_src[1] ? slot + (R.need_src[0] ? R.npix : 0) : nullptr;
   e.cross = t >= R.cfg.start_step ? 1 : 0;
   if (!e.cross && !e.illum && !e.rillum) e.kind = EPI_NONE;
   return e;
@@ -1835,11 +1920,18 @@ bool batch_tick(std::vector<ShotRun*>& runs, const DevProp* dt, cudaStream_t st)
   double bytes = 0.0;
   for (auto& g : groups) launch_group(g.second, dt, st, bytes);
   if (timed) g_prof.end(st, e0, bytes);
-  // after the stress phase: sources on vz, stabilisation, stand-alone epilogues, checkpoints
+  // after the stress phase: sources on vz, stabilisation (the tick's
+  // low-passes in shared launches), stand-alone epilogues, checkpoints
+  std::vector<LowpassItem> lowpasses;
   for (TickItem& it : items) {
     ShotRun& R = *it.run;
     Prop& P = it.fwd ? *R.F : *R.B;
-    after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t);
+    after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t, &lowpasses);
+  }
+  if (!lowpasses.empty()) lowpass_props(lowpasses, st);
+  for (TickItem& it : items) {
+    ShotRun& R = *it.run;
+    Prop& P = it.fwd ? *R.F : *R.B;
     if (it.unfused) launch_epilogue(P, it.epi);
     if (R.phase == 0 && R.t_f % R.iv == 0) save_checkpoint(R, R.t_f / R.iv, st);
   }
@@ -2630,7 +2722,8 @@ int32_t ertm_postprocess(int32_t nz, int32_t nx, double dx, double dz, const dou
     g_launches += 2 + (laplacian ? 1 : 0);
     if (lowpass < 1.0) {
       DevBuf wa((size_t)n * sizeof(double2), st), wb((size_t)n * sizeof(double2), st);
-      lowpass2d(nz, nx, dz, dx, lowpass, cur, false, nx, other, false, nx, wa.as<double2>(), wb.as<double2>(), st);
+      lowpass2d_one(nz, nx, dz, dx, lowpass, cur, false, nx, other, false, nx, wa.as<double2>(), wb.as<double2>(),
+                    st);
       std::swap(cur, other);
     }
     k_mask_cast<<<g2, b2, 0, st>>>(cur, o.as<float>(), nz, nx, npml, top_mask);
@@ -2650,7 +2743,7 @@ int32_t ertm_lowpass_wavenumber(int32_t nz, int32_t nx, double dx, double dz, do
     InArray a(in, n * 8, st);
     OutArray b(out, n * 8, st);
     DevBuf wa(n * sizeof(double2), st), wb(n * sizeof(double2), st);
-    lowpass2d(nz, nx, dz, dx, cutoff, a.as<double>(), false, nx, b.d, false, nx, wa.as<double2>(),
+    lowpass2d_one(nz, nx, dz, dx, cutoff, a.as<double>(), false, nx, b.d, false, nx, wa.as<double2>(),
               wb.as<double2>(), st);
     b.finish();
     CK(cudaStreamSynchronize(st));

@@ -405,41 +405,50 @@ __device__ __forceinline__ double lowpass_taper(int iz, int jx, int nz, int nx, 
 }
 
 enum LineLoad : int32_t {
-  LINE_LOAD_F32 = 0,    // real float32 lines, pitch `src_pitch` floats (a padded field)
-  LINE_LOAD_F64 = 1,    // real float64 lines, pitch `src_pitch` doubles (an image)
-  LINE_LOAD_C = 2,      // complex lines, pitch n
-  LINE_LOAD_C_TAPER = 3 // complex lines times the taper at (line, m) of a (lines, n) spectrum
+  LINE_LOAD_F32 = 0,    // real float32 lines, pitch `src_pitch` floats (a padded field), per segment
+  LINE_LOAD_F64 = 1,    // real float64 lines, pitch `src_pitch` doubles (an image), per segment
+  LINE_LOAD_C = 2,      // complex lines of the segment's work array, pitch n
+  LINE_LOAD_C_TAPER = 3 // the same times the taper at (row, m) of a (seg_lines, n) spectrum
 };
+
+// Several arrays of the same shape ("segments", e.g. p and ε of every
+// propagator that needs the low-pass at this step) go through one launch:
+// line l is row l % seg_lines of segment l / seg_lines; every segment has its
+// own real input and its own complex work array.
+constexpr int kLineMaxSegs = 64;
 
 struct LineJob {
   FftPlanDev plan;
   int32_t load;
   int32_t use_smem;      // 1: work buffers in dynamic shared memory, else in `scratch`
-  int64_t lines;
-  const void* src;
+  int64_t lines;         // nseg · seg_lines
+  int32_t seg_lines;
+  int32_t nseg;
+  const void* src[kLineMaxSegs];   // real loads: each segment's first row
   int64_t src_pitch;
-  double2* dst;          // complex lines, pitch n (may equal src for LINE_LOAD_C*)
+  double2* cbuf[kLineMaxSegs];     // complex lines of each segment, pitch n: the input of complex loads and
+                                   // the output of every transform (in place)
   double fct;            // output scale (1, or 1/n for an inverse transform)
   double2* scratch;      // 2·n2 values per CTA when not in shared memory
   double dz, dx, cutoff; // taper of LINE_LOAD_C_TAPER
 };
 
-__device__ __forceinline__ Cx line_load(const LineJob& J, int64_t line, int m) {
+__device__ __forceinline__ Cx line_load(const LineJob& J, int seg, int row, int m) {
   const int n = J.plan.n;
   switch (J.load) {
     case LINE_LOAD_F32:
-      return {(double)static_cast<const float*>(J.src)[line * J.src_pitch + m], 0.0};
+      return {(double)static_cast<const float*>(J.src[seg])[(int64_t)row * J.src_pitch + m], 0.0};
     case LINE_LOAD_F64:
-      return {static_cast<const double*>(J.src)[line * J.src_pitch + m], 0.0};
+      return {static_cast<const double*>(J.src[seg])[(int64_t)row * J.src_pitch + m], 0.0};
     case LINE_LOAD_C: {
-      const double2 v = static_cast<const double2*>(J.src)[line * (int64_t)n + m];
+      const double2 v = J.cbuf[seg][(int64_t)row * n + m];
       return {v.x, v.y};
     }
     default: {
       // spectrum × taper as NumPy multiplies complex128 by float64: the taper
       // is the complex (h, 0)
-      const double2 v = static_cast<const double2*>(J.src)[line * (int64_t)n + m];
-      const double h = lowpass_taper((int)line, m, (int)J.lines, n, J.dz, J.dx, J.cutoff);
+      const double2 v = J.cbuf[seg][(int64_t)row * n + m];
+      const double h = lowpass_taper(row, m, J.seg_lines, n, J.dz, J.dx, J.cutoff);
       return {dsub(dmul(v.x, h), dmul(v.y, 0.0)), dadd(dmul(v.x, 0.0), dmul(v.y, h))};
     }
   }
@@ -448,9 +457,11 @@ __device__ __forceinline__ Cx line_load(const LineJob& J, int64_t line, int m) {
 // One CTA per line (grid-stride over lines): load, transform, scale, store.
 // A Bluestein line is multiplied by the chirp, zero-padded to n2, convolved
 // with the kernel through a forward and a backward length-n2 transform and
-// multiplied by the chirp again (fftblue::fft of the library).
-template <bool FWD>
-__global__ void __launch_bounds__(256) k_fft_lines(const LineJob J) {
+// multiplied by the chirp again (fftblue::fft of the library).  THREADS 512
+// serves long lines (one CTA per SM by shared memory), 256 short ones (two
+// CTAs per SM by registers).
+template <bool FWD, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_fft_lines(const LineJob J) {
   extern __shared__ double2 line_smem[];
   const FftPlanDev& P = J.plan;
   const int n = P.n, n2 = P.n2;
@@ -458,24 +469,25 @@ __global__ void __launch_bounds__(256) k_fft_lines(const LineJob J) {
                      : reinterpret_cast<Cx*>(J.scratch) + (size_t)blockIdx.x * 2 * n2;
   Cx* b = a + n2;
   for (int64_t line = blockIdx.x; line < J.lines; line += gridDim.x) {
+    const int seg = (int)(line / J.seg_lines), row = (int)(line - (int64_t)seg * J.seg_lines);
     if (P.blue) {
-      for (int m = threadIdx.x; m < n2; m += blockDim.x)
-        a[m] = m < n ? cx_smul<FWD>(line_load(J, line, m), cx_ld(P.bk + m)) : Cx{0.0, 0.0};
+      for (int m = threadIdx.x; m < n2; m += THREADS)
+        a[m] = m < n ? cx_smul<FWD>(line_load(J, seg, row, m), cx_ld(P.bk + m)) : Cx{0.0, 0.0};
     } else {
-      for (int m = threadIdx.x; m < n; m += blockDim.x) a[m] = line_load(J, line, m);
+      for (int m = threadIdx.x; m < n; m += THREADS) a[m] = line_load(J, seg, row, m);
     }
     __syncthreads();
     Cx* r;
     if (P.blue) {
       r = fft_passes<true>(P, a, b);
-      for (int m = threadIdx.x; m < n2; m += blockDim.x) r[m] = cx_smul<!FWD>(r[m], cx_ld(P.bkf + m));
+      for (int m = threadIdx.x; m < n2; m += THREADS) r[m] = cx_smul<!FWD>(r[m], cx_ld(P.bkf + m));
       __syncthreads();
       r = fft_passes<false>(P, r, r == a ? b : a);
     } else {
       r = fft_passes<FWD>(P, a, b);
     }
-    double2* out = J.dst + line * (int64_t)n;
-    for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    double2* out = J.cbuf[seg] + (int64_t)row * n;
+    for (int m = threadIdx.x; m < n; m += THREADS) {
       Cx v = r[m];
       if (P.blue) v = cx_smul<FWD>(v, cx_ld(P.bk + m));
       v = cx_scale(v, J.fct);
@@ -486,17 +498,25 @@ __global__ void __launch_bounds__(256) k_fft_lines(const LineJob J) {
 }
 
 // ---------------------------------------------------------------------------
-// transposes between the two axes (32×32 tiles through shared memory)
+// transposes between the two axes (32×32 tiles through shared memory), one
+// segment per blockIdx.z: complex (rows × cols) → complex (cols × rows), or
+// the real part back into each segment's own real array
 // ---------------------------------------------------------------------------
 enum TransposeOut : int32_t {
-  T_COMPLEX = 0,    // out[c·rows + r] = in[r·cols + c]
-  T_REAL_F32 = 1,   // out[c·ld + r] = float32(real part): back into a padded field
-  T_REAL_F64 = 2    // out[c·ld + r] = real part: an image
+  T_COMPLEX = 0,    // out[z][c·rows + r] = in[z][r·cols + c]
+  T_REAL_F32 = 1,   // out[z][c·ld + r] = float32(real part): back into a padded field
+  T_REAL_F64 = 2    // out[z][c·ld + r] = real part: an image
+};
+
+struct TransposeArgs {
+  const double2* in[kLineMaxSegs];
+  void* out[kLineMaxSegs];
 };
 
 template <int MODE>
-__global__ void k_transpose_lines(const double2* __restrict__ in, int rows, int cols, void* out, int64_t ld) {
+__global__ void k_transpose_lines(const __grid_constant__ TransposeArgs T, int rows, int cols, int64_t ld) {
   __shared__ double2 tile[32][33];
+  const double2* in = T.in[blockIdx.z];
   const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
   for (int y = threadIdx.y; y < 32; y += blockDim.y) {
     const int r = r0 + y, c = c0 + threadIdx.x;
@@ -507,9 +527,9 @@ __global__ void k_transpose_lines(const double2* __restrict__ in, int rows, int 
     const int c = c0 + y, r = r0 + threadIdx.x;
     if (r < rows && c < cols) {
       const double2 v = tile[threadIdx.x][y];
-      if (MODE == T_COMPLEX) static_cast<double2*>(out)[(int64_t)c * rows + r] = v;
-      else if (MODE == T_REAL_F32) static_cast<float*>(out)[(int64_t)c * ld + r] = __double2float_rn(v.x);
-      else static_cast<double*>(out)[(int64_t)c * ld + r] = v.x;
+      if (MODE == T_COMPLEX) static_cast<double2*>(T.out[blockIdx.z])[(int64_t)c * rows + r] = v;
+      else if (MODE == T_REAL_F32) static_cast<float*>(T.out[blockIdx.z])[(int64_t)c * ld + r] = __double2float_rn(v.x);
+      else static_cast<double*>(T.out[blockIdx.z])[(int64_t)c * ld + r] = v.x;
     }
   }
 }

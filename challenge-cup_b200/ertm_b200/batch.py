@@ -40,8 +40,13 @@ class _Prepared:
     acc: Any = None
 
 
-def shot_device_bytes(mig: ShotMigrator, n_steps: int, n_images: int, n_buffers: int = 2) -> int:
-    """Device memory one shot of a batch holds while it runs."""
+def shot_device_bytes(mig: ShotMigrator, n_steps: int, n_images: int, n_buffers: int = 2,
+                      modes: tuple[str, ...] | None = None) -> int:
+    """Device memory one shot of a batch holds while it runs: two
+    propagators, the checkpoints, the replay buffers (one stored source field
+    per step and imaged source wave: P for pp/ps, S for sp/ss), the imaging
+    accumulators, and the complex work arrays of the compensated
+    viscoacoustic low-pass."""
     info = mig.prop.info()
     state = int(info.state_bytes)
     g = mig.model.grid
@@ -49,9 +54,14 @@ def shot_device_bytes(mig: ShotMigrator, n_steps: int, n_images: int, n_buffers:
     coef = 12 * info.nzp * info.ld * 4          # upper bound on the coefficient block
     interval = max(1, mig.interval_for(n_steps))
     n_states = (n_steps + interval - 1) // interval
-    replay = n_buffers * interval * 2 * npix * 4
+    n_src = 2 if modes is None else max(1, len({str(m).lower()[0] for m in modes}))
+    replay = n_buffers * interval * n_src * npix * 4
     acc = (2 * n_images + 2) * npix * 8
-    return 2 * (state + coef) + n_states * state + replay + acc
+    lowpass = 0
+    q = getattr(mig.back, "q_options", None)
+    if mig.engine == "viscoacoustic" and q is not None and q.compensation:
+        lowpass = 2 * 16 * info.nzp * info.nxp
+    return 2 * (state + coef) + n_states * state + replay + acc + lowpass
 
 
 class BatchMigrator:
@@ -94,7 +104,7 @@ class BatchMigrator:
                 raise ImagingError(f"invalid imaging input: {exc}") from exc
             mig = ShotMigrator(self.imager, model)
             w = None if wavelets is None else wavelets[k]
-            need = shot_device_bytes(mig, mig.spec.nt if w is None else len(w), len(modes))
+            need = shot_device_bytes(mig, mig.spec.nt if w is None else len(w), len(modes), modes=modes)
             if group and used + need > budget:
                 self._run(group, results)
                 group, used = [], 0
@@ -169,43 +179,93 @@ class BatchMigrator:
             results[k] = out
 
 
-def migrate_device_batch(imager: RTMImager, migrators: Sequence[ShotMigrator], sources: Sequence[Any],
-                         receivers: Sequence[Any], records: Sequence[Any], names: Sequence[str],
-                         wavelets: Sequence[np.ndarray], *, modes: tuple[str, ...] = ("pp",)):
-    """Device-resident batched form: one migrator (propagator pair) per shot,
-    built beforehand and reused; ``records[k]`` is a contiguous device tensor
-    (n_comp, nt, nrec) aligned to the propagation dt.  Returns a list of
-    device tensors (n_modes, nz, nx) float32 of final images."""
+@dataclass
+class DeviceShot:
+    """One shot of a device-resident batched call: its migrator (propagator
+    pair, built beforehand and reusable), source, receivers, record
+    (contiguous device tensor (n_comp, nt, nrec) at the propagation dt) with
+    its component names, wavelet and imaging modes."""
+    mig: ShotMigrator
+    source: Any
+    receivers: Any
+    record: Any
+    names: Sequence[str]
+    wavelet: np.ndarray
+    modes: tuple[str, ...] = ("pp",)
+
+
+def migrate_device_items(items: Sequence[DeviceShot], *, memory_budget: int | None = None):
+    """Device-resident batched form over shots that may differ in engine,
+    grid, length, components and modes.  Shots run in groups whose device
+    footprint fits the budget (default 80 % of free memory); each group is
+    one ``ertm_migrate_batch`` call.  Returns, per shot, a device tensor
+    (n_modes, nz, nx) float32 of its post-processed images."""
     import torch
 
-    n = len(migrators)
-    shots = (_lib.BatchShot * n)()
-    accs = []
-    for k, mig in enumerate(migrators):
-        w = np.ascontiguousarray(wavelets[k], dtype=np.float32)
-        pairs, store, start = mig._prepare(sources[k], receivers[k], modes, len(w))
-        cfg = mig._config(pairs, list(names), store, start, len(w))
-        g = mig.model.grid
-        acc = torch.empty((3, len(pairs), g.nz, g.nx), dtype=torch.float64, device=records[k].device)
-        accs.append((acc, w))
-        s = shots[k]
-        s.fwd, s.back, s.cfg = mig.prop.handle, mig.back.handle, cfg
-        s.wavelet = _lib.ptr(w)
-        s.record = _lib.ptr(records[k])
-        s.num, s.illum, s.rillum = _lib.ptr(acc[0]), _lib.ptr(acc[1]), _lib.ptr(acc[2])
-    _lib.check(_lib.lib().ertm_migrate_batch(n, shots), "migrate_batch")
-    out = []
-    for k, mig in enumerate(migrators):
-        mig.prop._psi_allocated = mig.back._psi_allocated = True
-        acc = accs[k][0]
-        g = mig.model.grid
-        imgs = torch.empty((len(modes), g.nz, g.nx), dtype=torch.float32, device=acc.device)
-        a = mig._post_args()
-        for j in range(len(modes)):
-            _lib.check(_lib.lib().ertm_postprocess(
-                g.nz, g.nx, float(a["dx"]), float(a["dz"]), _lib.ptr(acc[0, j]), _lib.ptr(acc[1, j]),
-                _lib.ptr(acc[2, j]), int(a["by_illum"]), int(a["by_rillum"]), a["eps"], int(a["laplacian"]),
-                a["lowpass_fraction"], int(a["npml"]), int(a["boundary"] == "cpml"), _lib.ptr(imgs[j]), None),
-                "postprocess")
-        out.append(imgs)
+    if memory_budget is None:
+        free, _ = torch.cuda.mem_get_info()
+        memory_budget = int(0.8 * free)
+    out: list = [None] * len(items)
+    group: list[int] = []
+    used = 0
+    for k, it in enumerate(items):
+        need = shot_device_bytes(it.mig, len(it.wavelet), len(it.modes), modes=tuple(it.modes))
+        if group and used + need > memory_budget:
+            _run_device_group(items, group, out)
+            group, used = [], 0
+        group.append(k)
+        used += need
+    if group:
+        _run_device_group(items, group, out)
     return out
+
+
+def _run_device_group(items: Sequence[DeviceShot], group: list[int], out: list) -> None:
+    import torch
+
+    shots = (_lib.BatchShot * len(group))()
+    accs = []
+    for j, k in enumerate(group):
+        it = items[k]
+        w = np.ascontiguousarray(it.wavelet, dtype=np.float32)
+        pairs, store, start = it.mig._prepare(it.source, it.receivers, tuple(it.modes), len(w))
+        cfg = it.mig._config(pairs, list(it.names), store, start, len(w))
+        g = it.mig.model.grid
+        acc = torch.empty((3, len(pairs), g.nz, g.nx), dtype=torch.float64, device=it.record.device)
+        accs.append((acc, w))
+        s = shots[j]
+        s.fwd, s.back, s.cfg = it.mig.prop.handle, it.mig.back.handle, cfg
+        s.wavelet = _lib.ptr(w)
+        s.record = _lib.ptr(it.record)
+        s.num, s.illum, s.rillum = _lib.ptr(acc[0]), _lib.ptr(acc[1]), _lib.ptr(acc[2])
+    _lib.check(_lib.lib().ertm_migrate_batch(len(group), shots), "migrate_batch")
+    for j, k in enumerate(group):
+        it = items[k]
+        mig = it.mig
+        mig.prop._psi_allocated = mig.back._psi_allocated = True
+        acc = accs[j][0]
+        g = mig.model.grid
+        imgs = torch.empty((len(it.modes), g.nz, g.nx), dtype=torch.float32, device=acc.device)
+        a = mig._post_args()
+        for m in range(len(it.modes)):
+            _lib.check(_lib.lib().ertm_postprocess(
+                g.nz, g.nx, float(a["dx"]), float(a["dz"]), _lib.ptr(acc[0, m]), _lib.ptr(acc[1, m]),
+                _lib.ptr(acc[2, m]), int(a["by_illum"]), int(a["by_rillum"]), a["eps"], int(a["laplacian"]),
+                a["lowpass_fraction"], int(a["npml"]), int(a["boundary"] == "cpml"), _lib.ptr(imgs[m]), None),
+                "postprocess")
+        out[k] = imgs
+
+
+def migrate_device_batch(imager: RTMImager, migrators: Sequence[ShotMigrator], sources: Sequence[Any],
+                         receivers: Sequence[Any], records: Sequence[Any], names: Sequence[str],
+                         wavelets: Sequence[np.ndarray], *, modes: tuple[str, ...] = ("pp",),
+                         memory_budget: int | None = None):
+    """Device-resident batched form for shots of one imaging setting: one
+    migrator (propagator pair) per shot, built beforehand and reused;
+    ``records[k]`` is a contiguous device tensor (n_comp, nt, nrec) aligned
+    to the propagation dt.  Returns a list of device tensors (n_modes, nz,
+    nx) float32 of final images."""
+    del imager   # the migrators carry the imaging settings
+    items = [DeviceShot(m, sources[k], receivers[k], records[k], names, wavelets[k], tuple(modes))
+             for k, m in enumerate(migrators)]
+    return migrate_device_items(items, memory_budget=memory_budget)

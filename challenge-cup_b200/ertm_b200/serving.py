@@ -83,7 +83,9 @@ def shot_footprint_bound(model: Any, imager: RTMImager, n_steps: int, n_modes: i
     every field, ψ term and coefficient taken at full padded size; checkpoints
     at the reference's interval (fields-only state bytes, imaging.py:121-124)
     times the full state; two replay buffers of interval·2·nz·nx floats; the
-    float64 accumulators; the record and the wavelet."""
+    float64 accumulators; the record and the wavelet; for a compensated
+    viscoacoustic backward pass, the two complex work arrays of its
+    wavenumber low-pass."""
     from .imaging import checkpoint_interval
     g = model.grid
     engine = imager.solver_config.engine
@@ -102,7 +104,9 @@ def shot_footprint_bound(model: Any, imager: RTMImager, n_steps: int, n_modes: i
     replay = 2 * iv * 2 * npix * 4
     acc = (2 * n_modes + 2) * npix * 8 + 3 * n_modes * npix * 8 + n_modes * npix * 4
     record = n_comp * n_steps * nrec * 4 + n_steps * 4
-    return int(2 * prop + n_states * state + replay + acc + record)
+    q = imager.q_config
+    lowpass = 2 * 16 * nzp * nxp if engine == "viscoacoustic" and q is not None and q.enabled else 0
+    return int(2 * prop + n_states * state + replay + acc + record + lowpass)
 
 
 def percentile(values, q: float) -> float | None:

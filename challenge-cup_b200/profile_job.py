@@ -1,16 +1,18 @@
-"""Profiling entry point: one benchmark workload's migration job, alone in
-the process, for ncu launch lists and kernel captures.
+"""Profiling tool (not part of the package): one benchmark workload's
+migration job, alone in the process, for ncu launch lists and kernel
+captures.
 
-    PYTHONPATH=challenge-cup_b200 python -m ertm_b200.profiling \\
-        [--config elastic4c] [--nt 48] [--shots 8] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--autotune 1] [--lane-assign 0] [--frame-rows 0] [--march 4] [--march-stress 0] [--tma 0] [--save x.npy]
+    python challenge-cup_b200/profile_job.py \\
+        [--config visco] [--nt 48] [--shots 4] [--path batched|plain] [--repeat 2] [--tile-rows 0] [--split 0] [--lanes 0] [--autotune 1] [--lane-assign 0] [--frame-rows 0] [--march 4] [--march-stress 0] [--tma 0] [--save x.npy]
 
-The job is what ``bench.py`` times: every shot of the workload migrated
+The job is a benchmark step: ``--shots`` shots of the workload migrated
 (batched lockstep ticks, or one shot at a time with ``--path plain``) and the
 images stacked.  Records come from the GPU forward model first.  Each repeat
 is preceded by a 256 MiB fill (the benchmark's L2 flush), which also marks the
-start of a repeat in a launch list.  Prints one JSON line: the launches of this
-library and the job time per repeat, and the stencil profiler's per-tick time
-and bytes over the last repeat.
+start of a repeat in a launch list; the last repeat runs inside the NVTX
+range ``job`` (``ncu --nvtx --nvtx-include job/`` captures it alone).  Prints
+one JSON line: the launches of this library and the job time per repeat, and
+the stencil profiler's per-tick time and bytes over the last repeat.
 """
 
 from __future__ import annotations
@@ -18,13 +20,17 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import sys
+from pathlib import Path
 
 import numpy as np
 
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+
 
 def main(argv=None) -> None:
-    ap = argparse.ArgumentParser(prog="python -m ertm_b200.profiling")
-    ap.add_argument("--config", default="elastic4c")
+    ap = argparse.ArgumentParser(prog="python challenge-cup_b200/profile_job.py")
+    ap.add_argument("--config", default="visco")
     ap.add_argument("--nt", type=int, default=48)
     ap.add_argument("--shots", type=int, default=None)
     ap.add_argument("--path", choices=("batched", "plain"), default="batched")
@@ -43,14 +49,20 @@ def main(argv=None) -> None:
                     help="two-lane ticks: 0 alternate works (replay | backward), 1 alternate shots")
     ap.add_argument("--tma", type=int, default=0, help="stage interior tiles with TMA (1) or cp.async (0)")
     ap.add_argument("--save", default=None, help="write the stacked images of the last repeat (.npy)")
+    ap.add_argument("--lowpass", default=None, metavar="NZxNX",
+                    help="time the wavenumber low-pass of one float64 NZxNX array instead of a job")
     args = ap.parse_args(argv)
 
     import torch
 
-    from . import _lib, workloads
-    from .batch import migrate_device_batch
-    from .imaging import ShotMigrator
-    from .propagation import source_wavelet
+    if args.lowpass:
+        lowpass_only(args)
+        return
+
+    from ertm_b200 import _lib, workloads
+    from ertm_b200.batch import migrate_device_batch
+    from ertm_b200.imaging import ShotMigrator
+    from ertm_b200.propagation import source_wavelet
 
     L = _lib.lib(0)
     _lib.check(L.ertm_set_tile_rows(args.tile_rows), "tile rows")
@@ -62,7 +74,9 @@ def main(argv=None) -> None:
     _lib.check(L.ertm_set_march(args.march), "march")
     _lib.check(L.ertm_set_march_stress(args.march_stress), "march stress")
     _lib.check(L.ertm_set_tma(args.tma), "tma")
-    wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt, **({"n_shots": args.shots} if args.shots else {}))
+    wl = workloads.WORKLOADS[args.config](seed=0, nt=args.nt)
+    if args.shots:
+        wl.sources = wl.sources[: args.shots]
     imager, solver = workloads.imager_for(wl)
     shots = workloads.synthesize(wl, solver, wl.sources)
     names = list(wl.components)
@@ -98,10 +112,15 @@ def main(argv=None) -> None:
         flush.fill_(1.0)
         before = L.ertm_launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        last = r == args.repeat - 1
+        if last:
+            torch.cuda.nvtx.range_push("job")
         e0.record()
         job()
         e1.record()
         torch.cuda.synchronize()
+        if last:
+            torch.cuda.nvtx.range_pop()
         job_ms.append(e0.elapsed_time(e1))
         launches.append(int(L.ertm_launch_count() - before))
     if args.save:
@@ -118,6 +137,33 @@ def main(argv=None) -> None:
                       "checksum": float(out.double().abs().sum().item()),
                       "stage_timeouts": int(L.ertm_stage_timeouts()),
                       "autotune": L.ertm_autotune_report().decode().strip().splitlines()}), flush=True)
+
+
+def lowpass_only(args) -> None:
+    """Repeated ertm_lowpass_wavenumber calls on a device array (the last
+    repeat inside the NVTX range ``job``); prints the time per call."""
+    import torch
+
+    from ertm_b200 import _lib
+    L = _lib.lib(0)
+    nz, nx = (int(v) for v in args.lowpass.lower().split("x"))
+    a = torch.randn(nz, nx, dtype=torch.float64, device="cuda")
+    b = torch.empty_like(a)
+    ms = []
+    for r in range(args.repeat):
+        last = r == args.repeat - 1
+        torch.cuda.synchronize()
+        if last:
+            torch.cuda.nvtx.range_push("job")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(L.ertm_lowpass_wavenumber(nz, nx, 5.0, 5.0, 0.5, a.data_ptr(), b.data_ptr(), None), "lowpass")
+        e1.record()
+        torch.cuda.synchronize()
+        if last:
+            torch.cuda.nvtx.range_pop()
+        ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"lowpass": [nz, nx], "ms_per_call": ms}), flush=True)
 
 
 if __name__ == "__main__":
