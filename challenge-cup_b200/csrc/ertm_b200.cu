@@ -216,10 +216,10 @@ void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
     std::lock_guard<std::mutex> lock(attr_mutex);
     if (!attr_set[dev]) {
       const int m = (int)kLineSmemMax;
-      CK(cudaFuncSetAttribute(k_fft_lines<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
-      CK(cudaFuncSetAttribute(k_fft_lines<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
-      CK(cudaFuncSetAttribute(k_fft_lines<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
-      CK(cudaFuncSetAttribute(k_fft_lines<false, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
       attr_set[dev] = true;
     }
   }
@@ -235,14 +235,16 @@ void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
     scratch = DevBuf((size_t)grid * smem, st);
     J.scratch = scratch.as<double2>();
   }
-  const size_t dyn = J.use_smem ? smem : 0;
   const bool wide = smem > kLineSmemWide;
-  if (fwd) {
-    if (wide) k_fft_lines<true, 512><<<grid, 512, dyn, st>>>(J);
-    else k_fft_lines<true, 256><<<grid, 256, dyn, st>>>(J);
+  if (!J.use_smem) {
+    if (fwd) k_fft_lines<true, 512, false><<<grid, 512, 0, st>>>(J);
+    else k_fft_lines<false, 512, false><<<grid, 512, 0, st>>>(J);
+  } else if (fwd) {
+    if (wide) k_fft_lines<true, 512, true><<<grid, 512, smem, st>>>(J);
+    else k_fft_lines<true, 256, true><<<grid, 256, smem, st>>>(J);
   } else {
-    if (wide) k_fft_lines<false, 512><<<grid, 512, dyn, st>>>(J);
-    else k_fft_lines<false, 256><<<grid, 256, dyn, st>>>(J);
+    if (wide) k_fft_lines<false, 512, true><<<grid, 512, smem, st>>>(J);
+    else k_fft_lines<false, 256, true><<<grid, 256, smem, st>>>(J);
   }
   ++g_launches;
   CK(cudaGetLastError());

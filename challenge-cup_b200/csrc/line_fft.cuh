@@ -77,7 +77,7 @@ struct Butterfly;
 
 template <bool FWD>
 struct Butterfly<FWD, 2> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     h[0] = cx_add(c[0], c[1]);
     h[1] = cx_sub(c[0], c[1]);
   }
@@ -85,7 +85,7 @@ struct Butterfly<FWD, 2> {
 
 template <bool FWD>
 struct Butterfly<FWD, 3> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double twr = -0.5, twi = (FWD ? -1.0 : 1.0) * kTw3;
     const Cx t0 = c[0], t1 = cx_add(c[1], c[2]), t2 = cx_sub(c[1], c[2]);
     h[0] = cx_add(t0, t1);
@@ -98,7 +98,7 @@ struct Butterfly<FWD, 3> {
 
 template <bool FWD>
 struct Butterfly<FWD, 4> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const Cx t2 = cx_add(c[0], c[2]), t1 = cx_sub(c[0], c[2]);
     const Cx t3 = cx_add(c[1], c[3]);
     const Cx t4 = cx_rot90<FWD>(cx_sub(c[1], c[3]));
@@ -111,7 +111,7 @@ struct Butterfly<FWD, 4> {
 
 template <bool FWD>
 struct Butterfly<FWD, 8> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     Cx a1 = cx_add(c[1], c[5]), a5 = cx_sub(c[1], c[5]);
     Cx a3 = cx_add(c[3], c[7]), a7 = cx_sub(c[3], c[7]);
     {
@@ -200,7 +200,7 @@ __device__ __forceinline__ void odd_prime(const Cx* c, Cx* h, const double* tr, 
 
 template <bool FWD>
 struct Butterfly<FWD, 5> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double tr[2] = {kTw5[0], kTw5[2]}, ti[2] = {kTw5[1], kTw5[3]};
     constexpr int xr[2][2] = {{1, 2}, {2, 1}};
     constexpr int ys[2][2] = {{1, 2}, {2, -1}};
@@ -210,7 +210,7 @@ struct Butterfly<FWD, 5> {
 
 template <bool FWD>
 struct Butterfly<FWD, 7> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double tr[3] = {kTw7[0], kTw7[2], kTw7[4]}, ti[3] = {kTw7[1], kTw7[3], kTw7[5]};
     constexpr int xr[3][3] = {{1, 2, 3}, {2, 3, 1}, {3, 1, 2}};
     constexpr int ys[3][3] = {{1, 2, 3}, {2, -3, -1}, {3, -1, 2}};
@@ -220,7 +220,7 @@ struct Butterfly<FWD, 7> {
 
 template <bool FWD>
 struct Butterfly<FWD, 11> {
-  __device__ static void run(const Cx* c, Cx* h) {
+  __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double tr[5] = {kTw11[0], kTw11[2], kTw11[4], kTw11[6], kTw11[8]};
     const double ti[5] = {kTw11[1], kTw11[3], kTw11[5], kTw11[7], kTw11[9]};
     constexpr int xr[5][5] = {{1, 2, 3, 4, 5}, {2, 4, 5, 3, 1}, {3, 5, 2, 1, 4}, {4, 3, 1, 5, 2}, {5, 1, 4, 2, 3}};
@@ -254,7 +254,7 @@ struct FftPlanDev {
 // ch[i + ido·(k + l1·j)], output j ≥ 1 of butterfly i ≥ 1 twiddled by
 // WA(j−1, i) = wa[i−1 + (j−1)·(ido−1)].
 template <bool FWD, int IP>
-__device__ void fft_pass(int ido, int l1, const Cx* cc, Cx* ch, const double2* wa) {
+__device__ __forceinline__ void fft_pass(int ido, int l1, const Cx* cc, Cx* ch, const double2* wa) {
   const int nb = l1 * ido;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int k = b / ido, i = b - k * ido;
@@ -277,7 +277,8 @@ __device__ void fft_pass(int ido, int l1, const Cx* cc, Cx* ch, const double2* w
 // differences CH, phase 2 the ip outputs in place of the input (CX), with
 // the library's loop order over l and j.  `wal` roots come from tws.
 template <bool FWD>
-__device__ void fft_pass_generic(int ido, int ip, int l1, Cx* cc, Cx* ch, const double2* wa, const double2* tws) {
+__device__ __forceinline__ void fft_pass_generic(int ido, int ip, int l1, Cx* cc, Cx* ch, const double2* wa,
+                                                 const double2* tws) {
   const int ipph = (ip + 1) / 2;
   const int idl1 = ido * l1;
   for (int ik = threadIdx.x; ik < idl1; ik += blockDim.x) {
@@ -354,7 +355,7 @@ __device__ void fft_pass_generic(int ido, int ip, int l1, Cx* cc, Cx* ch, const 
 // All passes of a Cooley-Tukey plan over a (in) with b as the other buffer;
 // returns the buffer that holds the result.  Callers synchronise before.
 template <bool FWD>
-__device__ Cx* fft_passes(const FftPlanDev& p, Cx* a, Cx* b) {
+__device__ __forceinline__ Cx* fft_passes(const FftPlanDev& p, Cx* a, Cx* b) {
   Cx* p1 = a;
   Cx* p2 = b;
   int l1 = 1;
@@ -459,14 +460,14 @@ __device__ __forceinline__ Cx line_load(const LineJob& J, int seg, int row, int 
 // with the kernel through a forward and a backward length-n2 transform and
 // multiplied by the chirp again (fftblue::fft of the library).  THREADS 512
 // serves long lines (one CTA per SM by shared memory), 256 short ones (two
-// CTAs per SM by registers).
-template <bool FWD, int THREADS>
+// CTAs per SM by registers).  SMEM: the two work buffers in dynamic shared
+// memory (shared loads and stores), else in per-CTA global scratch.
+template <bool FWD, int THREADS, bool SMEM>
 __global__ void __launch_bounds__(THREADS) k_fft_lines(const LineJob J) {
   extern __shared__ double2 line_smem[];
   const FftPlanDev& P = J.plan;
   const int n = P.n, n2 = P.n2;
-  Cx* a = J.use_smem ? reinterpret_cast<Cx*>(line_smem)
-                     : reinterpret_cast<Cx*>(J.scratch) + (size_t)blockIdx.x * 2 * n2;
+  Cx* a = SMEM ? reinterpret_cast<Cx*>(line_smem) : reinterpret_cast<Cx*>(J.scratch) + (size_t)blockIdx.x * 2 * n2;
   Cx* b = a + n2;
   for (int64_t line = blockIdx.x; line < J.lines; line += gridDim.x) {
     const int seg = (int)(line / J.seg_lines), row = (int)(line - (int64_t)seg * J.seg_lines);

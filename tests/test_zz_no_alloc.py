@@ -62,3 +62,45 @@ def test_stack_noalloc_rejects_host_pointers_and_too_many_images():
     many = (C.c_void_p * 1025)(*([dev[0].data_ptr()] * 1025))
     assert lib.ertm_stack_noalloc(1025, 16, C.cast(many, C.c_void_p), 1, out.data_ptr(), None) != 0
     assert "1024" in _lib.last_error()
+
+
+def test_stack_noalloc_single_image_is_a_copy():
+    """One image: both entry points return it unchanged (pipeline.py:140-141
+    returns a lone image as is), on two calls in a row."""
+    import torch
+
+    from ertm_b200 import _lib
+
+    lib = _lib.lib()
+    rng = np.random.default_rng(7)
+    for scale in (1.0, 50.0):
+        img = torch.from_numpy(rng.normal(scale=scale, size=(300, 211)).astype(np.float32)).cuda()
+        want = torch.empty_like(img)
+        got = torch.full_like(img, np.nan)
+        assert _stack(lib, "ertm_stack", [img], True, want) == 0, _lib.last_error()
+        assert _stack(lib, "ertm_stack_noalloc", [img], True, got) == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(got.cpu().numpy(), img.cpu().numpy())
+        assert np.array_equal(want.cpu().numpy(), img.cpu().numpy())
+
+
+def test_stack_noalloc_nan_image_left_undivided_like_the_reference():
+    """An image holding a NaN has max|image| = NaN in the reference
+    (np.max propagates it), so `scale > 0` fails and that image is added
+    undivided; the other images are still normalised."""
+    import torch
+
+    import oracle as orc
+    from ertm_b200 import _lib
+
+    lib = _lib.lib()
+    rng = np.random.default_rng(11)
+    host = [rng.normal(scale=3.0 * (k + 1), size=(130, 97)).astype(np.float32) for k in range(3)]
+    host[1][40, 50] = np.nan
+    want = orc.stack_images(host, normalize=True)
+    imgs = [torch.from_numpy(h).cuda() for h in host]
+    for fn in ("ertm_stack", "ertm_stack_noalloc", "ertm_stack_noalloc"):
+        got = torch.empty((130, 97), dtype=torch.float32, device="cuda")
+        assert _stack(lib, fn, imgs, True, got) == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(got.cpu().numpy(), want, equal_nan=True), fn
