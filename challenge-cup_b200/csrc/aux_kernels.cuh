@@ -271,6 +271,12 @@ __global__ void k_epilogue(const DevProp* props, int pi, Epilogue E) {
   run_epilogue(E, c, (size_t)P.nz * P.nx, pv, sv);
 }
 
+// Status words of every propagator of a launch table (one small copy back).
+__global__ void k_gather_status(const DevProp* table, int n, uint32_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = *table[i].status;
+}
+
 __global__ void k_kahan_to_f64(const float* s, const float* c, double* out, int64_t n) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) out[k] = (double)s[k] - (double)c[k];

@@ -422,7 +422,7 @@ struct Prop {
   int M = 4;
   int n_psi = 2;
   size_t field_elems = 0, state_floats = 0;
-  DevBuf state, coefs, prof, qidx, relax, peak, stab;
+  DevBuf state, coefs, prof, qidx, relax, peak, stab, status;
   int64_t step_index = 0;
   int tiles_x = 0, tiles = 0, tz = 32;
   int lowpass_steps = 0;
@@ -1268,6 +1268,9 @@ Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, cons
   P->peak = DevBuf(64, P->st);
   CK(cudaMemsetAsync(P->peak.p, 0, 64, P->st));
   h.peak = P->peak.as<float>();
+  P->status = DevBuf(sizeof(uint32_t), P->st);
+  CK(cudaMemsetAsync(P->status.p, 0, sizeof(uint32_t), P->st));
+  h.status = P->status.as<uint32_t>();
   P->stab = DevBuf(sizeof(StabState), P->st);
   CK(cudaMemsetAsync(P->stab.p, 0, sizeof(StabState), P->st));
   DevBuf tables;
@@ -1398,6 +1401,8 @@ void prepare_run(ShotRun& R, Prop& F, Prop& B, const ertm_migrate_config& cfg, c
     }
   R.F = &F;
   R.B = &B;
+  CK(cudaMemsetAsync(F.status.p, 0, sizeof(uint32_t), st));
+  CK(cudaMemsetAsync(B.status.p, 0, sizeof(uint32_t), st));
   R.cfg = cfg;
   R.nt = cfg.nt;
   R.iv = cfg.interval;
@@ -1552,6 +1557,22 @@ void inject_one(ShotRun& R, int t, cudaStream_t st) {
                                                             (int64_t)t * R.nrec);
 }
 
+// Status word of a propagator after the work queued on `st`.
+uint32_t read_status(const Prop& P, cudaStream_t st) {
+  uint32_t v = 0;
+  CK(cudaMemcpyAsync(&v, P.status.p, sizeof(v), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return v;
+}
+
+// The error of a run whose propagators flagged non-finite values.
+void require_finite(const ShotRun& R, cudaStream_t st, const std::string& what) {
+  const uint32_t f = read_status(*R.F, st), b = read_status(*R.B, st);
+  if ((f | b) & STATUS_NONFINITE)
+    throw Error(ERTM_ERR_NONFINITE, what + ": the " + std::string(f ? "source (forward/replay)" : "backward") +
+                                        " wavefield became non-finite (NaN or infinity)");
+}
+
 // Plain driver: one shot, steps one after the other (imaging.py:255-331).
 void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wavelet, const float* record,
              double* num_out, double* illum_out, double* rillum_out) {
@@ -1604,6 +1625,7 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
   }
   CK(cudaGetLastError());
   finish_run(R, st);
+  require_finite(R, st, "migrate");
 }
 
 // --------------------------------------------------------------------------
@@ -2005,6 +2027,14 @@ void migrate_batch(std::vector<ShotRun>& runs, cudaStream_t st) {
   while (batch_tick(ptrs, dtable.as<DevProp>(), st)) {
   }
   for (ShotRun& R : runs) finish_run(R, st);
+  std::string bad;
+  for (size_t k = 0; k < runs.size(); ++k) {
+    const uint32_t f = read_status(*runs[k].F, st), b = read_status(*runs[k].B, st);
+    if ((f | b) & STATUS_NONFINITE) bad += (bad.empty() ? "" : ", ") + std::to_string(k);
+  }
+  if (!bad.empty())
+    throw Error(ERTM_ERR_NONFINITE, "migrate_batch: the wavefields of shot(s) " + bad +
+                                        " became non-finite (NaN or infinity); the other shots' images are complete");
 }
 
 // --------------------------------------------------------------------------
@@ -2015,8 +2045,9 @@ struct Session {
   cudaStream_t st = nullptr;
   std::vector<std::unique_ptr<ShotRun>> runs;
   std::vector<int64_t> tags;
+  std::vector<int64_t> failed;   // tags of shots taken out for non-finite wavefields
   std::vector<DevProp> table;
-  DevBuf dtable;
+  DevBuf dtable, status;
   bool dirty = true;
   int64_t ticks = 0;
 };
@@ -2339,6 +2370,7 @@ int32_t ertm_prop_reset(void* prop) {
     Prop& P = *static_cast<Prop*>(prop);
     CK(cudaMemsetAsync(P.state.p, 0, P.state_floats * 4, P.st));
     CK(cudaMemsetAsync(P.stab.p, 0, sizeof(StabState), P.st));
+    CK(cudaMemsetAsync(P.status.p, 0, sizeof(uint32_t), P.st));
     P.step_index = 0;
     P.lowpass_steps = 0;
     CK(cudaStreamSynchronize(P.st));
@@ -2653,6 +2685,28 @@ int32_t ertm_session_advance(void* session, int32_t max_ticks, int64_t* done_tag
       if (!batch_tick(ptrs, S.dtable.as<DevProp>(), S.st)) break;
       ++S.ticks;
     }
+    // shots whose wavefields became non-finite leave the session; the others run on
+    const int n_tab = (int)S.table.size();
+    if (n_tab > 0) {
+      if (S.status.bytes < (size_t)n_tab * 4) S.status = DevBuf((size_t)n_tab * 4, S.st);
+      k_gather_status<<<(n_tab + 127) / 128, 128, 0, S.st>>>(S.dtable.as<DevProp>(), n_tab, S.status.as<uint32_t>());
+      ++g_launches;
+      std::vector<uint32_t> flags(n_tab);
+      CK(cudaMemcpyAsync(flags.data(), S.status.p, (size_t)n_tab * 4, cudaMemcpyDeviceToHost, S.st));
+      CK(cudaStreamSynchronize(S.st));
+      for (size_t i = 0; i < S.runs.size();) {
+        const ShotRun& R = *S.runs[i];
+        if (!((flags[R.fi] | flags[R.bi]) & STATUS_NONFINITE)) {
+          ++i;
+          continue;
+        }
+        release_streams(*S.runs[i], S.st);
+        S.failed.push_back(S.tags[i]);
+        S.runs.erase(S.runs.begin() + (std::ptrdiff_t)i);
+        S.tags.erase(S.tags.begin() + (std::ptrdiff_t)i);
+        S.dirty = true;
+      }
+    }
     for (size_t i = 0; i < S.runs.size() && *n_done < cap;) {
       if (S.runs[i]->phase != 4) {
         ++i;
@@ -2665,6 +2719,25 @@ int32_t ertm_session_advance(void* session, int32_t max_ticks, int64_t* done_tag
       S.tags.erase(S.tags.begin() + (std::ptrdiff_t)i);
       S.dirty = true;
     }
+  });
+}
+
+int32_t ertm_session_take_failed(void* session, int64_t* tags, int32_t cap, int32_t* n) {
+  return guarded([&] {
+    REQUIRE(session && n && cap >= 0 && (tags || cap == 0), "bad arguments");
+    Session& S = *static_cast<Session*>(session);
+    const int32_t k = (int32_t)std::min<size_t>((size_t)cap, S.failed.size());
+    for (int32_t i = 0; i < k; ++i) tags[i] = S.failed[i];
+    S.failed.erase(S.failed.begin(), S.failed.begin() + k);
+    *n = k;
+  });
+}
+
+int32_t ertm_prop_status(void* prop, uint32_t* status) {
+  return guarded([&] {
+    REQUIRE(prop && status, "bad arguments");
+    const Prop& P = *static_cast<Prop*>(prop);
+    *status = read_status(P, P.st);
   });
 }
 

@@ -71,7 +71,19 @@ struct DevProp {
   int32_t free_surface;               // 1: zero the free-surface row (acoustic/elastic)
   const void* tmap;                   // 9 tensor maps (tile heights 8/16/32 × halo/cell/coef) or null
   float* peak;                        // visco compensation: max|p| of the last step (float bits)
+  uint32_t* status;                   // STATUS_* bits, set by the stress phase (see nonfinite4)
 };
+
+// Status bits of a propagator.  The stress phase sets STATUS_NONFINITE when
+// it writes a NaN or an infinity (an unstable or overflowing run); hosts read
+// the word between steps and fail that run alone.
+constexpr uint32_t STATUS_NONFINITE = 1u;
+
+__device__ __forceinline__ bool nonfinite4(const float4& v) {
+  // NaN fails every comparison; |±inf| exceeds the largest finite float
+  return !(fabsf(v.x) <= 3.402823466e38f && fabsf(v.y) <= 3.402823466e38f && fabsf(v.z) <= 3.402823466e38f &&
+           fabsf(v.w) <= 3.402823466e38f);
+}
 
 // What the stress phase does with the finished fields of each physical cell
 // (fused so the image fields are never re-read from HBM).

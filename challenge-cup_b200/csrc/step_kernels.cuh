@@ -1121,6 +1121,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_c
         }
       }
       st4(p + g, out);
+      if (nonfinite4(out)) atomicOr(P.status, STATUS_NONFINITE);
       if constexpr (VISCO) st4(eps + g, epsv);
       if (w.epi.kind != EPI_NONE) st4(e_p + rr * 32 + 4 * threadIdx.x, out);
     }
@@ -1199,6 +1200,7 @@ k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_c
         }
       }
       st4(p + g, out);
+      if (nonfinite4(out)) atomicOr(P.status, STATUS_NONFINITE);
       if constexpr (VISCO) st4(eps + g, epsv);
       if (w.epi.kind != EPI_NONE) st4(e_p + rr * 32 + 4 * threadIdx.x, out);
     }
@@ -1322,6 +1324,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
       st4(sxx + g, oxx);
       st4(szz + g, ozz);
       st4(sxz + g, oxz);
+      if (nonfinite4(oxx) || nonfinite4(ozz) || nonfinite4(oxz)) atomicOr(P.status, STATUS_NONFINITE);
       if (epi) {
         float4 pv4, sv4;
 #pragma unroll
@@ -1431,6 +1434,7 @@ k_elastic_stress(const DevProp* __restrict__ props, const WS ws, const __grid_co
       st4(sxx + g, oxx);
       st4(szz + g, ozz);
       st4(sxz + g, oxz);
+      if (nonfinite4(oxx) || nonfinite4(ozz) || nonfinite4(oxz)) atomicOr(P.status, STATUS_NONFINITE);
       if (sz >= 0) {
         st4(psz2 + (size_t)sz * G.ld + j, q2.z);
         st4(psz3 + (size_t)sz * G.ld + j, q3.z);
@@ -1727,6 +1731,7 @@ k_elastic_stress_march(const DevProp* __restrict__ props, const WS ws) {
       st4(sxx + g, oxx);
       st4(szz + g, ozz);
       st4(sxz + g, oxz);
+      if (nonfinite4(oxx) || nonfinite4(ozz) || nonfinite4(oxz)) atomicOr(P.status, STATUS_NONFINITE);
       if (epi) {
         float4 pv4, sv4;
 #pragma unroll

@@ -14,7 +14,8 @@ __version__ = "0.1.0"
 from . import segy
 from .config import ImagingConfig, QConfig, SolverConfig
 from .data import NumpyDataStore
-from .exceptions import ConfigError, DataError, ERTMError, ImagingError, PipelineError, SolverError
+from .exceptions import (ConfigError, DataError, ERTMError, ImagingError, NonFiniteWavefieldError, PipelineError,
+                         SolverError)
 from .imaging import RTMImager, build_imager
 from .preprocess import prepare_shot
 from .propagation import (AcousticPropagator, ElasticPropagator, PropagationSpec, QOptions,
@@ -29,7 +30,7 @@ __all__ = [
     "AcousticPropagator", "ConfigError", "DataError", "ERTMError", "ElasticModel", "ElasticPropagator",
     "FiniteDifferenceSolver", "GridSpec", "ImageResult", "ImagingConfig", "ImagingError", "PipelineError",
     "PropagationSpec", "QConfig", "QOptions", "RTMImager", "ReceiverSpec", "ShotRecord", "SolverConfig",
-    "SolverError", "SourceSpec", "ViscoacousticPropagator", "build_imager", "build_propagator", "build_solver",
+    "NonFiniteWavefieldError", "SolverError", "SourceSpec", "ViscoacousticPropagator", "build_imager", "build_propagator", "build_solver",
     "check_stability", "forward_shot", "run_forward", "source_wavelet", "stack_images",
     "NumpyDataStore", "QCompensator", "attenuate_record", "build_compensator", "prepare_shot", "segy",
 ]

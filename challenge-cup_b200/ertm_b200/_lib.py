@@ -14,7 +14,7 @@ from pathlib import Path
 
 import numpy as np
 
-from .exceptions import SolverError
+from .exceptions import NonFiniteWavefieldError, SolverError
 
 # ERTM_B200_LIBRARY selects another build of the library (e.g. one compiled
 # with different tile options); the default is the in-tree build.
@@ -91,6 +91,7 @@ _SIGNATURES = {
     "ertm_prop_destroy": (None, [_P]),
     "ertm_prop_info_get": (_I32, [_P, C.POINTER(PropInfo)]),
     "ertm_prop_reset": (_I32, [_P]),
+    "ertm_prop_status": (_I32, [_P, _P]),
     "ertm_prop_set_source": (_I32, [_P, _I32, _I32, _I32]),
     "ertm_prop_set_receivers": (_I32, [_P, _I32, _P, _P]),
     "ertm_prop_step": (_I32, [_P, _I32, _P]),
@@ -124,6 +125,7 @@ _SIGNATURES = {
     "ertm_session_add": (_I32, [_P, C.POINTER(BatchShot), C.c_int64]),
     "ertm_session_advance": (_I32, [_P, _I32, C.POINTER(C.c_int64), _I32, C.POINTER(C.c_int32)]),
     "ertm_session_active": (_I32, [_P]),
+    "ertm_session_take_failed": (_I32, [_P, _P, _I32, _P]),
     "ertm_session_ticks": (C.c_int64, [_P]),
     "ertm_session_destroy": (_I32, [_P]),
     "ertm_stack_finish": (_I32, [C.c_int64, _P, C.c_int64, _P, _P]),
@@ -172,7 +174,13 @@ def last_error() -> str:
     return msg.decode() if msg else ""
 
 
+ERR_NONFINITE = -4
+STATUS_NONFINITE = 1
+
+
 def check(rc: int, what: str) -> None:
+    if rc == ERR_NONFINITE:
+        raise NonFiniteWavefieldError(f"{what} failed: {last_error()}")
     if rc != 0:
         raise SolverError(f"{what} failed: {last_error()}")
 

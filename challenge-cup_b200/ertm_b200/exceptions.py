@@ -42,6 +42,13 @@ class ImagingError(ERTMError):
     """Imaging input or condition failure."""
 
 
+class NonFiniteWavefieldError(SolverError):
+    """A wavefield became NaN or infinite during a run (an unstable or
+    overflowing propagation), detected on the device by the stress phase.
+    No counterpart in the reference, which finishes such a run with a
+    non-finite image."""
+
+
 class DataError(ERTMError):
     """Data format failure."""
 

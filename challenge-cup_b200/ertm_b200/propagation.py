@@ -15,6 +15,7 @@ sm_100a kernels.  Differences a caller can see:
 
 from __future__ import annotations
 
+import ctypes as C
 import weakref
 from dataclasses import dataclass
 from typing import Any
@@ -340,6 +341,18 @@ class Propagator2D:
         amp = np.array([float(source_amplitude)], dtype=np.float64)
         _lib.check(_lib.lib().ertm_prop_step(self._handle, 1, _lib.ptr(amp)), "step")
         self._psi_allocated = True
+
+    @property
+    def status(self) -> int:
+        """Device status bits after the queued steps (no reference counterpart):
+        bit 0 set once a step wrote NaN or infinity into a wavefield."""
+        out = C.c_uint32()
+        _lib.check(_lib.lib().ertm_prop_status(self._handle, C.byref(out)), "status")
+        return int(out.value)
+
+    @property
+    def finite(self) -> bool:
+        return not (self.status & _lib.STATUS_NONFINITE)
 
     def run(self, amplitudes: np.ndarray) -> None:
         """Advance len(amplitudes) steps in one call (no reference counterpart)."""

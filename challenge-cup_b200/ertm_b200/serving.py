@@ -38,7 +38,7 @@ from typing import Any, Callable
 import numpy as np
 
 from . import _lib
-from .exceptions import ImagingError
+from .exceptions import ImagingError, NonFiniteWavefieldError
 from .imaging import RTMImager, ShotMigrator
 from .types import ImageResult
 
@@ -253,6 +253,8 @@ class RTMServer:
         next_tag = 0
         done = (C.c_int64 * 64)()
         n_done = C.c_int32()
+        failed = (C.c_int64 * 64)()
+        n_failed = C.c_int32()
         t_start = None
         try:
             while True:
@@ -299,6 +301,16 @@ class RTMServer:
                     continue
                 _lib.check(L.ertm_session_advance(handle, self.ticks_per_poll, done, len(done), C.byref(n_done)),
                            "session advance")
+                # shots whose wavefields became non-finite left the session: their jobs fail, others run on
+                while True:
+                    _lib.check(L.ertm_session_take_failed(handle, failed, len(failed), C.byref(n_failed)),
+                               "session failed shots")
+                    for k in range(n_failed.value):
+                        slot = slots.pop(int(failed[k]))
+                        used -= slot.bytes
+                        self._shot_failed(slot)
+                    if n_failed.value < len(failed):
+                        break
                 for k in range(n_done.value):
                     slot = slots.pop(int(done[k]))
                     used -= slot.bytes
@@ -384,6 +396,17 @@ class RTMServer:
                 self._job_failed(js, exc)
         js.free.append(mig)
         self._maybe_finish(js)
+
+    def _shot_failed(self, slot: _Slot) -> None:
+        """A shot whose wavefield became non-finite on the device: its job
+        fails (once its other running shots have left the session); the
+        propagator pair is dropped rather than reused."""
+        js = slot.job
+        js.active -= 1
+        self.stats["shots_failed"] = self.stats.get("shots_failed", 0) + 1
+        self._job_failed(js, NonFiniteWavefieldError(
+            f"shot {slot.index} of job {js.job.name!r}: a wavefield became non-finite (NaN or infinity) on the "
+            f"device"))
 
     def _maybe_finish(self, js: _Job) -> None:
         if js.active or js.future.done():

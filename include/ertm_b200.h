@@ -30,6 +30,11 @@ extern "C" {
 #define ERTM_ERR_ARG (-1)
 #define ERTM_ERR_CUDA (-2)
 #define ERTM_ERR_STATE (-3)
+/* a wavefield became non-finite (NaN or infinity) during a run: an unstable
+ * or overflowing propagation; other shots of a batch are unaffected */
+#define ERTM_ERR_NONFINITE (-4)
+/* propagator status bits (ertm_prop_status) */
+#define ERTM_STATUS_NONFINITE 1u
 
 /* engines (propagation.py:986-1001) */
 #define ERTM_ENGINE_ACOUSTIC 0
@@ -187,8 +192,14 @@ void* ertm_prop_create(const ertm_prop_config* cfg, const float* vp, const float
                        const float* relax_a, void* stream);
 void ertm_prop_destroy(void* prop);
 int32_t ertm_prop_info_get(void* prop, ertm_prop_info* info);
-/* Propagator2D.reset (propagation.py:309-311, 423-428). */
+/* Propagator2D.reset (propagation.py:309-311, 423-428); clears the status word. */
 int32_t ertm_prop_reset(void* prop);
+/* Status word of a propagator (ERTM_STATUS_* bits), read after its queued
+ * work: the stress phase sets ERTM_STATUS_NONFINITE when it writes NaN or
+ * infinity.  No reference counterpart (the reference lets such a run finish
+ * with a non-finite image); the checks follow the finite-value contracts of
+ * types.py:106-122, 202-236 on the run's outputs. */
+int32_t ertm_prop_status(void* prop, uint32_t* status);
 /* Propagator2D.set_source (propagation.py:264-267): padded node and mechanism. */
 int32_t ertm_prop_set_source(void* prop, int32_t iz, int32_t ix, int32_t mechanism);
 /* Propagator2D.set_receivers (propagation.py:269-271): physical coordinates. */
@@ -260,6 +271,11 @@ int32_t ertm_session_advance(void* session, int32_t max_ticks, int64_t* done_tag
 int32_t ertm_session_active(void* session);
 int64_t ertm_session_ticks(void* session);
 int32_t ertm_session_destroy(void* session);
+/* Shots of a session whose wavefields became non-finite: each advance checks
+ * every active shot's propagators and takes such shots out of the session
+ * (their accumulators are not finished); this returns and forgets up to cap
+ * of their tags.  The other shots keep running. */
+int32_t ertm_session_take_failed(void* session, int64_t* tags, int32_t cap, int32_t* n);
 
 /* lowpass_wavenumber (numerics.py:424-442): out = Re(ifft2(fft2(in) · taper))
  * of an (nz, nx) float64 array, the radial taper 1 − (k − cutoff)/0.15
