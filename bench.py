@@ -57,6 +57,8 @@ def parse_args(argv=None) -> argparse.Namespace:
     ap.add_argument("--serve-scale", choices=("short", "full"), default="short",
                     help="short: grids up to 1024x512, nt 500-2000, 1-4 shots (seconds); full: the serving "
                          "configuration (grids up to 4096x2048, nt 1000-8000, 1-16 shots, minutes)")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="run only the serving stream (--serve-jobs, --serve-scale) and print its JSON")
     ap.add_argument("--uneven-shots", type=int, default=24,
                     help="shots of the uneven batch (256-shot configuration) timed batched vs plain (0: skip)")
     ap.add_argument("--no-adjacent", action="store_true",
@@ -835,7 +837,17 @@ def main() -> None:
     # other ranks exit at once instead of waiting for rank 0 in a collective
     dist = Dist(join=args.impl != "reference")
     try:
-        if args.impl == "reference":
+        if args.serving_only:
+            import torch
+            torch.cuda.set_device(dist.local)
+            fr = (0.5, 0.8) if args.serve_scale == "short" else (0.25, 0.5, 0.75, 1.0, 1.25)
+            clocks = Clocks(dist.local)
+            clocks.start()
+            out = serving_run(args.serve_jobs, args.serve_scale, fr)
+            out["clocks"] = clocks.stop()
+            if dist.rank == 0:
+                print(json.dumps({"serving": out}), flush=True)
+        elif args.impl == "reference":
             run_reference(args, dist)
         else:
             run_ours(args, dist)

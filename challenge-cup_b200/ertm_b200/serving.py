@@ -21,7 +21,10 @@ engine, grid and length on one device:
 A shot's image does not depend on what else runs in the session: each
 propagator performs the same steps in the same order as the one-shot path.
 A job whose shot fails to prepare (bad input, a mode the engine cannot image)
-fails alone; its shots already on the device run out and are dropped.
+fails alone; its shots already on the device run out and are dropped.  So
+does a job one of whose shots writes NaN or infinity into a wavefield on the
+device (an overflowing or unstable run): the session takes that shot out at
+the next poll and the job's future raises NonFiniteWavefieldError.
 """
 
 from __future__ import annotations
@@ -142,7 +145,7 @@ class _Slot:
 class RTMServer:
     """Request loop: ``submit`` jobs from any thread, read ``Future`` results."""
 
-    def __init__(self, *, device: int = 0, memory_budget: int | None = None, max_shots: int = 32,
+    def __init__(self, *, device: int = 0, memory_budget: int | None = None, max_shots: int = 64,
                  ticks_per_poll: int = 64, fault_hook: Callable[[str, int, int], None] | None = None) -> None:
         self.device = int(device)
         self.max_shots = int(max_shots)

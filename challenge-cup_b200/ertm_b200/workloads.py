@@ -198,9 +198,11 @@ def imager_for(wl: Workload):
 
 
 def synthesize(wl: Workload, solver, sources):
-    """Shot records of ``sources`` from the GPU forward model."""
+    """Shot records of ``sources`` from the GPU forward model (with the
+    workload's Q settings for the viscoacoustic engine)."""
+    from .config import QConfig
     from .solver import FiniteDifferenceSolver
-    fd = FiniteDifferenceSolver(solver)
+    fd = FiniteDifferenceSolver(solver, QConfig(**wl.q) if wl.q else None)
     return [fd.forward(wl.model, s, wl.receivers, components=wl.components) for s in sources]
 
 
@@ -259,3 +261,26 @@ def serving_jobs(seed: int = 0, n_jobs: int = 32, *, max_scale: tuple[float, flo
         jobs.append(ServeJob(shots=shots, model=model, imager=imager, modes=modes,
                              name=f"{engine} {nx}x{nz} nt={nt} shots={len(shots)}"))
     return jobs
+
+
+def serving_workload(index: int, seed: int = 1, *, max_scale: tuple[float, float] = (16.0, 8.0),
+                     nt_range: tuple[int, int] = (1000, 8000), max_shots: int = 16) -> Workload:
+    """Job ``index`` of the serving stream ``serving_jobs(seed, …)`` as a
+    workload (its model, sources, receivers, time axis and imaging settings;
+    records are then synthesised rather than the stream's noise)."""
+    job = serving_jobs(seed=seed, n_jobs=index + 1, max_scale=max_scale, nt_range=nt_range,
+                       max_shots=max_shots)[index]
+    solver = job.imager.solver_config
+    imaging = job.imager.config
+    q = job.imager.q_config
+    qd = {}
+    if solver.engine == "viscoacoustic":
+        qd = dict(enabled=True, model="gsls", alpha_c=q.alpha_c, f_ref=q.f_ref, gain_budget_db=q.gain_budget_db,
+                  f_max=q.f_max, amplitude_cap=q.amplitude_cap, lowpass_interval=q.lowpass_interval,
+                  n_mechanisms=q.n_mechanisms)
+    shot0 = job.shots[0]
+    comps = tuple(shot0.components) if shot0.components else ("p",)
+    return Workload(f"serving job {index}: {job.name}", solver.engine, job.model, [s.source for s in job.shots],
+                    shot0.receivers, float(solver.dt), int(solver.nt), solver.boundary, int(solver.npml),
+                    imaging.condition, separation=imaging.separation, modes=tuple(job.modes), components=comps,
+                    checkpoint_mb=float(imaging.checkpoint_mb), q=qd)

@@ -42,6 +42,9 @@ CASES = {
     "elastic4c": ([0, 5], 4, False, {}),
     "visco": ([10, 40], 8, False, {"checkpoint_mb": 2048.0}),
     "uneven": ([1, 4], 4, False, {}),
+    # a compensated viscoacoustic job of the serving stream (job 13 of the
+    # full-scale stream: 396x1378, nt 1586), its first shot
+    "serving": ([0], 4, False, {}),
 }
 
 
@@ -60,6 +63,9 @@ def case_workloads(config: str):
     if config == "uneven":
         batch = workloads.uneven_batch(0, 8)
         return [workloads.Workload(**{**batch[i].__dict__, **over}) for i in shots]
+    if config == "serving":
+        wl = workloads.serving_workload(13)
+        return [workloads.Workload(**{**wl.__dict__, "sources": [wl.sources[i]], **over}) for i in shots]
     wl = workloads.WORKLOADS[config](seed=0)
     return [workloads.Workload(**{**wl.__dict__, "sources": [wl.sources[i]], **over}) for i in shots]
 
