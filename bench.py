@@ -734,8 +734,9 @@ def run_ours(args, dist: Dist) -> None:
     # shots as host records (pinned), migrates its shard and gets the stacked
     # host images back; host<->device copies are inside the timed region
     e2e_times, h2d, d2h = [], 0, 0
-    spm = ShotParallelMigrator(imager, group=None)
-    for k in timed_steps[: max(0, args.e2e_steps)]:
+    spm = ShotParallelMigrator(imager, group=None)     # keeps its propagator pairs between calls
+    e2e_steps = timed_steps[: max(0, args.e2e_steps)]
+    for n_call, k in enumerate(e2e_steps[:1] + e2e_steps):   # the first call (untimed) builds the pairs
         glob = [(k * per_step + j) % n_job for j in range(per_step)]
         costs = [shot_cost(g.nx, g.nz, wl.nt, wl.engine)] * per_step
         mine = set(plan_shards(costs, dist.world)[dist.rank])
@@ -755,7 +756,8 @@ def run_ours(args, dist: Dist) -> None:
         t0 = time.perf_counter()
         stacked = spm.migrate_job(host_shots, wl.model, modes=wl.modes)
         torch.cuda.synchronize()
-        e2e_times.append(time.perf_counter() - t0)
+        if n_call:
+            e2e_times.append(time.perf_counter() - t0)
         assert all(np.isfinite(r.image).all() for r in stacked)
     comp_bytes = len(names) * wl.nt * wl.receivers.nrec * 4
     model_bytes = 3 * npix * 4 * 2                      # vp, vs, rho per propagator, two propagators
@@ -804,7 +806,8 @@ def run_ours(args, dist: Dist) -> None:
         "batched_equals_plain": same,
         "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "steps": len(e2e_times), "path": "ShotParallelMigrator.migrate_job: host records in, stacked host "
-                                                 "images out, one step's shots per call"},
+                                                 "images out, one step's shots per call; one untimed call before "
+                                                 "builds the propagator pairs the later calls reuse"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (None if traffic_ratio is None else
                                  traffic_ratio * float(byt.value) / max(int(cnt.value), 1)),

@@ -207,6 +207,10 @@ constexpr int64_t kLineScratchCtas = 296;         // CTAs of a launch whose line
 // Launch the line transforms of J (J.plan, load, sources, lines set by the
 // caller): work buffers in shared memory when they fit, else per-CTA global
 // scratch; 512 threads for lines that leave one CTA per SM, 256 otherwise.
+// Threads per CTA of the line transforms: 0 = chosen per transform length,
+// else forced (ertm_set_line_threads).  Results do not depend on it.
+std::atomic<int> g_line_threads{0};
+
 void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
   static std::mutex attr_mutex;
   static std::map<int, bool> attr_set;
@@ -236,15 +240,17 @@ void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
     J.scratch = scratch.as<double2>();
   }
   const bool wide = smem > kLineSmemWide;
+  const int forced = g_line_threads.load();
+  const int t = !J.use_smem ? 512 : forced > 0 ? forced : wide ? 512 : 256;
   if (!J.use_smem) {
-    if (fwd) k_fft_lines<true, 512, false><<<grid, 512, 0, st>>>(J);
-    else k_fft_lines<false, 512, false><<<grid, 512, 0, st>>>(J);
+    if (fwd) k_fft_lines<true, 512, false><<<grid, t, 0, st>>>(J);
+    else k_fft_lines<false, 512, false><<<grid, t, 0, st>>>(J);
   } else if (fwd) {
-    if (wide) k_fft_lines<true, 512, true><<<grid, 512, smem, st>>>(J);
-    else k_fft_lines<true, 256, true><<<grid, 256, smem, st>>>(J);
+    if (t > 256) k_fft_lines<true, 512, true><<<grid, t, smem, st>>>(J);
+    else k_fft_lines<true, 256, true><<<grid, t, smem, st>>>(J);
   } else {
-    if (wide) k_fft_lines<false, 512, true><<<grid, 512, smem, st>>>(J);
-    else k_fft_lines<false, 256, true><<<grid, 256, smem, st>>>(J);
+    if (t > 256) k_fft_lines<false, 512, true><<<grid, t, smem, st>>>(J);
+    else k_fft_lines<false, 256, true><<<grid, t, smem, st>>>(J);
   }
   ++g_launches;
   CK(cudaGetLastError());
@@ -2219,6 +2225,14 @@ int32_t ertm_set_march_stress(int32_t enable) {
   return guarded([&] {
     REQUIRE(enable == 0 || enable == 1, "march_stress must be 0 or 1");
     g_march_stress.store(enable);
+  });
+}
+
+int32_t ertm_set_line_threads(int32_t threads) {
+  return guarded([&] {
+    REQUIRE(threads == 0 || (threads >= 64 && threads <= 512 && threads % 32 == 0),
+            "threads must be 0 (automatic) or a multiple of 32 in [64, 512]");
+    g_line_threads = threads;
   });
 }
 

@@ -458,12 +458,12 @@ __device__ __forceinline__ Cx line_load(const LineJob& J, int seg, int row, int 
 // One CTA per line (grid-stride over lines): load, transform, scale, store.
 // A Bluestein line is multiplied by the chirp, zero-padded to n2, convolved
 // with the kernel through a forward and a backward length-n2 transform and
-// multiplied by the chirp again (fftblue::fft of the library).  THREADS 512
-// serves long lines (one CTA per SM by shared memory), 256 short ones (two
-// CTAs per SM by registers).  SMEM: the two work buffers in dynamic shared
+// multiplied by the chirp again (fftblue::fft of the library).  The launch
+// has at most MAXT threads; how many only sets how the butterflies of a pass
+// are spread over them.  SMEM: the two work buffers in dynamic shared
 // memory (shared loads and stores), else in per-CTA global scratch.
-template <bool FWD, int THREADS, bool SMEM>
-__global__ void __launch_bounds__(THREADS) k_fft_lines(const LineJob J) {
+template <bool FWD, int MAXT, bool SMEM>
+__global__ void __launch_bounds__(MAXT) k_fft_lines(const LineJob J) {
   extern __shared__ double2 line_smem[];
   const FftPlanDev& P = J.plan;
   const int n = P.n, n2 = P.n2;
@@ -472,23 +472,23 @@ __global__ void __launch_bounds__(THREADS) k_fft_lines(const LineJob J) {
   for (int64_t line = blockIdx.x; line < J.lines; line += gridDim.x) {
     const int seg = (int)(line / J.seg_lines), row = (int)(line - (int64_t)seg * J.seg_lines);
     if (P.blue) {
-      for (int m = threadIdx.x; m < n2; m += THREADS)
+      for (int m = threadIdx.x; m < n2; m += blockDim.x)
         a[m] = m < n ? cx_smul<FWD>(line_load(J, seg, row, m), cx_ld(P.bk + m)) : Cx{0.0, 0.0};
     } else {
-      for (int m = threadIdx.x; m < n; m += THREADS) a[m] = line_load(J, seg, row, m);
+      for (int m = threadIdx.x; m < n; m += blockDim.x) a[m] = line_load(J, seg, row, m);
     }
     __syncthreads();
     Cx* r;
     if (P.blue) {
       r = fft_passes<true>(P, a, b);
-      for (int m = threadIdx.x; m < n2; m += THREADS) r[m] = cx_smul<!FWD>(r[m], cx_ld(P.bkf + m));
+      for (int m = threadIdx.x; m < n2; m += blockDim.x) r[m] = cx_smul<!FWD>(r[m], cx_ld(P.bkf + m));
       __syncthreads();
       r = fft_passes<false>(P, r, r == a ? b : a);
     } else {
       r = fft_passes<FWD>(P, a, b);
     }
     double2* out = J.cbuf[seg] + (int64_t)row * n;
-    for (int m = threadIdx.x; m < n; m += THREADS) {
+    for (int m = threadIdx.x; m < n; m += blockDim.x) {
       Cx v = r[m];
       if (P.blue) v = cx_smul<FWD>(v, cx_ld(P.bk + m));
       v = cx_scale(v, J.fct);

@@ -78,6 +78,7 @@ _SIGNATURES = {
     "ertm_set_tick_lanes": (_I32, [_I32]),
     "ertm_set_lane_assign": (_I32, [_I32]),
     "ertm_set_frame_rows": (_I32, [_I32]),
+    "ertm_set_line_threads": (_I32, [_I32]),
     "ertm_set_march": (_I32, [_I32]),
     "ertm_set_march_stress": (_I32, [_I32]),
     "ertm_set_autotune": (_I32, [_I32]),

@@ -10,7 +10,10 @@ the plain path's image bit for bit.
 
 Shots are grouped so that a group's device memory (two propagators, the
 checkpoints, two replay buffers and the accumulators per shot) stays within a
-budget; groups run one after another.
+budget; groups run one after another.  A ``BatchMigrator`` keeps the
+propagator pairs it built for the models of its last call and resets them for
+the next group or call, so a stream of calls on one model builds the material
+tables, CPML profiles and device fields once.
 """
 
 from __future__ import annotations
@@ -22,7 +25,7 @@ import numpy as np
 
 from . import _lib
 from .exceptions import ImagingError
-from .imaging import RTMImager, ShotMigrator
+from .imaging import MigratorPool, RTMImager, ShotMigrator, pair_device_bytes
 from .types import ImageResult
 
 
@@ -51,7 +54,6 @@ def shot_device_bytes(mig: ShotMigrator, n_steps: int, n_images: int, n_buffers:
     state = int(info.state_bytes)
     g = mig.model.grid
     npix = g.nx * g.nz
-    coef = 12 * info.nzp * info.ld * 4          # upper bound on the coefficient block
     interval = max(1, mig.interval_for(n_steps))
     n_states = (n_steps + interval - 1) // interval
     n_src = 2 if modes is None else max(1, len({str(m).lower()[0] for m in modes}))
@@ -61,7 +63,7 @@ def shot_device_bytes(mig: ShotMigrator, n_steps: int, n_images: int, n_buffers:
     q = getattr(mig.back, "q_options", None)
     if mig.engine == "viscoacoustic" and q is not None and q.compensation:
         lowpass = 2 * 16 * info.nzp * info.nxp
-    return 2 * (state + coef) + n_states * state + replay + acc + lowpass
+    return pair_device_bytes(mig) + n_states * state + replay + acc + lowpass
 
 
 class BatchMigrator:
@@ -73,13 +75,21 @@ class BatchMigrator:
         # per shot of the last migrate_shots call: its post-processed images,
         # (n_modes, nz, nx) float32 on the device (the host images are copies)
         self.device_images: list = []
+        # propagator pairs of the last call's models, reused by the next
+        self._pool = MigratorPool(imager)
 
     def _budget(self) -> int:
         if self.memory_budget is not None:
             return int(self.memory_budget)
         import torch
         free, _ = torch.cuda.mem_get_info()
-        return int(0.8 * free)
+        # pooled pairs are reused, so the memory they hold is available to
+        # the group that takes them
+        return int(0.8 * (free + self._pool.held_bytes()))
+
+    def release(self) -> None:
+        """Drop the pooled propagator pairs (their device memory is freed)."""
+        self._pool.clear()
 
     def migrate_shots(self, shots: Sequence[Any], models: Any, *, modes: tuple[str, ...] | None = None,
                       wavelets: Sequence[np.ndarray] | None = None) -> list[list[ImageResult]]:
@@ -90,11 +100,9 @@ class BatchMigrator:
             raise ImagingError("one model per shot (or one model for all)")
         results: list[list[ImageResult] | None] = [None] * len(shots)
         self.device_images = [None] * len(shots)
-        group: list[tuple[int, _Prepared]] = []
-        used = 0
-        budget = self._budget()
+        self._pool.begin(model_list)
         checked: set[int] = set()
-        for k, (shot, model) in enumerate(zip(shots, model_list)):
+        for shot, model in zip(shots, model_list):
             try:
                 shot.validate()
                 if id(model) not in checked:        # one model often serves every shot
@@ -102,12 +110,18 @@ class BatchMigrator:
                     checked.add(id(model))
             except ValueError as exc:
                 raise ImagingError(f"invalid imaging input: {exc}") from exc
-            mig = ShotMigrator(self.imager, model)
+        group: list[tuple[int, _Prepared]] = []
+        taken: dict[int, int] = {}
+        used = 0
+        budget = self._budget()
+        for k, (shot, model) in enumerate(zip(shots, model_list)):
             w = None if wavelets is None else wavelets[k]
-            need = shot_device_bytes(mig, mig.spec.nt if w is None else len(w), len(modes), modes=modes)
+            sizer = self._pool.sizer(model)
+            need = shot_device_bytes(sizer, sizer.spec.nt if w is None else len(w), len(modes), modes=modes)
             if group and used + need > budget:
                 self._run(group, results)
-                group, used = [], 0
+                group, used, taken = [], 0, {}
+            mig = self._pool.take(model, taken)
             group.append((k, self._prepare(mig, shot, modes, w)))
             used += need
         if group:

@@ -10,6 +10,8 @@ PML mask run on the device as well (``ertm_postprocess``).
 
 from __future__ import annotations
 
+import threading
+import weakref
 from dataclasses import dataclass, field
 from typing import Any, Callable
 
@@ -143,6 +145,8 @@ class RTMImager:
             raise ImagingError(f"accumulation must be one of {sorted(_lib.ACCUM)}")
         self.accumulation = accumulation
         self._validate_engine_mode()
+        self._pool = MigratorPool(self)
+        self._pool_lock = threading.Lock()
 
     def q_options(self, *, compensation: bool = False) -> QOptions | None:
         """imaging.py:187-202."""
@@ -176,8 +180,21 @@ class RTMImager:
             model.validate()
         except ValueError as exc:
             raise ImagingError(f"invalid imaging input: {exc}") from exc
-        mig = ShotMigrator(self, model)
-        return mig.migrate(shot, wavelet=wavelet, preprocess=preprocess, modes=modes)
+        # the last model's propagator pair is kept for the next call; a call
+        # made while another thread migrates with this imager builds its own
+        if not self._pool_lock.acquire(blocking=False):
+            return ShotMigrator(self, model).migrate(shot, wavelet=wavelet, preprocess=preprocess, modes=modes)
+        try:
+            self._pool.begin([model])
+            mig = self._pool.take(model, {})
+            return mig.migrate(shot, wavelet=wavelet, preprocess=preprocess, modes=modes)
+        finally:
+            self._pool_lock.release()
+
+    def release(self) -> None:
+        """Free the propagator pair kept from the last call."""
+        with self._pool_lock:
+            self._pool.clear()
 
     def image_condition(self, source_wavefield: np.ndarray, receiver_wavefield: np.ndarray) -> np.ndarray:
         s, r = np.asarray(source_wavefield), np.asarray(receiver_wavefield)
@@ -425,6 +442,101 @@ class ShotMigrator:
                 a["lowpass_fraction"], int(a["npml"]), int(a["boundary"] == "cpml"), _lib.ptr(out[k]), stream),
                 "postprocess")
         return out
+
+
+def pair_device_bytes(mig: ShotMigrator) -> int:
+    """Device memory a migrator's two propagators hold between runs: state
+    fields and (an upper bound on) the coefficient block, twice."""
+    info = mig.prop.info()
+    return 2 * (int(info.state_bytes) + 12 * info.nzp * info.ld * 4)
+
+
+class MigratorPool:
+    """Propagator pairs kept between calls, per model object.
+
+    Building a ``ShotMigrator`` uploads the model, derives the CPML profiles
+    and (viscoacoustic) fits the relaxation tables; a stream of calls on one
+    model pays that once.  ``begin`` starts a call: it frees the pairs of
+    models the call does not use, pairs beyond the call's shot count of a
+    model, and pairs whose inputs changed since they were built (the imager's
+    solver or Q settings, the grid, or the material arrays changed in place).
+    ``take`` hands out a model's pairs in order within one group of shots
+    and builds another only when the group holds more shots of that model
+    than any group before."""
+
+    _FIELDS = ("vp", "vs", "rho", "qp", "qs")
+
+    def __init__(self, imager: "RTMImager") -> None:
+        # a weak reference: an imager that owns its pool is freed, with the
+        # pool's device memory, as soon as the last reference to it goes
+        self._imager = weakref.ref(imager)
+        # id(model) -> (model, the inputs its pairs were built from, pairs)
+        self._entries: dict[int, tuple[Any, tuple, list[ShotMigrator]]] = {}
+
+    @property
+    def imager(self) -> "RTMImager":
+        im = self._imager()
+        if im is None:
+            raise ImagingError("the imager of this migrator pool no longer exists")
+        return im
+
+    def _inputs(self, model: Any) -> tuple:
+        im = self.imager
+        g = model.grid
+        arrays = tuple(None if getattr(model, n, None) is None else np.array(getattr(model, n), copy=True)
+                       for n in self._FIELDS)
+        settings = (repr(im.solver_config), repr(im.q_options(compensation=False)),
+                    repr(im.q_options(compensation=True)),
+                    tuple(getattr(g, a, None) for a in ("nx", "nz", "dx", "dz", "x0", "z0")))
+        return settings, arrays
+
+    @staticmethod
+    def _same(a: tuple, b: tuple) -> bool:
+        if a[0] != b[0]:
+            return False
+        for x, y in zip(a[1], b[1]):
+            if (x is None) != (y is None):
+                return False
+            if x is not None and (x.shape != y.shape or not np.array_equal(x, y)):
+                return False
+        return True
+
+    def begin(self, models: list) -> None:
+        counts: dict[int, int] = {}
+        for m in models:
+            counts[id(m)] = counts.get(id(m), 0) + 1
+        for key in list(self._entries):
+            model, inputs, migs = self._entries[key]
+            # a live pooled model and a model of this call with the same id
+            # are the same object (the pool holds a reference to it)
+            if key not in counts or not self._same(inputs, self._inputs(model)):
+                del self._entries[key]
+            else:
+                del migs[counts[key]:]
+
+    def take(self, model: Any, taken: dict[int, int]) -> ShotMigrator:
+        key = id(model)
+        entry = self._entries.get(key)
+        if entry is None:
+            entry = self._entries[key] = (model, self._inputs(model), [])
+        k = taken.get(key, 0)
+        taken[key] = k + 1
+        if k == len(entry[2]):
+            entry[2].append(ShotMigrator(self.imager, model))
+        return entry[2][k]
+
+    def sizer(self, model: Any) -> ShotMigrator:
+        """A pair of ``model`` to size a shot with (every pair of a model has
+        the same footprint), built if the model has none yet; it is not
+        taken."""
+        return self.take(model, {})
+
+    def held_bytes(self) -> int:
+        return sum(pair_device_bytes(m) for _, _, migs in self._entries.values() for m in migs)
+
+    def clear(self) -> None:
+        """Drop every pair (their device memory is freed)."""
+        self._entries.clear()
 
 
 def build_imager(config: ImagingConfig, solver_config: SolverConfig | None = None,

@@ -133,6 +133,12 @@ class ShotParallelMigrator:
         self.normalize = bool(normalize)
         self._local = local or self._migrate_local
         self._finish = finish or _device_finish
+        self._batch = None      # one BatchMigrator across jobs: its propagator pairs are reused
+
+    def release(self) -> None:
+        """Free the propagator pairs kept from the last job."""
+        if self._batch is not None:
+            self._batch.release()
 
     def _migrate_local(self, shots, models, modes, wavelets, normalize: bool) -> ShardResult:
         from .batch import BatchMigrator
@@ -141,7 +147,9 @@ class ShotParallelMigrator:
             shape = (g.nz, g.nx) if g is not None else (0, 0)
             import torch
             return ShardResult(torch.zeros((len(modes),) + shape, dtype=torch.float64, device="cuda"), 0, [])
-        bm = BatchMigrator(self.imager, memory_budget=self.memory_budget)
+        if self._batch is None:
+            self._batch = BatchMigrator(self.imager, memory_budget=self.memory_budget)
+        bm = self._batch
         per_shot = bm.migrate_shots(shots, models, modes=modes, wavelets=wavelets)
         shape = per_shot[0][0].image.shape
         # the images are still on the device: stack them there

@@ -95,3 +95,44 @@ def test_batch_memory_grouping_gives_same_images():
     b = BatchMigrator(imager, memory_budget=1).migrate_shots(shots, model)
     for x, y in zip(a, b):
         assert np.array_equal(x[0].image, y[0].image)
+
+
+def test_pooled_pairs_give_fresh_results():
+    """A BatchMigrator and an RTMImager reuse their propagator pairs between
+    calls; the images equal those of freshly built pairs bit for bit, and a
+    model changed in place gets new pairs."""
+    from ertm_b200 import RTMImager
+    from ertm_b200.batch import BatchMigrator
+    fx, model, shots, imaging, solver, q = _inputs("mig_visco_comp")
+    imager = RTMImager(imaging, solver, q)
+    bm = BatchMigrator(imager)
+    first = bm.migrate_shots(shots, model)
+    pairs = list(bm._pool._entries[id(model)][2])
+    again = bm.migrate_shots(shots[::-1], model)
+    assert [p is q_ for p, q_ in zip(bm._pool._entries[id(model)][2], pairs)] == [True] * len(pairs)
+    for a, b in zip(first, again[::-1]):
+        assert np.array_equal(a[0].image, b[0].image)
+    # one pair serves every group when the budget forces one shot per group
+    small = BatchMigrator(imager, memory_budget=1)
+    one = small.migrate_shots(shots, model)
+    assert len(small._pool._entries[id(model)][2]) == 1
+    for a, b in zip(first, one):
+        assert np.array_equal(a[0].image, b[0].image)
+    # the imager's single-shot path keeps one pair for the next call
+    p1 = imager.migrate(shots[1], model)
+    kept = imager._pool._entries[id(model)][2][0]
+    p2 = imager.migrate(shots[1], model)
+    assert imager._pool._entries[id(model)][2][0] is kept
+    assert np.array_equal(p1.image, p2.image) and np.array_equal(p1.image, first[1][0].image)
+    # a model changed in place: new pairs, images of the changed model
+    vp0 = model.vp.copy()
+    try:
+        model.vp[model.vp.shape[0] // 2:, :] *= np.float32(0.97)     # slower: stays stable
+        changed = bm.migrate_shots(shots, model)
+        assert all(p is not q_ for p, q_ in zip(bm._pool._entries[id(model)][2], pairs))
+        fresh = BatchMigrator(RTMImager(imaging, solver, q)).migrate_shots(shots, model)
+        for a, b in zip(changed, fresh):
+            assert np.array_equal(a[0].image, b[0].image)
+        assert not np.array_equal(changed[0][0].image, first[0][0].image)
+    finally:
+        model.vp[...] = vp0

@@ -38,6 +38,37 @@ def test_lowpass_wavenumber_bit_exact(nz, nx):
         assert np.array_equal(got, want), (nz, nx, cutoff, float(np.max(np.abs(got - want))))
 
 
+# threads per CTA of the line transforms (0: the per-length choice); every
+# count must give the same bits
+LINE_THREADS = [64, 96, 128, 192, 288, 512]
+
+
+@pytest.mark.parametrize("threads", LINE_THREADS)
+def test_lowpass_bit_exact_for_every_thread_count(threads):
+    from ertm_b200 import _lib
+    from ertm_b200.numerics import lowpass_wavenumber
+    L = _lib.lib()
+    _lib.check(L.ertm_set_line_threads(threads), "line threads")
+    try:
+        for nz, nx in ((13, 169), (53, 71), (101, 97), (211, 311), (811, 2011), (2058, 4106)):
+            rng = np.random.default_rng(nz + 7 * nx)
+            field = rng.standard_normal((nz, nx))
+            got = lowpass_wavenumber(field, 5.0, 10.0, 0.55)
+            want = orc.lowpass_wavenumber(field, 5.0, 10.0, 0.55)
+            assert np.array_equal(got, want), (threads, nz, nx)
+    finally:
+        _lib.check(L.ertm_set_line_threads(0), "line threads")
+
+
+def test_line_threads_knob_rejects_bad_values():
+    from ertm_b200 import _lib
+    L = _lib.lib()
+    assert L.ertm_set_line_threads(100) != 0
+    assert L.ertm_set_line_threads(1024) != 0
+    assert L.ertm_set_line_threads(32) != 0
+    assert L.ertm_set_line_threads(0) == 0
+
+
 def test_lowpass_wavenumber_of_float32_field_device_resident():
     """A float32 field in place on the device (the compensated visco path's
     input form goes through the same transforms)."""

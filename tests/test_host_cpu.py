@@ -4,6 +4,7 @@ schedules and error behaviour (no kernel is launched here)."""
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import re
 from pathlib import Path
 
@@ -173,3 +174,52 @@ def test_serving_fails_loudly_without_a_device():
         fut.result(timeout=60)
     srv.stop(timeout=60)
     assert percentile([1.0, 2.0, 3.0, 4.0], 50) == 2.5 and percentile([], 99) is None
+
+
+def test_migrator_pool_reuses_and_rebuilds(monkeypatch):
+    """Pool bookkeeping with a stand-in migrator (no device): pairs are
+    handed out in order per group, reused by the next call, trimmed to the
+    call's shot count, dropped for models the call does not use, and rebuilt
+    when the material arrays or the solver settings change."""
+    from ertm_b200 import ImagingConfig, RTMImager, SolverConfig
+    from ertm_b200 import imaging
+    from ertm_b200.types import ElasticModel, GridSpec
+
+    built = []
+
+    class Stub:
+        def __init__(self, imager, model):
+            self.model = model
+            built.append(self)
+
+    monkeypatch.setattr(imaging, "ShotMigrator", Stub)
+    g = GridSpec(nx=8, nz=6, dx=5.0, dz=5.0)
+
+    def model(v):
+        a = np.full(g.shape, v, np.float32)
+        return ElasticModel(grid=g, vp=a, vs=a / 2, rho=a.copy(), qp=a.copy(), qs=a.copy())
+
+    imager = RTMImager(ImagingConfig(), SolverConfig(engine="acoustic"))
+    pool = imaging.MigratorPool(imager)
+    m1, m2 = model(2000.0), model(2500.0)
+    pool.begin([m1, m1, m2])
+    t: dict = {}
+    a = [pool.take(m1, t), pool.take(m1, t), pool.take(m2, t)]
+    assert len(built) == 3 and a[0] is not a[1]
+    t = {}                                        # the next group of the same call reuses them
+    assert pool.take(m1, t) is a[0] and pool.take(m1, t) is a[1] and len(built) == 3
+    pool.begin([m1])                              # next call: one shot of m1 -> m2 dropped, m1 trimmed to one
+    assert pool.take(m1, {}) is a[0] and len(built) == 3
+    assert list(pool._entries) == [id(m1)] and len(pool._entries[id(m1)][2]) == 1
+    m1.vp[2, 3] += 1.0                            # changed in place: stale
+    pool.begin([m1])
+    assert pool.take(m1, {}) is not a[0] and len(built) == 4
+    imager.solver_config = dataclasses.replace(imager.solver_config, order=4)   # new settings: stale
+    pool.begin([m1])
+    pool.take(m1, {})
+    assert len(built) == 5
+    pool.begin([m1])                              # unchanged: kept
+    pool.take(m1, {})
+    assert len(built) == 5
+    pool.clear()
+    assert pool._entries == {}
