@@ -201,6 +201,12 @@ std::map<std::pair<int, int>, std::unique_ptr<LineFftPlan>> g_line_plans;
 std::mutex g_line_mutex;
 
 constexpr size_t kLineSmemMax = 227 * 1024;       // opt-in dynamic shared memory per CTA
+#ifndef ERTM_LINE_NARROW_MIN_BLOCKS
+#define ERTM_LINE_NARROW_MIN_BLOCKS 3
+#endif
+// Resident CTAs per SM the 256-thread line transforms are compiled for (the
+// register cap follows: 3 → 80 registers, 2 → 128)
+constexpr int kLineNarrowMinBlocks = ERTM_LINE_NARROW_MIN_BLOCKS;
 constexpr size_t kLineSmemWide = 113 * 1024;      // above this only one CTA fits an SM: use 512 threads
 constexpr int64_t kLineScratchCtas = 296;         // CTAs of a launch whose lines do not fit in shared memory
 
@@ -220,10 +226,14 @@ void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
     std::lock_guard<std::mutex> lock(attr_mutex);
     if (!attr_set[dev]) {
       const int m = (int)kLineSmemMax;
-      CK(cudaFuncSetAttribute(k_fft_lines<true, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
-      CK(cudaFuncSetAttribute(k_fft_lines<false, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 256, true, kLineNarrowMinBlocks>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 256, true, kLineNarrowMinBlocks>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
       CK(cudaFuncSetAttribute(k_fft_lines<true, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
       CK(cudaFuncSetAttribute(k_fft_lines<false, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 768, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 768, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<true, 1024, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+      CK(cudaFuncSetAttribute(k_fft_lines<false, 1024, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
       attr_set[dev] = true;
     }
   }
@@ -246,11 +256,15 @@ void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
     if (fwd) k_fft_lines<true, 512, false><<<grid, t, 0, st>>>(J);
     else k_fft_lines<false, 512, false><<<grid, t, 0, st>>>(J);
   } else if (fwd) {
-    if (t > 256) k_fft_lines<true, 512, true><<<grid, t, smem, st>>>(J);
-    else k_fft_lines<true, 256, true><<<grid, t, smem, st>>>(J);
+    if (t > 768) k_fft_lines<true, 1024, true, 1><<<grid, t, smem, st>>>(J);
+    else if (t > 512) k_fft_lines<true, 768, true, 1><<<grid, t, smem, st>>>(J);
+    else if (t > 256) k_fft_lines<true, 512, true><<<grid, t, smem, st>>>(J);
+    else k_fft_lines<true, 256, true, kLineNarrowMinBlocks><<<grid, t, smem, st>>>(J);
   } else {
-    if (t > 256) k_fft_lines<false, 512, true><<<grid, t, smem, st>>>(J);
-    else k_fft_lines<false, 256, true><<<grid, t, smem, st>>>(J);
+    if (t > 768) k_fft_lines<false, 1024, true, 1><<<grid, t, smem, st>>>(J);
+    else if (t > 512) k_fft_lines<false, 768, true, 1><<<grid, t, smem, st>>>(J);
+    else if (t > 256) k_fft_lines<false, 512, true><<<grid, t, smem, st>>>(J);
+    else k_fft_lines<false, 256, true, kLineNarrowMinBlocks><<<grid, t, smem, st>>>(J);
   }
   ++g_launches;
   CK(cudaGetLastError());
@@ -2230,8 +2244,8 @@ int32_t ertm_set_march_stress(int32_t enable) {
 
 int32_t ertm_set_line_threads(int32_t threads) {
   return guarded([&] {
-    REQUIRE(threads == 0 || (threads >= 64 && threads <= 512 && threads % 32 == 0),
-            "threads must be 0 (automatic) or a multiple of 32 in [64, 512]");
+    REQUIRE(threads == 0 || (threads >= 64 && threads <= 1024 && threads % 32 == 0),
+            "threads must be 0 (automatic) or a multiple of 32 in [64, 1024]");
     g_line_threads = threads;
   });
 }

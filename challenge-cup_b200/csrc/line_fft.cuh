@@ -198,8 +198,71 @@ __device__ __forceinline__ void odd_prime(const Cx* c, Cx* h, const double* tr, 
   }
 }
 
+// The same butterfly handing each output to `out(j, value)` as soon as it is
+// formed, so that a pass can twiddle and store it at once instead of holding
+// all P outputs in registers.
+template <bool FWD, int P, int H, class Out>
+__device__ __forceinline__ void odd_prime_out(const Cx* c, const double* tr, const double* ti, const int (&xr)[H][H],
+                                          const int (&ys)[H][H], Out out) {
+  Cx tp[H + 1], tm[H + 1];
+#pragma unroll
+  for (int m = 1; m <= H; ++m) {
+    tp[m] = cx_add(c[m], c[P - m]);
+    tm[m] = cx_sub(c[m], c[P - m]);
+  }
+  double h0r = c[0].r, h0i = c[0].i;
+#pragma unroll
+  for (int m = 1; m <= H; ++m) {
+    h0r = dadd(h0r, tp[m].r);
+    h0i = dadd(h0i, tp[m].i);
+  }
+  const Cx c0 = c[0];
+  out(0, Cx{h0r, h0i});
+  const double sg = FWD ? -1.0 : 1.0;
+#pragma unroll
+  for (int u = 1; u <= H; ++u) {
+    double car = c0.r, cai = c0.i;
+#pragma unroll
+    for (int m = 1; m <= H; ++m) {
+      const double x = tr[xr[u - 1][m - 1] - 1];
+      car = dadd(car, dmul(x, tp[m].r));
+      cai = dadd(cai, dmul(x, tp[m].i));
+    }
+    double cbi = 0.0, cbr = 0.0;
+#pragma unroll
+    for (int m = 1; m <= H; ++m) {
+      const int s = ys[u - 1][m - 1];
+      const double y = sg * ti[(s < 0 ? -s : s) - 1];
+      const double pr = dmul(y, tm[m].r), pi = dmul(y, tm[m].i);
+      if (m == 1) {
+        cbi = pr;
+        cbr = pi;
+      } else if (s > 0) {
+        cbi = dadd(cbi, pr);
+        cbr = dadd(cbr, pi);
+      } else {
+        cbi = dsub(cbi, pr);
+        cbr = dsub(cbr, pi);
+      }
+    }
+    const Cx ca{car, cai}, cb{-cbr, cbi};
+    out(u, cx_add(ca, cb));
+    out(P - u, cx_sub(ca, cb));
+  }
+}
+
+// run() fills h with the P outputs; run_out() hands each one to `out` as
+// it is formed.  The constants are local arrays indexed by compile-time
+// indices only, so they fold into immediates.
 template <bool FWD>
 struct Butterfly<FWD, 5> {
+  template <class Out>
+  __device__ __forceinline__ static void run_out(const Cx* c, Out out) {
+    const double tr[2] = {kTw5[0], kTw5[2]}, ti[2] = {kTw5[1], kTw5[3]};
+    constexpr int xr[2][2] = {{1, 2}, {2, 1}};
+    constexpr int ys[2][2] = {{1, 2}, {2, -1}};
+    odd_prime_out<FWD, 5, 2>(c, tr, ti, xr, ys, out);
+  }
   __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double tr[2] = {kTw5[0], kTw5[2]}, ti[2] = {kTw5[1], kTw5[3]};
     constexpr int xr[2][2] = {{1, 2}, {2, 1}};
@@ -210,6 +273,13 @@ struct Butterfly<FWD, 5> {
 
 template <bool FWD>
 struct Butterfly<FWD, 7> {
+  template <class Out>
+  __device__ __forceinline__ static void run_out(const Cx* c, Out out) {
+    const double tr[3] = {kTw7[0], kTw7[2], kTw7[4]}, ti[3] = {kTw7[1], kTw7[3], kTw7[5]};
+    constexpr int xr[3][3] = {{1, 2, 3}, {2, 3, 1}, {3, 1, 2}};
+    constexpr int ys[3][3] = {{1, 2, 3}, {2, -3, -1}, {3, -1, 2}};
+    odd_prime_out<FWD, 7, 3>(c, tr, ti, xr, ys, out);
+  }
   __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double tr[3] = {kTw7[0], kTw7[2], kTw7[4]}, ti[3] = {kTw7[1], kTw7[3], kTw7[5]};
     constexpr int xr[3][3] = {{1, 2, 3}, {2, 3, 1}, {3, 1, 2}};
@@ -220,6 +290,15 @@ struct Butterfly<FWD, 7> {
 
 template <bool FWD>
 struct Butterfly<FWD, 11> {
+  template <class Out>
+  __device__ __forceinline__ static void run_out(const Cx* c, Out out) {
+    const double tr[5] = {kTw11[0], kTw11[2], kTw11[4], kTw11[6], kTw11[8]};
+    const double ti[5] = {kTw11[1], kTw11[3], kTw11[5], kTw11[7], kTw11[9]};
+    constexpr int xr[5][5] = {{1, 2, 3, 4, 5}, {2, 4, 5, 3, 1}, {3, 5, 2, 1, 4}, {4, 3, 1, 5, 2}, {5, 1, 4, 2, 3}};
+    constexpr int ys[5][5] = {{1, 2, 3, 4, 5}, {2, 4, -5, -3, -1}, {3, -5, -2, 1, 4}, {4, -3, 1, 5, -2},
+                              {5, -1, 4, -2, 3}};
+    odd_prime_out<FWD, 11, 5>(c, tr, ti, xr, ys, out);
+  }
   __device__ __forceinline__ static void run(const Cx* c, Cx* h) {
     const double tr[5] = {kTw11[0], kTw11[2], kTw11[4], kTw11[6], kTw11[8]};
     const double ti[5] = {kTw11[1], kTw11[3], kTw11[5], kTw11[7], kTw11[9]};
@@ -253,21 +332,31 @@ struct FftPlanDev {
 // A fixed-radix pass: CC(i, j, k) = cc[i + ido·(j + IP·k)] → CH(i, k, j) =
 // ch[i + ido·(k + l1·j)], output j ≥ 1 of butterfly i ≥ 1 twiddled by
 // WA(j−1, i) = wa[i−1 + (j−1)·(ido−1)].
-template <bool FWD, int IP>
+template <bool FWD, int IP, bool EAGER>
 __device__ __forceinline__ void fft_pass(int ido, int l1, const Cx* cc, Cx* ch, const double2* wa) {
   const int nb = l1 * ido;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int k = b / ido, i = b - k * ido;
-    Cx c[IP], h[IP];
+    Cx c[IP];
 #pragma unroll
     for (int j = 0; j < IP; ++j) c[j] = cc[i + ido * (j + IP * k)];
-    Butterfly<FWD, IP>::run(c, h);
-    ch[i + ido * k] = h[0];
+    if constexpr (EAGER && (IP == 5 || IP == 7 || IP == 11)) {
+      // odd primes: each output twiddled and stored as soon as it is formed
+      // (fewer live registers where the launch caps them)
+      Butterfly<FWD, IP>::run_out(c, [&](int j, Cx v) {
+        if (j > 0 && i > 0) v = cx_smul<FWD>(v, cx_ld(wa + (i - 1) + (j - 1) * (ido - 1)));
+        ch[i + ido * (k + l1 * j)] = v;
+      });
+    } else {
+      Cx h[IP];
+      Butterfly<FWD, IP>::run(c, h);
+      ch[i + ido * k] = h[0];
 #pragma unroll
-    for (int j = 1; j < IP; ++j) {
-      Cx v = h[j];
-      if (i > 0) v = cx_smul<FWD>(v, cx_ld(wa + (i - 1) + (j - 1) * (ido - 1)));
-      ch[i + ido * (k + l1 * j)] = v;
+      for (int j = 1; j < IP; ++j) {
+        Cx v = h[j];
+        if (i > 0) v = cx_smul<FWD>(v, cx_ld(wa + (i - 1) + (j - 1) * (ido - 1)));
+        ch[i + ido * (k + l1 * j)] = v;
+      }
     }
   }
 }
@@ -354,7 +443,7 @@ __device__ __forceinline__ void fft_pass_generic(int ido, int ip, int l1, Cx* cc
 
 // All passes of a Cooley-Tukey plan over a (in) with b as the other buffer;
 // returns the buffer that holds the result.  Callers synchronise before.
-template <bool FWD>
+template <bool FWD, bool EAGER>
 __device__ __forceinline__ Cx* fft_passes(const FftPlanDev& p, Cx* a, Cx* b) {
   Cx* p1 = a;
   Cx* p2 = b;
@@ -365,13 +454,13 @@ __device__ __forceinline__ Cx* fft_passes(const FftPlanDev& p, Cx* a, Cx* b) {
     const double2* wa = p.tw + p.twoff[f];
     bool swap = true;
     switch (ip) {
-      case 2: fft_pass<FWD, 2>(ido, l1, p1, p2, wa); break;
-      case 3: fft_pass<FWD, 3>(ido, l1, p1, p2, wa); break;
-      case 4: fft_pass<FWD, 4>(ido, l1, p1, p2, wa); break;
-      case 5: fft_pass<FWD, 5>(ido, l1, p1, p2, wa); break;
-      case 7: fft_pass<FWD, 7>(ido, l1, p1, p2, wa); break;
-      case 8: fft_pass<FWD, 8>(ido, l1, p1, p2, wa); break;
-      case 11: fft_pass<FWD, 11>(ido, l1, p1, p2, wa); break;
+      case 2: fft_pass<FWD, 2, EAGER>(ido, l1, p1, p2, wa); break;
+      case 3: fft_pass<FWD, 3, EAGER>(ido, l1, p1, p2, wa); break;
+      case 4: fft_pass<FWD, 4, EAGER>(ido, l1, p1, p2, wa); break;
+      case 5: fft_pass<FWD, 5, EAGER>(ido, l1, p1, p2, wa); break;
+      case 7: fft_pass<FWD, 7, EAGER>(ido, l1, p1, p2, wa); break;
+      case 8: fft_pass<FWD, 8, EAGER>(ido, l1, p1, p2, wa); break;
+      case 11: fft_pass<FWD, 11, EAGER>(ido, l1, p1, p2, wa); break;
       default:
         fft_pass_generic<FWD>(ido, ip, l1, p1, p2, wa, p.tw + p.twsoff[f]);
         swap = false;   // the generic pass leaves its result in place
@@ -461,9 +550,13 @@ __device__ __forceinline__ Cx line_load(const LineJob& J, int seg, int row, int 
 // multiplied by the chirp again (fftblue::fft of the library).  The launch
 // has at most MAXT threads; how many only sets how the butterflies of a pass
 // are spread over them.  SMEM: the two work buffers in dynamic shared
-// memory (shared loads and stores), else in per-CTA global scratch.
-template <bool FWD, int MAXT, bool SMEM>
-__global__ void __launch_bounds__(MAXT) k_fft_lines(const LineJob J) {
+// memory (shared loads and stores), else in per-CTA global scratch.  MINB:
+// resident CTAs per SM the register allocation is capped for (0: none
+// beyond MAXT's); where the cap is tight (several CTAs, or more than 512
+// threads) the odd-prime passes store their outputs eagerly.
+template <bool FWD, int MAXT, bool SMEM, int MINB = 0>
+__global__ void __launch_bounds__(MAXT, MINB) k_fft_lines(const LineJob J) {
+  constexpr bool EAGER = MINB > 1 || MAXT > 512;   // registers capped below ~110
   extern __shared__ double2 line_smem[];
   const FftPlanDev& P = J.plan;
   const int n = P.n, n2 = P.n2;
@@ -480,12 +573,12 @@ __global__ void __launch_bounds__(MAXT) k_fft_lines(const LineJob J) {
     __syncthreads();
     Cx* r;
     if (P.blue) {
-      r = fft_passes<true>(P, a, b);
+      r = fft_passes<true, EAGER>(P, a, b);
       for (int m = threadIdx.x; m < n2; m += blockDim.x) r[m] = cx_smul<!FWD>(r[m], cx_ld(P.bkf + m));
       __syncthreads();
-      r = fft_passes<false>(P, r, r == a ? b : a);
+      r = fft_passes<false, EAGER>(P, r, r == a ? b : a);
     } else {
-      r = fft_passes<FWD>(P, a, b);
+      r = fft_passes<FWD, EAGER>(P, a, b);
     }
     double2* out = J.cbuf[seg] + (int64_t)row * n;
     for (int m = threadIdx.x; m < n; m += blockDim.x) {

@@ -144,7 +144,7 @@ int32_t ertm_set_lane_assign(int32_t mode);
  * the interior's).  Results do not depend on it. */
 int32_t ertm_set_frame_rows(int32_t rows);
 /* Threads per CTA of the FFT line transforms of the wavenumber low-pass (a
- * multiple of 32 in [64, 512]; 0 = chosen per transform length).  Results do
+ * multiple of 32 in [64, 1024]; 0 = chosen per transform length).  Results do
  * not depend on it. */
 int32_t ertm_set_line_threads(int32_t threads);
 /* 2, 4 or 8 (1 = 8): the elastic velocity phase of 32-row interior

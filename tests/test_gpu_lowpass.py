@@ -40,7 +40,7 @@ def test_lowpass_wavenumber_bit_exact(nz, nx):
 
 # threads per CTA of the line transforms (0: the per-length choice); every
 # count must give the same bits
-LINE_THREADS = [64, 96, 128, 192, 288, 512]
+LINE_THREADS = [64, 96, 128, 192, 288, 512, 640, 1024]
 
 
 @pytest.mark.parametrize("threads", LINE_THREADS)
@@ -64,7 +64,7 @@ def test_line_threads_knob_rejects_bad_values():
     from ertm_b200 import _lib
     L = _lib.lib()
     assert L.ertm_set_line_threads(100) != 0
-    assert L.ertm_set_line_threads(1024) != 0
+    assert L.ertm_set_line_threads(1056) != 0
     assert L.ertm_set_line_threads(32) != 0
     assert L.ertm_set_line_threads(0) == 0
 
