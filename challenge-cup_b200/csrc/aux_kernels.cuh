@@ -383,6 +383,39 @@ __global__ void k_stack_add(const float* img, int64_t n, const unsigned int* sca
   acc[k] = dadd(acc[k], d);
 }
 
+// Every image's max|·| in one launch: blockIdx.y is the image.
+__global__ void k_absmax_images(const float* const* imgs, int64_t n, unsigned int* out_bits) {
+  const float* a = imgs[blockIdx.y];
+  float m = 0.f;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    m = max_nan(m, fabsf(a[k]));
+  for (int o = 16; o > 0; o >>= 1) m = max_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out_bits + blockIdx.y, __float_as_uint(m));
+}
+
+// The stack of all images at each pixel in one launch: the float64 sum runs
+// over the images in order, each term the k_stack_add term (divided by its
+// image's max|·| when normalising and that is > 0), starting from sum[k]
+// (or 0 without `sum`); the total goes back to `sum` and, with `out`, the
+// k_stack_finish mean to `out`.
+__global__ void k_stack_images(const float* const* imgs, int n_images, int64_t n, const unsigned int* scale_bits,
+                               int normalize, double* sum, int count, float* out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double acc = sum ? sum[k] : 0.0;
+#pragma unroll 4
+  for (int i = 0; i < n_images; ++i) {
+    double d = (double)imgs[i][k];
+    if (normalize) {
+      const double s = (double)__uint_as_float(scale_bits[i]);
+      if (s > 0.0) d = __ddiv_rn(d, s);
+    }
+    acc = dadd(acc, d);
+  }
+  if (sum) sum[k] = acc;
+  if (out) out[k] = __double2float_rn(__ddiv_rn(acc, (double)count));
+}
+
 __global__ void k_stack_finish(const double* acc, int64_t n, int count, float* out) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) out[k] = __double2float_rn(__ddiv_rn(acc[k], (double)count));

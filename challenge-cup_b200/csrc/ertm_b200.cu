@@ -2186,6 +2186,60 @@ struct OutArray {
   T* as() const { return static_cast<T*>(d); }
 };
 
+// The per-shot-normalised float64 stack of `n_images` images in two
+// launches per group of images: every image's max|·|, then at each pixel the
+// sum over the images in order onto `sum` (or from 0 without it) and, with
+// `out`, the mean.  Device images are read in place; host images are
+// uploaded first, in groups of at most 1 GiB.  The terms and their order are
+// those of one k_absmax_f32 + k_stack_add pair per image.
+void stack_group(int n_images, int64_t n, const float* const* images, bool normalize, double* sum, int count,
+                 float* out, cudaStream_t st) {
+  std::vector<const float*> ptrs(images, images + n_images);
+  int n_host = 0;
+  for (const float* q : ptrs) n_host += is_device_ptr(q) ? 0 : 1;
+  DevBuf stage(n_host > 0 ? (size_t)n_host * n * 4 : 0, st);
+  for (int k = 0, h = 0; k < n_images; ++k) {
+    if (is_device_ptr(ptrs[k])) continue;
+    float* dst = stage.as<float>() + (size_t)h++ * n;
+    upload(dst, ptrs[k], n * 4, st);
+    ptrs[k] = dst;
+  }
+  DevBuf table((size_t)n_images * (sizeof(float*) + sizeof(unsigned)), st);
+  upload(table.p, ptrs.data(), (size_t)n_images * sizeof(float*), st);
+  const float* const* dptrs = table.as<const float*>();
+  unsigned* scales = reinterpret_cast<unsigned*>(table.as<char>() + (size_t)n_images * sizeof(float*));
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (normalize) {
+    CK(cudaMemsetAsync(scales, 0, (size_t)n_images * sizeof(unsigned), st));
+    const unsigned bx = std::max(1u, std::min<unsigned>(g, (2368u + n_images - 1) / n_images));
+    k_absmax_images<<<dim3(bx, n_images), 256, 0, st>>>(dptrs, n, scales);
+    ++g_launches;
+  }
+  k_stack_images<<<g, 256, 0, st>>>(dptrs, n_images, n, scales, normalize ? 1 : 0, sum, count, out);
+  ++g_launches;
+  CK(cudaGetLastError());
+}
+
+void stack_all(int n_images, int64_t n, const float* const* images, bool normalize, double* sum, int count,
+               float* out, cudaStream_t st) {
+  if (n_images <= 0) return;
+  const int per = (int)std::max<int64_t>(1, std::min<int64_t>(65535, (int64_t(1) << 30) / (n * 4)));
+  if (n_images <= per) {
+    stack_group(n_images, n, images, normalize, sum, count, out, st);
+    return;
+  }
+  DevBuf acc(sum ? 0 : (size_t)n * 8, st);
+  double* s = sum;
+  if (!s) {
+    s = acc.as<double>();
+    CK(cudaMemsetAsync(s, 0, (size_t)n * 8, st));
+  }
+  for (int k0 = 0; k0 < n_images; k0 += per) {
+    const int nk = std::min(per, n_images - k0);
+    stack_group(nk, n, images + k0, normalize, s, count, k0 + nk == n_images ? out : nullptr, st);
+  }
+}
+
 }  // namespace
 
 // ==========================================================================
@@ -3014,20 +3068,10 @@ int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int3
       CK(cudaStreamSynchronize(st));
       return;
     }
-    DevBuf acc(n * 8, st), img(n * 4, st), o(n * 4, st), sc(4, st);
-    CK(cudaMemsetAsync(acc.p, 0, n * 8, st));
-    const unsigned g = (unsigned)((n + 255) / 256);
-    for (int k = 0; k < n_images; ++k) {
-      upload(img.p, images[k], n * 4, st);
-      CK(cudaMemsetAsync(sc.p, 0, 4, st));
-      if (normalize) k_absmax_f32<<<std::min<unsigned>(g, 1184), 256, 0, st>>>(img.as<float>(), n, sc.as<unsigned>());
-      k_stack_add<<<g, 256, 0, st>>>(img.as<float>(), n, sc.as<unsigned>(), normalize, acc.as<double>());
-      g_launches += normalize ? 2 : 1;
-    }
-    k_stack_finish<<<g, 256, 0, st>>>(acc.as<double>(), n, n_images, o.as<float>());
-    ++g_launches;
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDefault, st));
+    const bool dev_out = is_device_ptr(out);
+    DevBuf o(dev_out ? 0 : n * 4, st);
+    stack_all(n_images, n, images, normalize != 0, nullptr, n_images, dev_out ? out : o.as<float>(), st);
+    if (!dev_out) CK(cudaMemcpyAsync(out, o.p, n * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
   });
 }
@@ -3038,23 +3082,7 @@ int32_t ertm_stack_partial(int32_t n_images, int64_t n, const float* const* imag
     REQUIRE(n_images >= 0 && n >= 1 && (images || n_images == 0) && sum, "bad arguments");
     require_device_pointer(sum, "sum");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    DevBuf img, sc(4, st);
-    const unsigned g = (unsigned)((n + 255) / 256);
-    for (int k = 0; k < n_images; ++k) {
-      const float* src = images[k];
-      cudaPointerAttributes a{};
-      CK(cudaPointerGetAttributes(&a, src));
-      if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) {
-        if (!img.p) img = DevBuf(n * 4, st);
-        upload(img.p, src, n * 4, st);
-        src = img.as<float>();
-      }
-      CK(cudaMemsetAsync(sc.p, 0, 4, st));
-      if (normalize) k_absmax_f32<<<std::min<unsigned>(g, 1184), 256, 0, st>>>(src, n, sc.as<unsigned>());
-      k_stack_add<<<g, 256, 0, st>>>(src, n, sc.as<unsigned>(), normalize, sum);
-      g_launches += normalize ? 2 : 1;
-    }
-    CK(cudaGetLastError());
+    stack_all(n_images, n, images, normalize != 0, sum, 1, nullptr, st);
     CK(cudaStreamSynchronize(st));
   });
 }
