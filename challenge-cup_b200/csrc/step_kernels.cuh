@@ -678,7 +678,9 @@ __device__ __forceinline__ ColInfo col_info(const Geo& G, int j, const float* ax
 // 700-705): r_l ← r_l·a_l(Q) + b_l·Δε for l = 0 … L−1, total = Σ_l r_l in
 // that order.  Each r_l and b_l row is one aligned 16-byte word, so a
 // mechanism costs two vector loads and one vector store.  Columns with
-// keep[c] set are left as they are.
+// keep[c] set are left as they are.  Up to kRelaxUnroll mechanisms run
+// unrolled.
+constexpr int kRelaxUnroll = 4;
 __device__ __forceinline__ void relax4(float* r0, const float* b0, size_t fstride, const uint8_t* qidx,
                                        const float* relax_a, int nL, size_t g, const float (&inc)[4],
                                        const bool (&keep)[4], float (&tot)[4]) {
@@ -686,6 +688,34 @@ __device__ __forceinline__ void relax4(float* r0, const float* b0, size_t fstrid
   const int q[4] = {q4.x, q4.y, q4.z, q4.w};
 #pragma unroll
   for (int c = 0; c < 4; ++c) tot[c] = 0.f;
+  if (nL <= kRelaxUnroll) {
+    // every mechanism's memory and coefficient loaded before any memory is
+    // stored, so all the loads are in flight together (the compiler cannot
+    // move a load of r_{l+1} above the store of r_l by itself: it does not
+    // know that the arrays are distinct)
+    float4 r4[kRelaxUnroll], b4[kRelaxUnroll];
+#pragma unroll
+    for (int l = 0; l < kRelaxUnroll; ++l) {
+      if (l < nL) {
+        r4[l] = ld4(r0 + l * fstride + g);
+        b4[l] = ldg4(b0 + l * fstride + g);
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < kRelaxUnroll; ++l) {
+      if (l < nL) {
+        float4 o4;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float rv = fadd(fmul(comp(r4[l], c), __ldg(relax_a + q[c] * nL + l)), fmul(comp(b4[l], c), inc[c]));
+          set_comp(o4, c, keep[c] ? comp(r4[l], c) : rv);
+          tot[c] = (l == 0) ? rv : fadd(tot[c], rv);
+        }
+        st4(r0 + l * fstride + g, o4);
+      }
+    }
+    return;
+  }
   for (int l = 0; l < nL; ++l) {
     float* rl = r0 + l * fstride;
     const float4 r4 = ld4(rl + g);
@@ -1025,10 +1055,18 @@ __device__ __forceinline__ void block_max_to(float v, float* dst) {
   }
 }
 
+// Resident blocks per SM the viscoacoustic interior stress kernel is
+// compiled for.  Its relaxation loads are all issued before the stores,
+// which uncapped takes 80 registers (6 blocks per SM); capped for 9 blocks
+// (56 registers, no spills) a 4-shot tick of the 2001×801 job took 159 µs,
+// against 171 µs uncapped and 170 µs with one mechanism loaded at a time.
+template <bool VISCO, int KIND, int R>
+constexpr int kStressMinBlocks = (VISCO && KIND == TILES_INTERIOR && R == 1) ? 9 : 1;
+
 // Acoustic (VISCO=false): p += (dt·κ)·div.  Viscoacoustic (VISCO=true):
 // ε += dt·div; r_l ← r_l·a_l + b_l·Δε; p = K_R·ε + Σ r_l.
 template <int M, int BZ, int R, bool VISCO, int KIND, class WS, class TM>
-__global__ void __launch_bounds__(XT* BZ)
+__global__ void __launch_bounds__(XT* BZ, kStressMinBlocks<VISCO, KIND, R>)
 k_pressure_stress(const DevProp* __restrict__ props, const WS ws, const __grid_constant__ TM tm) {
   constexpr int TZ = BZ * R;
   using T = TileShape<M, TZ>;
