@@ -394,6 +394,29 @@ __device__ __forceinline__ void run_epilogue(const Epilogue& E, size_t c, size_t
       // imaging.py:313-324: illum += S², rillum += R² (all steps); num += S·R (t ≥ start)
       const float s0 = E.src[0] ? E.src[0][c] : 0.f;
       const float s1 = E.src[1] ? E.src[1][c] : 0.f;
+      if (!E.kahan) {
+        // float64 sums: every accumulator value is loaded before any is
+        // stored, so the loads are in flight together (the compiler cannot
+        // move a load above a store to another accumulator by itself)
+        double vi[MAX_EPI_IMAGES], vr[MAX_EPI_IMAGES], vn[MAX_EPI_IMAGES];
+#pragma unroll
+        for (int k = 0; k < MAX_EPI_IMAGES; ++k) {
+          if (k >= E.n_images) break;
+          if (E.illum && E.ill[k]) vi[k] = E.ill[k][c];
+          if (E.rillum && E.ril[k]) vr[k] = E.ril[k][c];
+          if (E.cross) vn[k] = E.num[k][c];
+        }
+#pragma unroll
+        for (int k = 0; k < MAX_EPI_IMAGES; ++k) {
+          if (k >= E.n_images) break;
+          const float s = E.src_slot[k] ? s1 : s0;
+          const float r = E.rcv_wave[k] ? sv : pv;
+          if (E.illum && E.ill[k]) E.ill[k][c] = dadd(vi[k], (double)fmul(s, s));
+          if (E.rillum && E.ril[k]) E.ril[k][c] = dadd(vr[k], (double)fmul(r, r));
+          if (E.cross) E.num[k][c] = dadd(vn[k], (double)fmul(s, r));
+        }
+        break;
+      }
 #pragma unroll
       for (int k = 0; k < MAX_EPI_IMAGES; ++k) {
         if (k >= E.n_images) break;
