@@ -51,6 +51,9 @@ def main(argv=None) -> None:
     ap.add_argument("--save", default=None, help="write the stacked images of the last repeat (.npy)")
     ap.add_argument("--lowpass", default=None, metavar="NZxNX",
                     help="time the wavenumber low-pass of one float64 NZxNX array instead of a job")
+    ap.add_argument("--line-threads", default="0", metavar="T[,T...]",
+                    help="with --lowpass: threads per CTA of the line transforms, one run per value (0: automatic); "
+                         "every run's result is compared with the first")
     args = ap.parse_args(argv)
 
     import torch
@@ -140,8 +143,10 @@ def main(argv=None) -> None:
 
 
 def lowpass_only(args) -> None:
-    """Repeated ertm_lowpass_wavenumber calls on a device array (the last
-    repeat inside the NVTX range ``job``); prints the time per call."""
+    """Repeated ertm_lowpass_wavenumber calls on a device array for each
+    --line-threads value (the last repeat of each inside the NVTX range
+    ``job``); prints the time per call and whether the result equals the
+    first value's."""
     import torch
 
     from ertm_b200 import _lib
@@ -149,21 +154,31 @@ def lowpass_only(args) -> None:
     nz, nx = (int(v) for v in args.lowpass.lower().split("x"))
     a = torch.randn(nz, nx, dtype=torch.float64, device="cuda")
     b = torch.empty_like(a)
-    ms = []
-    for r in range(args.repeat):
-        last = r == args.repeat - 1
-        torch.cuda.synchronize()
-        if last:
-            torch.cuda.nvtx.range_push("job")
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        _lib.check(L.ertm_lowpass_wavenumber(nz, nx, 5.0, 5.0, 0.5, a.data_ptr(), b.data_ptr(), None), "lowpass")
-        e1.record()
-        torch.cuda.synchronize()
-        if last:
-            torch.cuda.nvtx.range_pop()
-        ms.append(e0.elapsed_time(e1))
-    print(json.dumps({"lowpass": [nz, nx], "ms_per_call": ms}), flush=True)
+    first = None
+    try:
+        for threads in (int(v) for v in args.line_threads.split(",")):
+            _lib.check(L.ertm_set_line_threads(threads), "line threads")
+            ms = []
+            for r in range(args.repeat):
+                last = r == args.repeat - 1
+                torch.cuda.synchronize()
+                if last:
+                    torch.cuda.nvtx.range_push("job")
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _lib.check(L.ertm_lowpass_wavenumber(nz, nx, 5.0, 5.0, 0.5, a.data_ptr(), b.data_ptr(), None),
+                           "lowpass")
+                e1.record()
+                torch.cuda.synchronize()
+                if last:
+                    torch.cuda.nvtx.range_pop()
+                ms.append(e0.elapsed_time(e1))
+            if first is None:
+                first = b.clone()
+            print(json.dumps({"lowpass": [nz, nx], "line_threads": threads, "ms_per_call": ms,
+                              "equal_to_first": bool(torch.equal(first, b))}), flush=True)
+    finally:
+        _lib.check(L.ertm_set_line_threads(0), "line threads")
 
 
 if __name__ == "__main__":
