@@ -251,7 +251,9 @@ void launch_lines(LineJob J, bool fwd, cudaStream_t st) {
   }
   const bool wide = smem > kLineSmemWide;
   const int forced = g_line_threads.load();
-  const int t = !J.use_smem ? 512 : forced > 0 ? forced : wide ? 512 : 256;
+  // one CTA per SM (wide lines): 704 threads of the 768-thread build; else
+  // 256 threads, three CTAs per SM (the fastest counts on 811×2011 fields)
+  const int t = !J.use_smem ? 512 : forced > 0 ? forced : wide ? 704 : 256;
   if (!J.use_smem) {
     if (fwd) k_fft_lines<true, 512, false><<<grid, t, 0, st>>>(J);
     else k_fft_lines<false, 512, false><<<grid, t, 0, st>>>(J);
