@@ -314,6 +314,33 @@ __global__ void k_stab_scale(const DevProp* props, int pi, StabState* st, double
   }
 }
 
+// k_stab_scale followed by k_epilogue in one pass, for a compensated
+// viscoacoustic step with no low-pass between them: each thread owns one
+// padded cell, scales every field there when the cap clips (the cells and
+// the arithmetic of k_stab_scale), and a physical cell's epilogue images
+// the p value of its own cell (image_value of a pressure engine), which the
+// same thread has just scaled.
+template <int M>
+__global__ void k_stab_epilogue(const DevProp* props, int pi, StabState* st, double cap, Epilogue E) {
+  const DevProp& P = props[pi];
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;   // padded column, < ld
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;   // padded row, < nzp
+  if (ii >= P.nzp || jj >= P.ld) return;
+  const size_t k = (size_t)ii * P.ld + jj;
+  const double peak = (double)*P.peak;
+  const double ref = st->ref_amp > 1e-30 ? st->ref_amp : 1e-30;
+  const double limit = cap * ref;
+  if (peak > limit) {
+    const float s = __double2float_rn(__ddiv_rn(limit, peak));
+    if (ii == 0 && jj == 0) st->clipped += 1;
+    const int nf = 4 + P.L;
+    for (int f = 0; f < nf; ++f) P.f[f][k] = fmul(P.f[f][k], s);
+  }
+  const int pz = ii - P.pad, px = jj - P.pad;
+  if (pz < 0 || pz >= P.nz || px < 0 || px >= P.nx) return;
+  run_epilogue(E, (size_t)pz * P.nx + px, (size_t)P.nz * P.nx, image_value<M>(P, WAVE_P, E.sep, ii, jj), 0.f);
+}
+
 // ---------------------------------------------------------------------------
 // image post-processing (imaging.py:326-331, 476-502; numerics.py:398-404)
 // ---------------------------------------------------------------------------

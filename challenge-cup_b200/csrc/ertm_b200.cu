@@ -201,12 +201,10 @@ std::map<std::pair<int, int>, std::unique_ptr<LineFftPlan>> g_line_plans;
 std::mutex g_line_mutex;
 
 constexpr size_t kLineSmemMax = 227 * 1024;       // opt-in dynamic shared memory per CTA
-#ifndef ERTM_LINE_NARROW_MIN_BLOCKS
-#define ERTM_LINE_NARROW_MIN_BLOCKS 3
-#endif
 // Resident CTAs per SM the 256-thread line transforms are compiled for (the
-// register cap follows: 3 → 80 registers, 2 → 128)
-constexpr int kLineNarrowMinBlocks = ERTM_LINE_NARROW_MIN_BLOCKS;
+// register cap follows: 3 → 80 registers; 2 → 128 registers was 3 % slower
+// on 811×2011 fields, 1 → 174–200 registers 26 % slower)
+constexpr int kLineNarrowMinBlocks = 3;
 constexpr size_t kLineSmemWide = 113 * 1024;      // above this only one CTA fits an SM: use 512 threads
 constexpr int64_t kLineScratchCtas = 296;         // CTAs of a launch whose lines do not fit in shared memory
 
@@ -448,6 +446,7 @@ struct Prop {
   int64_t step_index = 0;
   int tiles_x = 0, tiles = 0, tz = 32;
   int lowpass_steps = 0;
+  bool stab_pending = false;   // after_step left the stabilisation scale to launch_epilogue
   float k_src = 0.f;             // K_R at the source node (viscoacoustic)
   std::vector<double> rx, rz;
   std::map<int, std::unique_ptr<SamplePlanHost>> samples;
@@ -1151,7 +1150,11 @@ StepWork make_work(const Prop& P, double amp64, const float* wave, int t, const 
 // With `defer`, a low-pass due at this step is appended there for the
 // caller to run (together with other propagators' low-passes) before
 // anything reads the fields again; otherwise it runs here.
-void after_step(Prop& P, double amp64, const float* wave, int t, std::vector<LowpassItem>* defer = nullptr) {
+// fuse_stab: the caller launches this propagator's stand-alone epilogue
+// next (launch_epilogue), so on a step without a low-pass the stabilisation
+// scale is left pending and runs inside that launch.
+void after_step(Prop& P, double amp64, const float* wave, int t, std::vector<LowpassItem>* defer = nullptr,
+                bool fuse_stab = false) {
   const bool force_z = P.h.engine == ENGINE_ELASTIC && P.h.mech == MECH_FORCE_Z && P.h.src_iz >= 0;
   if (force_z && (wave || amp64 != 0.0)) {
     const int64_t idx = (int64_t)P.h.src_iz * P.h.ld + P.h.src_ix;
@@ -1161,13 +1164,17 @@ void after_step(Prop& P, double amp64, const float* wave, int t, std::vector<Low
   }
   if (P.h.engine == ENGINE_VISCO && P.cfg.compensation) {
     const int64_t s = P.step_index;
-    ++g_launches;
+    const int every = P.cfg.lowpass_interval;
+    const bool lowpass = s >= 30 && every > 1 && s % every == 0;
     if (s < 30) {
       k_stab_reference<<<1, 32, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>());
+      ++g_launches;
+    } else if (fuse_stab && !lowpass) {
+      P.stab_pending = true;
     } else {
       k_stab_scale<<<296, 256, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>(), P.cfg.amplitude_cap);
-      const int every = P.cfg.lowpass_interval;
-      if (every > 1 && s % every == 0) {
+      ++g_launches;
+      if (lowpass) {
         ++P.lowpass_steps;
         const double time = (double)s * P.cfg.dt;
         const double ratio = std::max(0.9 - 0.4 * std::min(time / 1.0, 1.0), 0.35);
@@ -1180,14 +1187,15 @@ void after_step(Prop& P, double amp64, const float* wave, int t, std::vector<Low
   ++P.step_index;
 }
 
-void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, const Epilogue* epi = nullptr) {
+void step_once(Prop& P, double amp64, const float* wave = nullptr, int t = 0, const Epilogue* epi = nullptr,
+               bool fuse_stab = false) {
   WorkSet1 ws{make_work(P, amp64, wave, t, epi)};
   cudaEvent_t e0 = nullptr;
   const bool timed = g_prof.begin(P.st, e0);
   const Prop* hosts[1] = {&P};
   launch_works(P.M, P.tz, P.h.engine, P.dp(), ws, 1, hosts, P.st);
   if (timed) g_prof.end(P.st, e0, step_bytes(P) + (epi ? epilogue_bytes(*epi, (size_t)P.h.nz * P.h.nx) : 0.0));
-  after_step(P, amp64, wave, t);
+  after_step(P, amp64, wave, t, nullptr, fuse_stab);
 }
 
 void image_field(Prop& P, int wave, int sep, float* out) {
@@ -1357,12 +1365,20 @@ Prop* create(const ertm_prop_config* cfg, const float* vp, const float* vs, cons
 // migrate
 // --------------------------------------------------------------------------
 template <int M>
-void launch_epilogue_M(const Prop& P, const Epilogue& E) {
-  const dim3 b2(32, 8), g2((P.h.nx + 31) / 32, (P.h.nz + 7) / 8);
+void launch_epilogue_M(Prop& P, const Epilogue& E) {
+  const dim3 b2(32, 8);
+  if (P.stab_pending) {
+    // the step's stabilisation scale with the epilogue (after_step left it)
+    P.stab_pending = false;
+    const dim3 g2((unsigned)((P.h.ld + 31) / 32), (unsigned)((P.h.nzp + 7) / 8));
+    k_stab_epilogue<M><<<g2, b2, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>(), P.cfg.amplitude_cap, E);
+    return;
+  }
+  const dim3 g2((P.h.nx + 31) / 32, (P.h.nz + 7) / 8);
   k_epilogue<M><<<g2, b2, 0, P.st>>>(P.dp(), 0, E);
 }
 
-void launch_epilogue(const Prop& P, const Epilogue& E) {
+void launch_epilogue(Prop& P, const Epilogue& E) {
   switch (P.M) {
     case 1: launch_epilogue_M<1>(P, E); break;
     case 2: launch_epilogue_M<2>(P, E); break;
@@ -1614,7 +1630,7 @@ void migrate(Prop& F, Prop& B, const ertm_migrate_config& cfg, const float* wave
     if (e.kind == EPI_NONE) {
       step_once(B, 0.0);
     } else if (R.bwd_unfused) {
-      step_once(B, 0.0);
+      step_once(B, 0.0, nullptr, 0, nullptr, true);
       launch_epilogue(B, e);
     } else {
       step_once(B, 0.0, nullptr, 0, &e);
@@ -1972,7 +1988,7 @@ bool batch_tick(std::vector<ShotRun*>& runs, const DevProp* dt, cudaStream_t st)
   for (TickItem& it : items) {
     ShotRun& R = *it.run;
     Prop& P = it.fwd ? *R.F : *R.B;
-    after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t, &lowpasses);
+    after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t, &lowpasses, it.unfused);
   }
   if (!lowpasses.empty()) lowpass_props(lowpasses, st);
   for (TickItem& it : items) {
