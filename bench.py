@@ -74,7 +74,11 @@ def launch_ranks(args) -> int:
         port = sk.getsockname()[1]
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
            "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
-    return subprocess.call(cmd)
+    try:   # a last bound well above the process group's own timeout
+        return subprocess.call(cmd, timeout=3600)
+    except subprocess.TimeoutExpired:
+        print(json.dumps({"error": "ranks did not finish within 3600 s"}), flush=True)
+        return 1
 
 
 # ---------------------------------------------------------------------------
@@ -95,7 +99,9 @@ class Dist:
             backend = "nccl" if torch.cuda.is_available() else "gloo"
             if backend == "nccl":
                 torch.cuda.set_device(self.local)
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            # short enough that ranks left waiting on a failed peer end with an error
+            # (the longest gap between collectives is the per-rank set-up, well under it)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.pg = dist
 
     def barrier(self) -> None:
