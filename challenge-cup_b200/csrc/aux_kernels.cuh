@@ -341,6 +341,50 @@ __global__ void k_stab_epilogue(const DevProp* props, int pi, StabState* st, dou
   run_epilogue(E, (size_t)pz * P.nx + px, (size_t)P.nz * P.nx, image_value<M>(P, WAVE_P, E.sep, ii, jj), 0.f);
 }
 
+// The stand-alone epilogues of a batched tick in one launch: blockIdx.z is
+// the item, x and y cover its padded grid (blocks outside it exit).  An item
+// with `stab` set first applies its step's stabilisation scale, as
+// k_stab_epilogue does; every item images its physical cells as k_epilogue
+// does (P and, for elastic S, from image_value).
+struct EpiItem {
+  int32_t prop;      // index into the launch's DevProp table
+  int32_t stab;      // 1: the step's stabilisation scale runs here first
+  double cap;        // amplitude cap (stab)
+  StabState* st;     // stabilisation state (stab)
+  Epilogue E;
+};
+struct EpiBatch {
+  int32_t n;
+  int32_t pad_;
+  EpiItem it[MAX_BATCH_WORKS];
+};
+
+template <int M>
+__global__ void k_epilogue_batch(const DevProp* table, const __grid_constant__ EpiBatch B) {
+  const EpiItem& I = B.it[blockIdx.z];
+  const DevProp& P = table[I.prop];
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;   // padded column, < ld
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;   // padded row, < nzp
+  if (ii >= P.nzp || jj >= P.ld) return;
+  if (I.stab) {
+    const double peak = (double)*P.peak;
+    const double ref = I.st->ref_amp > 1e-30 ? I.st->ref_amp : 1e-30;
+    const double limit = I.cap * ref;
+    if (peak > limit) {
+      const float s = __double2float_rn(__ddiv_rn(limit, peak));
+      if (ii == 0 && jj == 0) I.st->clipped += 1;
+      const size_t k = (size_t)ii * P.ld + jj;
+      const int nf = 4 + P.L;
+      for (int f = 0; f < nf; ++f) P.f[f][k] = fmul(P.f[f][k], s);
+    }
+  }
+  const int pz = ii - P.pad, px = jj - P.pad;
+  if (pz < 0 || pz >= P.nz || px < 0 || px >= P.nx) return;
+  const float pv = image_value<M>(P, WAVE_P, I.E.sep, ii, jj);
+  const float sv = (P.engine == ENGINE_ELASTIC && I.E.need_s) ? image_value<M>(P, WAVE_S, I.E.sep, ii, jj) : 0.f;
+  run_epilogue(I.E, (size_t)pz * P.nx + px, (size_t)P.nz * P.nx, pv, sv);
+}
+
 // ---------------------------------------------------------------------------
 // image post-processing (imaging.py:326-331, 476-502; numerics.py:398-404)
 // ---------------------------------------------------------------------------

@@ -1874,6 +1874,42 @@ void launch_group(std::vector<TickItem*>& items, const DevProp* table, cudaStrea
   }
 }
 
+// The stand-alone epilogues of a tick's items (all of stencil half-order M,
+// all on stream st) in launches of up to MAX_BATCH_WORKS items; an item
+// whose stabilisation scale after_step left pending gets it here.
+template <int M>
+void launch_epilogue_batch_M(const std::vector<TickItem*>& its, const DevProp* table, cudaStream_t st) {
+  static_assert(sizeof(EpiBatch) < 30000, "kernel parameter block too large");
+  for (size_t c0 = 0; c0 < its.size(); c0 += MAX_BATCH_WORKS) {
+    EpiBatch B{};
+    unsigned gx = 1, gy = 1;
+    for (size_t k = c0; k < std::min(its.size(), c0 + MAX_BATCH_WORKS); ++k) {
+      TickItem& it = *its[k];
+      Prop& P = it.fwd ? *it.run->F : *it.run->B;
+      EpiItem& I = B.it[B.n++];
+      I.prop = it.w.prop;
+      I.stab = P.stab_pending ? 1 : 0;
+      P.stab_pending = false;
+      I.cap = P.cfg.amplitude_cap;
+      I.st = P.stab.as<StabState>();
+      I.E = it.epi;
+      gx = std::max(gx, (unsigned)((P.h.ld + 31) / 32));
+      gy = std::max(gy, (unsigned)((P.h.nzp + 7) / 8));
+    }
+    k_epilogue_batch<M><<<dim3(gx, gy, (unsigned)B.n), dim3(32, 8), 0, st>>>(table, B);
+    ++g_launches;
+  }
+}
+
+void launch_epilogue_batch(int M, const std::vector<TickItem*>& its, const DevProp* table, cudaStream_t st) {
+  switch (M) {
+    case 1: launch_epilogue_batch_M<1>(its, table, st); break;
+    case 2: launch_epilogue_batch_M<2>(its, table, st); break;
+    case 3: launch_epilogue_batch_M<3>(its, table, st); break;
+    default: launch_epilogue_batch_M<4>(its, table, st); break;
+  }
+}
+
 // DevProp table of every propagator of `runs` (uploaded when the set changes).
 void upload_table(std::vector<ShotRun*>& runs, std::vector<DevProp>& table, DevBuf& dtable, cudaStream_t st) {
   table.clear();
@@ -1991,12 +2027,19 @@ bool batch_tick(std::vector<ShotRun*>& runs, const DevProp* dt, cudaStream_t st)
     after_step(P, 0.0, it.fwd ? R.wave.as<float>() : nullptr, it.w.t, &lowpasses, it.unfused);
   }
   if (!lowpasses.empty()) lowpass_props(lowpasses, st);
+  // stand-alone epilogues: one launch per stencil order (k_epilogue_batch)
+  // when they share the tick's stream, else one launch each
+  std::map<int, std::vector<TickItem*>> unfused;
   for (TickItem& it : items) {
     ShotRun& R = *it.run;
     Prop& P = it.fwd ? *R.F : *R.B;
-    if (it.unfused) launch_epilogue(P, it.epi);
+    if (it.unfused) {
+      if (P.st == st) unfused[P.M].push_back(&it);
+      else launch_epilogue(P, it.epi);
+    }
     if (R.phase == 0 && R.t_f % R.iv == 0) save_checkpoint(R, R.t_f / R.iv, st);
   }
+  for (auto& g : unfused) launch_epilogue_batch(g.first, g.second, dt, st);
   CK(cudaGetLastError());
   // advance the schedules
   for (ShotRun* Rp : runs) {
