@@ -314,6 +314,11 @@ __global__ void k_stab_scale(const DevProp* props, int pi, StabState* st, double
   }
 }
 
+// Column origin of the padded grid in k_epilogue_batch / k_stab_epilogue:
+// thread column t handles padded column t − epi_col_shift(pad), so that the
+// physical columns (and the accumulators' rows) start at a multiple of 32.
+__device__ __forceinline__ int epi_col_shift(int pad) { return ((pad + 31) / 32) * 32 - pad; }
+
 // k_stab_scale followed by k_epilogue in one pass, for a compensated
 // viscoacoustic step with no low-pass between them: each thread owns one
 // padded cell, scales every field there when the cap clips (the cells and
@@ -323,9 +328,9 @@ __global__ void k_stab_scale(const DevProp* props, int pi, StabState* st, double
 template <int M>
 __global__ void k_stab_epilogue(const DevProp* props, int pi, StabState* st, double cap, Epilogue E) {
   const DevProp& P = props[pi];
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x;   // padded column, < ld
-  const int ii = blockIdx.y * blockDim.y + threadIdx.y;   // padded row, < nzp
-  if (ii >= P.nzp || jj >= P.ld) return;
+  const int jj = (int)(blockIdx.x * blockDim.x + threadIdx.x) - epi_col_shift(P.pad);   // padded column
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;                                   // padded row
+  if (ii >= P.nzp || jj < 0 || jj >= P.ld) return;
   const size_t k = (size_t)ii * P.ld + jj;
   const double peak = (double)*P.peak;
   const double ref = st->ref_amp > 1e-30 ? st->ref_amp : 1e-30;
@@ -363,9 +368,9 @@ template <int M>
 __global__ void k_epilogue_batch(const DevProp* table, const __grid_constant__ EpiBatch B) {
   const EpiItem& I = B.it[blockIdx.z];
   const DevProp& P = table[I.prop];
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x;   // padded column, < ld
-  const int ii = blockIdx.y * blockDim.y + threadIdx.y;   // padded row, < nzp
-  if (ii >= P.nzp || jj >= P.ld) return;
+  const int jj = (int)(blockIdx.x * blockDim.x + threadIdx.x) - epi_col_shift(P.pad);   // padded column
+  const int ii = blockIdx.y * blockDim.y + threadIdx.y;                                   // padded row
+  if (ii >= P.nzp || jj < 0 || jj >= P.ld) return;
   if (I.stab) {
     const double peak = (double)*P.peak;
     const double ref = I.st->ref_amp > 1e-30 ? I.st->ref_amp : 1e-30;

@@ -1370,7 +1370,7 @@ void launch_epilogue_M(Prop& P, const Epilogue& E) {
   if (P.stab_pending) {
     // the step's stabilisation scale with the epilogue (after_step left it)
     P.stab_pending = false;
-    const dim3 g2((unsigned)((P.h.ld + 31) / 32), (unsigned)((P.h.nzp + 7) / 8));
+    const dim3 g2((unsigned)((P.h.ld + 31 + 31) / 32), (unsigned)((P.h.nzp + 7) / 8));   // + the column shift
     k_stab_epilogue<M><<<g2, b2, 0, P.st>>>(P.dp(), 0, P.stab.as<StabState>(), P.cfg.amplitude_cap, E);
     return;
   }
@@ -1893,7 +1893,7 @@ void launch_epilogue_batch_M(const std::vector<TickItem*>& its, const DevProp* t
       I.cap = P.cfg.amplitude_cap;
       I.st = P.stab.as<StabState>();
       I.E = it.epi;
-      gx = std::max(gx, (unsigned)((P.h.ld + 31) / 32));
+      gx = std::max(gx, (unsigned)((P.h.ld + 31 + 31) / 32));   // + the column shift (< 32)
       gy = std::max(gy, (unsigned)((P.h.nzp + 7) / 8));
     }
     k_epilogue_batch<M><<<dim3(gx, gy, (unsigned)B.n), dim3(32, 8), 0, st>>>(table, B);
