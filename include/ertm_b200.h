@@ -344,7 +344,11 @@ int32_t ertm_segy_decode(const uint8_t* traces, int64_t n_traces, int64_t ns, in
 int32_t ertm_segy_encode(const float* rec, int64_t ns, int64_t ntr, int32_t fmt, const uint8_t* headers,
                          uint8_t* traces, void* stream);
 
-/* stack_images (pipeline.py:133-161): images is n_images pointers to (n,) float32. */
+/* stack_images (pipeline.py:133-161): images is n_images pointers to (n,)
+ * float32, each host or device memory (device images are read in place, host
+ * images uploaded in groups of at most 1 GiB); out is host or device memory.
+ * All images of a group go through two launches: every image's max|.|, then
+ * the float64 sum over the images in order at each pixel. */
 int32_t ertm_stack(int32_t n_images, int64_t n, const float* const* images, int32_t normalize, float* out,
                    void* stream);
 
